@@ -1,0 +1,172 @@
+/*
+ * sphb200 — C ABI of the B200 (sm_100a) SPH-VE hydro hot path.
+ *
+ * Plain C types only: device pointers are passed as typed pointers into device memory, CUDA streams as void*
+ * (a cudaStream_t; NULL = the legacy default stream). Every function returns an sphb status code and never exits
+ * the process (the reference's checkGpuErrors calls exit(), cstone/cuda/errorcheck.cuh:15-26).
+ *
+ * Two layers:
+ *   1. kernel entry points on caller-owned device arrays — the drop-in for the cstone::*Gpu and sph::gpu::*
+ *      functions that the reference's host dispatchers call under HaveGpu<Accelerator> (each cited below);
+ *   2. an opaque simulation object (sphb_sim) that owns the particle dataset in HBM and runs the whole step of
+ *      HydroVeProp (main/src/propagator/ve_hydro.hpp:126-220): domain sync, neighbour search, VE chain, integration.
+ */
+#ifndef SPHB200_H
+#define SPHB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* status codes                                                                                                     */
+/* ---------------------------------------------------------------------------------------------------------------- */
+#define SPHB_OK 0
+#define SPHB_ERR_ARG 1           /* invalid argument (null pointer, bad size, ng0 > ngmax, ...)                     */
+#define SPHB_ERR_CUDA 2          /* a CUDA runtime call failed; message printed to stderr                           */
+#define SPHB_ERR_CAPACITY 3      /* a bounded device buffer or wait was exhausted (scratch, traversal, lookback)    */
+#define SPHB_ERR_NOT_CONVERGED 4 /* smoothing-length iteration left particles with nc <= 1 (update_h_gpu.cu:51-55) */
+#define SPHB_ERR_STATE 5         /* call out of order (e.g. step before upload)                                    */
+
+/* precision of the neighbour sums (the SPH-VE J-loops) */
+#define SPHB_FP64 0  /* every field and sum in double: the plain drop-in                                           */
+#define SPHB_MIXED 1 /* FP32 neighbour sums with compensated accumulation on FP64 relative coordinates            */
+
+/*! Coordinate box; replaces cstone::Box<double> (domain/include/cstone/sfc/box.hpp:94-174). periodic[k] != 0 makes
+ *  axis k periodic, else open. */
+typedef struct
+{
+    double lo[3];
+    double hi[3];
+    int periodic[3];
+} sphb_box;
+
+/*! Physics settings; defaults of ParticlesData (sph/include/sph/particles_data.hpp:85-143). */
+typedef struct
+{
+    uint32_t ng0;           /* target neighbour count (100)                                */
+    uint32_t ngmax;         /* neighbour list capacity per particle (150)                  */
+    double gamma;           /* adiabatic index (5/3)                                       */
+    double mui;             /* mean molecular weight of ions (10)                          */
+    double Kcour;           /* Courant factor (0.2)                                        */
+    double Krho;            /* 1/|divv| time-step factor (0.06)                            */
+    double alphamin;        /* AV switch floor (0.05)                                      */
+    double alphamax;        /* AV switch ceiling (1.0)                                     */
+    double decay_constant;  /* AV decay (0.2)                                              */
+    double sinc_index;      /* exponent n of the sinc^n kernel (6)                         */
+    double minDt;           /* initial time step                                           */
+    double minDt_m1;        /* previous time step                                          */
+    int precision;          /* SPHB_FP64 or SPHB_MIXED                                     */
+    uint32_t bucket_focus;  /* max particles per leaf of the neighbour-search tree (64)    */
+} sphb_params;
+
+/*! Fill p with the reference defaults listed above (precision = SPHB_FP64). */
+void sphb_default_params(sphb_params* p);
+
+/*! Library version string. */
+const char* sphb_version(void);
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* 1. Kernel entry points on caller-owned device arrays                                                             */
+/* ---------------------------------------------------------------------------------------------------------------- */
+
+/*! Hilbert SFC keys of n particles; keys equal to the removal key (1<<63) are kept as they are.
+ *  Replaces cstone::computeSfcKeysGpu (domain/include/cstone/sfc/sfc_gpu.cu:35-43; key math sfc.hpp:141-178,
+ *  hilbert.hpp:43-94). */
+int sphb_compute_sfc_keys(const double* x, const double* y, const double* z, uint64_t* keys, size_t n,
+                          const sphb_box* box, void* stream);
+
+/*! Scratch bytes needed by sphb_sort_by_key for n elements.
+ *  Replaces cstone::sortByKeyTempStorage (domain/include/cstone/primitives/primitives_gpu.cu:297-306). */
+size_t sphb_sort_by_key_scratch_bytes(size_t n);
+
+/*! Stable ascending sort of n (uint64 key, uint32 value) pairs in place, using caller scratch of at least
+ *  sphb_sort_by_key_scratch_bytes(n) bytes. If init_values != 0, values are first set to 0..n-1 (the sequence +
+ *  sort of GlobalAssignment::assign, domain/include/cstone/domain/assignment.hpp:110-112).
+ *  Replaces cstone::sortByKeyGpu (domain/include/cstone/primitives/primitives_gpu.cu:308-339). */
+int sphb_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* scratch, size_t scratch_bytes,
+                     void* stream);
+
+/*! dst_f[i] = src_f[order[i]] for num_fields arrays of 8-byte elements (double or uint64).
+ *  Replaces cstone::gatherGpu (domain/include/cstone/primitives/primitives_gpu.cu:73-88) applied per field by
+ *  Domain::updateLayout (domain/include/cstone/domain/domain.hpp:491-537). */
+int sphb_gather8(const uint32_t* order, size_t n, int num_fields, const void* const* src, void* const* dst,
+                 void* stream);
+
+/*! Fully converged cornerstone leaf array for sorted keys (host-blocking: loops until no node splits or merges).
+ *  Writes num_leaves + 1 keys to leaves and num_leaves counts, if num_leaves + 1 <= capacity.
+ *  Replaces cstone::computeOctree / updateOctree (domain/include/cstone/tree/csarray.hpp:409-440) and their GPU
+ *  counterparts computeNodeCountsGpu / rebalanceTreeGpu (csarray_gpu.cu:85-213). */
+int sphb_compute_octree(const uint64_t* sorted_keys, size_t n, unsigned bucket, uint64_t* leaves, uint32_t* counts,
+                        size_t capacity, size_t* num_leaves, void* stream);
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* 2. Simulation object: the whole hydro step of HydroVeProp                                                        */
+/* ---------------------------------------------------------------------------------------------------------------- */
+typedef struct sphb_sim sphb_sim;
+
+/*! Create a simulation of n particles on the current CUDA device; allocates every field in HBM.
+ *  Mirrors Domain(rank 0 of 1, bucketSize = max(64, n/100), bucketSizeFocus, theta 1) + ParticlesData
+ *  (main/src/sphexa/sphexa.cpp:129-138). */
+int sphb_sim_create(sphb_sim** sim, size_t n, const sphb_box* box, const sphb_params* params);
+int sphb_sim_destroy(sphb_sim* sim);
+
+/*! Copy the conserved fields in. fields holds 14 arrays of n doubles in the order
+ *  x,y,z,h,m,temp,vx,vy,vz,x_m1,y_m1,z_m1,du_m1,alpha; id holds n uint64. on_device != 0: the pointers are device
+ *  memory, else host memory (pinned or pageable). Resets the step state (first-call tree convergence). */
+int sphb_sim_upload(sphb_sim* sim, const double* const* fields, const uint64_t* id, int on_device);
+
+/*! The sync that the reference main program performs once before the first step (sphexa.cpp:141). */
+int sphb_sim_initial_sync(sphb_sim* sim);
+
+/*! First half of a step: HydroVeProp::computeForces (ve_hydro.hpp:126-203): domain sync (keys, sort, global and
+ *  focus cornerstone trees, gather), neighbour search with smoothing-length iteration, XMass, VeDefGradh, EOS,
+ *  IAD + divv/curlv, rho time step, AV switches, momentum-energy with Courant time step; then the conserved
+ *  quantities (main/src/observables/conserved_quantities.hpp:117-175). */
+int sphb_sim_compute_forces(sphb_sim* sim);
+
+/*! Second half: computeTimestep, computePositions, updateSmoothingLength (ve_hydro.hpp:205-220).
+ *  Returns SPHB_ERR_NOT_CONVERGED if any particle ended with nc <= 1 (its key is set to the removal key). */
+int sphb_sim_integrate(sphb_sim* sim);
+
+/*! compute_forces + integrate. */
+int sphb_sim_step(sphb_sim* sim);
+
+/*! Number of owned particles. */
+size_t sphb_sim_size(const sphb_sim* sim);
+
+/*! Copy a field, by its reference name (particles_data.hpp:262-266: x y z h m temp vx vy vz x_m1 y_m1 z_m1 du_m1
+ *  alpha xm kx gradh prho c c11 c12 c13 c22 c23 c33 divv curlv ax ay az du nc keys id), converted to double, into
+ *  out (n doubles; host memory if on_device == 0, else device memory). keys and id are copied as uint64 bits. */
+int sphb_sim_get_field(sphb_sim* sim, const char* name, double* out, int on_device);
+
+/*! Overwrite a field by name from n doubles (host memory if on_device == 0). */
+int sphb_sim_set_field(sphb_sim* sim, const char* name, const double* in, int on_device);
+
+/*! Scalars: minDt, minDt_m1, minDtCourant, minDtRho, ttot, etot, ecin, eint, linmom, angmom, totalNeighbors,
+ *  iteration, box xmin, xmax, ymin, ymax, zmin, zmax (18 doubles). */
+int sphb_sim_scalars(sphb_sim* sim, double* out);
+
+/*! Focus-tree leaves (num_leaves + 1 keys), leaf counts and particle layout (num_leaves + 1), host memory.
+ *  With null arrays only *num_leaves is written. */
+int sphb_sim_tree(sphb_sim* sim, size_t* num_leaves, uint64_t* leaves, uint32_t* counts, uint32_t* layout);
+
+/*! Neighbour lists of the last force computation as [n][ngmax] uint32 (host memory), entries beyond
+ *  min(nc-1, ngmax) undefined. */
+int sphb_sim_neighbors(sphb_sim* sim, uint32_t* out);
+
+/*! Per-stage device time of the last step in milliseconds (CUDA events): sync, neighbours, xmass, ve_def_gradh,
+ *  eos, iad_divv_curlv, av_switches, momentum_energy, integrate (9 floats). */
+int sphb_sim_stage_times(sphb_sim* sim, float* out);
+
+/*! Number of kernels this library launched since the simulation was created (for launch accounting). */
+uint64_t sphb_sim_kernel_launches(const sphb_sim* sim);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPHB200_H */

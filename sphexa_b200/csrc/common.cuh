@@ -1,0 +1,81 @@
+// Shared device/host helpers of the sm_100a hydro library.
+#pragma once
+
+#include <algorithm>
+#include <cstdint>
+#include <cstdio>
+#include <utility>
+#include <cuda_runtime.h>
+
+#include "../../include/sphb200.h"
+
+namespace sphb
+{
+
+//! Hilbert keys: 21 bits per dimension, 63 bits in total (cstone/tree/definitions.h:45-75)
+constexpr unsigned kMaxLevel  = 21;
+constexpr uint64_t kRootRange = uint64_t(1) << 63;
+//! the key that flags a particle for removal; it sorts after every valid key (definitions.h:70-75)
+constexpr uint64_t kRemoveKey = uint64_t(1) << 63;
+constexpr int kTableSize      = 20000;
+constexpr int kWarp           = 32;
+
+//! status codes shared with the C ABI
+enum Status : int
+{
+    kOk            = SPHB_OK,
+    kErrArg        = SPHB_ERR_ARG,
+    kErrCuda       = SPHB_ERR_CUDA,
+    kErrCapacity   = SPHB_ERR_CAPACITY,
+    kErrNotConverged = SPHB_ERR_NOT_CONVERGED,
+};
+
+#define SPHB_CUDA_TRY(expr)                                                                                            \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t err_ = (expr);                                                                                     \
+        if (err_ != cudaSuccess)                                                                                       \
+        {                                                                                                              \
+            std::fprintf(stderr, "sphb200: %s failed at %s:%d: %s\n", #expr, __FILE__, __LINE__,                      \
+                         cudaGetErrorString(err_));                                                                    \
+            return SPHB_ERR_CUDA;                                                                                      \
+        }                                                                                                              \
+    } while (0)
+
+#define SPHB_TRY(expr)                                                                                                 \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        int st_ = (expr);                                                                                              \
+        if (st_ != SPHB_OK) { return st_; }                                                                            \
+    } while (0)
+
+//! Coordinate box with inverse lengths and per-axis periodicity (cstone/sfc/box.hpp:94-174)
+struct DevBox
+{
+    double lo[3];
+    double hi[3];
+    double len[3];
+    double ilen[3];
+    int periodic[3];
+};
+
+inline DevBox makeDevBox(const sphb_box& b)
+{
+    DevBox d;
+    for (int k = 0; k < 3; ++k)
+    {
+        d.lo[k]       = b.lo[k];
+        d.hi[k]       = b.hi[k];
+        d.len[k]      = b.hi[k] - b.lo[k];
+        d.ilen[k]     = 1.0 / (b.hi[k] - b.lo[k]);
+        d.periodic[k] = b.periodic[k] ? 1 : 0;
+    }
+    return d;
+}
+
+inline unsigned ceilDiv(size_t a, unsigned b) { return unsigned((a + b - 1) / b); }
+
+//! number of SMs of the current device, cached per process
+int smCount();
+
+} // namespace sphb

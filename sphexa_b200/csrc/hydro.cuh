@@ -1,0 +1,109 @@
+// Device helpers and launch interface of the SPH-VE chain (see hydro_ve.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace sphb
+{
+
+//! physics constants of one simulation, in the J-loop type T
+template<class T>
+struct HydroConsts
+{
+    T K;           // kernel normalisation
+    T alphamin, alphamax, decay;
+    T Atmin, Atmax, ramp;
+    double Kcour;  // stored as the float the reference passes to tsKCourant (sph/include/sph/kernels.hpp:10-17)
+    double gamma, cv;
+    unsigned ngmax;
+};
+
+/*! Per-particle neighbour-side records, written by the stage that produces the values and gathered once per
+ *  neighbour by the next stages (one 16-byte-aligned record instead of one scattered load per field).
+ *  pos:   x, y, z, m            (double, every stage)
+ *  hydro: vx, vy, vz, h, xm, kx, c, prho   (T; written by VeDefGradh+EOS)
+ *  grad:  c11, c12, c13, c22, c23, c33, divv, alpha   (T; c_ij and divv by IAD, alpha by the AV switches) */
+template<class T>
+struct alignas(8 * sizeof(T)) HydroRec
+{
+    T vx, vy, vz, h, xm, kx, c, prho;
+};
+
+template<class T>
+struct alignas(8 * sizeof(T)) GradRec
+{
+    T c11, c12, c13, c22, c23, c33, divv, alpha;
+};
+
+//! device arrays of one simulation used by the chain; derived fields are stored in T
+template<class T>
+struct ChainArrays
+{
+    size_t n;
+    const double4* pos;       // x, y, z, m
+    const double* h;          // smoothing length (FP64 state)
+    const double* vx;
+    const double* vy;
+    const double* vz;
+    const double* temp;
+    double* alpha;            // AV coefficient (FP64 state)
+    const uint32_t* nidx;
+    const unsigned* nc;
+    const T* wh;
+    const T* whd;
+    T* xm;
+    T* kx;
+    T* gradh;
+    T* prho;
+    T* c;
+    T* cij[6];
+    T* divv;
+    T* curlv;
+    T* ax;
+    T* ay;
+    T* az;
+    double* du;
+    HydroRec<T>* hrec;
+    GradRec<T>* grec;
+    // reduction outputs: [0] max divv (ordered bits), [1] min Courant dt (ordered bits)
+    unsigned long long* reduce;
+};
+
+template<class T>
+int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
+template<class T>
+int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
+template<class T>
+int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
+template<class T>
+int launchAVswitches(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, double dt,
+                     cudaStream_t s);
+template<class T>
+int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
+
+//! order-preserving bit patterns of doubles for atomic min/max
+__host__ __device__ inline unsigned long long orderedBits(double v)
+{
+#ifdef __CUDA_ARCH__
+    long long b = __double_as_longlong(v);
+#else
+    long long b;
+    static_assert(sizeof(b) == sizeof(v));
+    __builtin_memcpy(&b, &v, sizeof(b));
+#endif
+    return b >= 0 ? (unsigned long long)(b) ^ 0x8000000000000000ull : ~(unsigned long long)(b);
+}
+
+__host__ __device__ inline double fromOrderedBits(unsigned long long u)
+{
+    unsigned long long b = (u & 0x8000000000000000ull) ? (u ^ 0x8000000000000000ull) : ~u;
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double((long long)b);
+#else
+    double v;
+    __builtin_memcpy(&v, &b, sizeof(v));
+    return v;
+#endif
+}
+
+} // namespace sphb

@@ -1,0 +1,673 @@
+// SPH-VE kernel chain on sm_100a: XMass, VeDefGradh (+ ideal-gas EOS), IAD + divv/curlv, AV switches,
+// momentum-energy. One thread per target particle; a warp is a group of 32 consecutive SFC-ordered particles whose
+// neighbour lists are read slot-major (one coalesced line per slot). Each J-loop walks the list in stored (ascending)
+// order, like the reference CPU loops, and reads neighbour data through the packed records of hydro.cuh.
+//
+// T = double: plain FP64 drop-in. T = float: the mixed form — pair geometry is formed in FP64 (x_i - x_j with the
+// periodic shift) and then rounded to FP32, all pair arithmetic is FP32, and every neighbour sum is a compensated
+// (Kahan) FP32 sum.
+//
+// Per-pair formulas follow the reference J-loops cited at each kernel; the order of operations inside each
+// expression is kept, so FP64 results differ from the reference CPU only by FMA contraction.
+#include "hydro.cuh"
+#include "neighbors.cuh"
+#include "primitives.cuh"
+
+namespace sphb
+{
+
+namespace
+{
+
+constexpr int kChainThreads = 128;
+
+template<class T>
+struct Sum;
+
+template<>
+struct Sum<double>
+{
+    double s;
+    __device__ explicit Sum(double v = 0.0)
+        : s(v)
+    {
+    }
+    __device__ void add(double v) { s += v; }
+    __device__ double get() const { return s; }
+};
+
+//! Kahan-compensated FP32 sum; explicit round-to-nearest intrinsics keep the compiler from fusing or reordering
+template<>
+struct Sum<float>
+{
+    float s, comp;
+    __device__ explicit Sum(float v = 0.f)
+        : s(v)
+        , comp(0.f)
+    {
+    }
+    __device__ void add(float v)
+    {
+        float y = __fsub_rn(v, comp);
+        float t = __fadd_rn(s, y);
+        comp    = __fsub_rn(__fsub_rn(t, s), y);
+        s       = t;
+    }
+    __device__ float get() const { return s; }
+};
+
+//! linear interpolation in a 20000-entry table on [0, 2] (sph/include/sph/table_lookup.hpp:14-26)
+template<class T>
+__device__ __forceinline__ T tableLookup(const T* __restrict__ table, T v)
+{
+    constexpr int numIntervals = kTableSize - 1;
+    constexpr T dx             = T(2.0) / numIntervals;
+    constexpr T invDx          = T(1) / dx;
+    int idx                    = int(v * invDx);
+    if (idx >= numIntervals) { return T(0); }
+    T t0 = __ldg(table + idx);
+    T t1 = __ldg(table + idx + 1);
+    T derivative = (t1 - t0) * invDx;
+    return t0 + derivative * (v - T(idx) * dx);
+}
+
+//! periodic shift of a pair separation by one box length if it exceeds r (cstone/sfc/box.hpp applyPBC, legacy form)
+__device__ __forceinline__ void shiftPbc(double& rx, double& ry, double& rz, double r, const DevBox& box)
+{
+    if (box.periodic[0])
+    {
+        if (rx > r) { rx -= box.len[0]; }
+        else if (rx < -r) { rx += box.len[0]; }
+    }
+    if (box.periodic[1])
+    {
+        if (ry > r) { ry -= box.len[1]; }
+        else if (ry < -r) { ry += box.len[1]; }
+    }
+    if (box.periodic[2])
+    {
+        if (rz > r) { rz -= box.len[2]; }
+        else if (rz < -r) { rz += box.len[2]; }
+    }
+}
+
+//! 32-byte read-only load as two 16-byte vector loads (one sector)
+__device__ __forceinline__ double4 ldg4(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 lo = __ldg(q), hi = __ldg(q + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
+template<class T>
+__device__ __forceinline__ HydroRec<T> loadHydro(const HydroRec<T>* p)
+{
+    HydroRec<T> r;
+    if constexpr (sizeof(T) == 8)
+    {
+        const double4* q = reinterpret_cast<const double4*>(p);
+        double4 a = ldg4(q), b = ldg4(q + 1);
+        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
+    }
+    else
+    {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        float4 a = __ldg(q), b = __ldg(q + 1);
+        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
+    }
+    return r;
+}
+
+template<class T>
+__device__ __forceinline__ GradRec<T> loadGrad(const GradRec<T>* p)
+{
+    GradRec<T> r;
+    if constexpr (sizeof(T) == 8)
+    {
+        const double4* q = reinterpret_cast<const double4*>(p);
+        double4 a = ldg4(q), b = ldg4(q + 1);
+        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
+    }
+    else
+    {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        float4 a = __ldg(q), b = __ldg(q + 1);
+        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
+    }
+    return r;
+}
+
+struct Target
+{
+    size_t i;
+    size_t group;
+    unsigned lane;
+    unsigned count;
+};
+
+__device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned ngmax, Target& t)
+{
+    t.i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (t.i >= n) { return false; }
+    t.group = t.i >> 5;
+    t.lane  = unsigned(t.i & 31);
+    t.count = min(nc[t.i] - 1u, ngmax);
+    return true;
+}
+
+__device__ __forceinline__ uint32_t neighborAt(const uint32_t* nidx, const Target& t, unsigned ngmax, unsigned k)
+{
+    return __ldg(nidx + nidxSlot(t.group, ngmax, k, t.lane));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// XMass: rho0_i = (m_i + sum_j W_ij m_j) K / h_i^3, xm_i = m_i / rho0_i (sph/include/sph/hydro_ve/xmass_kern.hpp:50-79)
+// ---------------------------------------------------------------------------------------------------------------
+template<class T>
+__global__ void __launch_bounds__(kChainThreads) xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+{
+    Target t;
+    if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
+    double4 pi = a.pos[t.i];
+    double hiD = a.h[t.i];
+    T hi       = T(hiD);
+    T mi       = T(pi.w);
+    T hInv     = T(1.0) / hi;
+    T h3Inv    = hInv * hInv * hInv;
+
+    Sum<T> rho0(mi);
+#pragma unroll 4
+    for (unsigned q = 0; q < t.count; ++q)
+    {
+        uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
+        double4 pj = ldg4(a.pos + j);
+        double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+        shiftPbc(rx, ry, rz, 2.0 * hiD, box);
+        T fx = T(rx), fy = T(ry), fz = T(rz);
+        T dist = sqrt(fx * fx + fy * fy + fz * fz);
+        T w    = tableLookup(a.wh, dist * hInv);
+        rho0.add(w * T(pj.w));
+    }
+    a.xm[t.i] = mi / (rho0.get() * k.K * h3Inv);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// VeDefGradh (sph/include/sph/hydro_ve/ve_def_gradh_kern.hpp:43-90) + ideal-gas EOS (hydro_ve/eos.hpp:52-94,
+// sph/include/sph/eos.hpp:19-50); writes kx, gradh, prho, c and the hydro record of the particle.
+// ---------------------------------------------------------------------------------------------------------------
+template<class T>
+__global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+{
+    Target t;
+    if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
+    double4 pi  = a.pos[t.i];
+    double hiD  = a.h[t.i];
+    T hi        = T(hiD);
+    T mi        = T(pi.w);
+    T xmassi    = a.xm[t.i];
+    T hInv      = T(1) / hi;
+    T h3Inv     = hInv * hInv * hInv;
+
+    Sum<T> kxS(xmassi), whomegaS(-T(3) * xmassi), wrho0S(-T(3) * mi);
+#pragma unroll 4
+    for (unsigned q = 0; q < t.count; ++q)
+    {
+        uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
+        double4 pj = ldg4(a.pos + j);
+        double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+        shiftPbc(rx, ry, rz, 2.0 * hiD, box);
+        T fx = T(rx), fy = T(ry), fz = T(rz);
+        T dist   = sqrt(fx * fx + fy * fy + fz * fz);
+        T vloc   = dist * hInv;
+        T w      = tableLookup(a.wh, vloc);
+        T dw     = tableLookup(a.whd, vloc);
+        T dterh  = -(T(3) * w + vloc * dw);
+        T xmassj = __ldg(a.xm + j);
+        kxS.add(w * xmassj);
+        whomegaS.add(dterh * xmassj);
+        wrho0S.add(dterh * T(pj.w));
+    }
+    T kxi      = kxS.get() * (k.K * h3Inv);
+    T whomegai = whomegaS.get() * (k.K * h3Inv * hInv);
+    T wrho0i   = wrho0S.get() * (k.K * h3Inv * hInv);
+    whomegai   = whomegai * mi / xmassi + (kxi - k.K * xmassi * h3Inv) * wrho0i;
+    T rhoi     = kxi * mi / xmassi;
+    T dhdrho   = -hi / (rhoi * T(3));
+    T gradhi   = T(1) - dhdrho * whomegai;
+
+    // EOS in FP64 (per particle): rho = kx m / xm, p = rho u (gamma - 1), c = sqrt(gamma u (gamma - 1))
+    double rho  = double(kxi) * double(mi) / double(xmassi);
+    double u    = k.cv * a.temp[t.i];
+    double tmp  = u * (k.gamma - 1.0);
+    double p    = rho * tmp;
+    double c    = sqrt(k.gamma * tmp);
+    double prho = p / (double(kxi) * double(mi) * double(mi) * double(gradhi));
+
+    a.kx[t.i]    = kxi;
+    a.gradh[t.i] = gradhi;
+    a.prho[t.i]  = T(prho);
+    a.c[t.i]     = T(c);
+    a.hrec[t.i]  = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), hi, xmassi, kxi, T(c), T(prho)};
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// IAD (sph/include/sph/hydro_ve/iad_kern.hpp:43-110) then divv/curlv with the particle's own c_ij
+// (sph/include/sph/hydro_ve/divv_curlv_kern.hpp:43-123); also the running max of divv for the rho time step.
+// ---------------------------------------------------------------------------------------------------------------
+template<class T>
+__device__ __forceinline__ int expOf(T v)
+{
+    return v == T(0) ? 0 : ilogb(v);
+}
+
+template<class T>
+__global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+{
+    Target t;
+    bool valid = targetOf(a.n, a.nc, k.ngmax, t);
+    double divvOut = -INFINITY;
+    if (valid)
+    {
+        double4 pi = a.pos[t.i];
+        double hiD = a.h[t.i];
+        T hi       = T(hiD);
+        T hiInv    = T(1) / hi;
+
+        Sum<T> s11, s12, s13, s22, s23, s33;
+#pragma unroll 4
+        for (unsigned q = 0; q < t.count; ++q)
+        {
+            uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
+            double4 pj = ldg4(a.pos + j);
+            HydroRec<T> hj = loadHydro(a.hrec + j);
+            double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
+            shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
+            T rx = T(rxD), ry = T(ryD), rz = T(rzD);
+            T dist   = sqrt(rx * rx + ry * ry + rz * rz);
+            T w      = tableLookup(a.wh, dist * hiInv);
+            T voljW  = hj.xm / hj.kx * w;
+            s11.add(rx * rx * voljW);
+            s12.add(rx * ry * voljW);
+            s13.add(rx * rz * voljW);
+            s22.add(ry * ry * voljW);
+            s23.add(ry * rz * voljW);
+            s33.add(rz * rz * voljW);
+        }
+        T tau11 = s11.get(), tau12 = s12.get(), tau13 = s13.get();
+        T tau22 = s22.get(), tau23 = s23.get(), tau33 = s33.get();
+        int expSum = expOf(tau11) + expOf(tau12) + expOf(tau13) + expOf(tau22) + expOf(tau23) + expOf(tau33);
+        T norm     = ldexp(T(1), -expSum / 6);
+        tau11 *= norm;
+        tau12 *= norm;
+        tau13 *= norm;
+        tau22 *= norm;
+        tau23 *= norm;
+        tau33 *= norm;
+        T det = tau11 * tau22 * tau33 + T(2) * tau12 * tau23 * tau13 - tau11 * tau23 * tau23 - tau22 * tau13 * tau13 -
+                tau33 * tau12 * tau12;
+        T factor = norm * (hi * hi * hi) / (det * k.K);
+        if (isnan(factor) && t.count == 0) { factor = T(0); }
+        T c11i = (tau22 * tau33 - tau23 * tau23) * factor;
+        T c12i = (tau13 * tau23 - tau33 * tau12) * factor;
+        T c13i = (tau12 * tau23 - tau22 * tau13) * factor;
+        T c22i = (tau11 * tau33 - tau13 * tau13) * factor;
+        T c23i = (tau13 * tau12 - tau11 * tau23) * factor;
+        T c33i = (tau11 * tau22 - tau12 * tau12) * factor;
+
+        HydroRec<T> hrI = a.hrec[t.i];
+        T vxi = hrI.vx, vyi = hrI.vy, vzi = hrI.vz;
+        T kxi = hrI.kx;
+        Sum<T> dVxx, dVxy, dVxz, dVyx, dVyy, dVyz, dVzx, dVzy, dVzz;
+#pragma unroll 4
+        for (unsigned q = 0; q < t.count; ++q)
+        {
+            uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
+            double4 pj = ldg4(a.pos + j);
+            HydroRec<T> hj = loadHydro(a.hrec + j);
+            double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
+            shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
+            T rx = T(rxD), ry = T(ryD), rz = T(rzD);
+            T r2    = rx * rx + ry * ry + rz * rz;
+            T dist  = sqrt(r2);
+            T vxji  = hj.vx - vxi;
+            T vyji  = hj.vy - vyi;
+            T vzji  = hj.vz - vzi;
+            T Wi    = tableLookup(a.wh, dist * hiInv);
+            T tA0   = -(c11i * rx + c12i * ry + c13i * rz) * Wi;
+            T tA1   = -(c12i * rx + c22i * ry + c23i * rz) * Wi;
+            T tA2   = -(c13i * rx + c23i * ry + c33i * rz) * Wi;
+            T fx    = vxji * hj.xm;
+            T fy    = vyji * hj.xm;
+            T fz    = vzji * hj.xm;
+            dVxx.add(fx * tA0);
+            dVxy.add(fx * tA1);
+            dVxz.add(fx * tA2);
+            dVyx.add(fy * tA0);
+            dVyy.add(fy * tA1);
+            dVyz.add(fy * tA2);
+            dVzx.add(fz * tA0);
+            dVzy.add(fz * tA1);
+            dVzz.add(fz * tA2);
+        }
+        T hiInv3  = hiInv * hiInv * hiInv;
+        T normKx  = k.K * hiInv3 / kxi;
+        T divv    = normKx * (dVxx.get() + dVyy.get() + dVzz.get());
+        T cx      = dVzy.get() - dVyz.get();
+        T cy      = dVxz.get() - dVzx.get();
+        T cz      = dVyx.get() - dVxy.get();
+        T curlv   = normKx * sqrt(cx * cx + cy * cy + cz * cz);
+
+        a.cij[0][t.i] = c11i;
+        a.cij[1][t.i] = c12i;
+        a.cij[2][t.i] = c13i;
+        a.cij[3][t.i] = c22i;
+        a.cij[4][t.i] = c23i;
+        a.cij[5][t.i] = c33i;
+        a.divv[t.i]   = divv;
+        a.curlv[t.i]  = curlv;
+        a.grec[t.i]   = GradRec<T>{c11i, c12i, c13i, c22i, c23i, c33i, divv, T(a.alpha[t.i])};
+        divvOut       = double(divv);
+    }
+    // block max of divv -> one atomic per block
+    double v = divvOut;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+    }
+    __shared__ double warpMax[kChainThreads / 32];
+    if ((threadIdx.x & 31) == 0) { warpMax[threadIdx.x >> 5] = v; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double m = warpMax[0];
+        for (int w = 1; w < kChainThreads / 32; ++w)
+        {
+            m = fmax(m, warpMax[w]);
+        }
+        atomicMax(a.reduce + 0, orderedBits(m));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// AV switches (sph/include/sph/hydro_ve/av_switches_kern.hpp:43-137)
+// ---------------------------------------------------------------------------------------------------------------
+template<class T>
+__global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box,
+                                                                  double dt)
+{
+    Target t;
+    if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
+    double4 pi     = a.pos[t.i];
+    double hiD     = a.h[t.i];
+    HydroRec<T> hr = a.hrec[t.i];
+    GradRec<T> gr  = a.grec[t.i];
+    T hi           = T(hiD);
+    T ci           = hr.c;
+    T vijsignalI   = T(1.e-40) * ci;
+    T hiInv        = T(1) / hi;
+    T hiInv3       = hiInv * hiInv * hiInv;
+    T divvI        = gr.divv;
+
+    Sum<T> gx, gy, gz;
+#pragma unroll 4
+    for (unsigned q = 0; q < t.count; ++q)
+    {
+        uint32_t j     = neighborAt(a.nidx, t, k.ngmax, q);
+        double4 pj     = ldg4(a.pos + j);
+        HydroRec<T> hj = loadHydro(a.hrec + j);
+        GradRec<T> gj  = loadGrad(a.grec + j);
+        double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
+        shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
+        T rx = T(rxD), ry = T(ryD), rz = T(rzD);
+        T r2   = rx * rx + ry * ry + rz * rz;
+        T dist = sqrt(r2);
+        T vxij = hr.vx - hj.vx;
+        T vyij = hr.vy - hj.vy;
+        T vzij = hr.vz - hj.vz;
+        T rv   = rx * vxij + ry * vyij + rz * vzij;
+        T vsig = T(0);
+        if (rv < T(0)) { vsig = ci + hj.c - T(3) * rv / dist; }
+        vijsignalI = vijsignalI > vsig ? vijsignalI : vsig;
+        T Wi   = k.K * hiInv3 * tableLookup(a.wh, dist * hiInv);
+        T tA1  = -(gr.c11 * rx + gr.c12 * ry + gr.c13 * rz) * Wi;
+        T tA2  = -(gr.c12 * rx + gr.c22 * ry + gr.c23 * rz) * Wi;
+        T tA3  = -(gr.c13 * rx + gr.c23 * ry + gr.c33 * rz) * Wi;
+        T volj = hj.xm / hj.kx;
+        T fac  = volj * (divvI - gj.divv);
+        gx.add(fac * tA1);
+        gy.add(fac * tA2);
+        gz.add(fac * tA3);
+    }
+    T gdx      = gx.get(), gdy = gy.get(), gdz = gz.get();
+    T graddivv = sqrt(gdx * gdx + gdy * gdy + gdz * gdz);
+    T alphaI   = T(a.alpha[t.i]);
+    T alphaloc = T(0);
+    if (divvI < T(0))
+    {
+        T aConst = hi * hi * graddivv;
+        alphaloc = k.alphamax * aConst / (aConst + hi * fabs(divvI) + T(0.05) * ci);
+    }
+    if (alphaloc >= alphaI) { alphaI = alphaloc; }
+    else
+    {
+        T decay    = hi / (k.decay * vijsignalI);
+        T alphadot = alphaloc >= k.alphamin ? (alphaloc - alphaI) / decay : (k.alphamin - alphaI) / decay;
+        alphaI += alphadot * T(dt);
+    }
+    a.alpha[t.i]      = double(alphaI);
+    a.grec[t.i].alpha = alphaI; // the alpha slot of the record is not read by this kernel
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Momentum and energy (sph/include/sph/hydro_ve/momentum_energy_kern.hpp:65-222, avClean = false;
+// artificial_viscosity sph/include/sph/kernels.hpp:71-85) with the Courant time step per particle
+// (tsKCourant, kernels.hpp:10-17) reduced to the minimum.
+// ---------------------------------------------------------------------------------------------------------------
+template<class T>
+__device__ __forceinline__ T powT(T b, T e)
+{
+    return pow(b, e);
+}
+
+template<class T>
+__global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+{
+    Target t;
+    bool valid   = targetOf(a.n, a.nc, k.ngmax, t);
+    double dtMin = INFINITY;
+    if (valid)
+    {
+        double4 pi     = a.pos[t.i];
+        double hiD     = a.h[t.i];
+        HydroRec<T> hr = a.hrec[t.i];
+        GradRec<T> gr  = a.grec[t.i];
+        T hi      = T(hiD);
+        T mi      = T(pi.w);
+        T ci      = hr.c;
+        T kxi     = hr.kx;
+        T alphaI  = gr.alpha;
+        T xmassi  = hr.xm;
+        T rhoi    = kxi * mi / xmassi;
+        T prhoi   = hr.prho;
+        T hiInv   = T(1) / hi;
+        T hiInv3  = hiInv * hiInv * hiInv;
+        T maxvsignalI = T(0);
+        Sum<T> momX, momY, momZ, energyS, aViscE;
+
+#pragma unroll 2
+        for (unsigned q = 0; q < t.count; ++q)
+        {
+            uint32_t j     = neighborAt(a.nidx, t, k.ngmax, q);
+            double4 pj     = ldg4(a.pos + j);
+            HydroRec<T> hj = loadHydro(a.hrec + j);
+            GradRec<T> gj  = loadGrad(a.grec + j);
+            double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
+            shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
+            T rx = T(rxD), ry = T(ryD), rz = T(rzD);
+            T r2    = rx * rx + ry * ry + rz * rz;
+            T dist  = sqrt(r2);
+            T vxij  = hr.vx - hj.vx;
+            T vyij  = hr.vy - hj.vy;
+            T vzij  = hr.vz - hj.vz;
+            T hjInv = T(1) / hj.h;
+            T v1    = dist * hiInv;
+            T v2    = dist * hjInv;
+            T hjInv3 = hjInv * hjInv * hjInv;
+            T Wi    = hiInv3 * tableLookup(a.wh, v1);
+            T Wj    = hjInv3 * tableLookup(a.wh, v2);
+
+            T tA1i = -(gr.c11 * rx + gr.c12 * ry + gr.c13 * rz) * Wi;
+            T tA2i = -(gr.c12 * rx + gr.c22 * ry + gr.c23 * rz) * Wi;
+            T tA3i = -(gr.c13 * rx + gr.c23 * ry + gr.c33 * rz) * Wi;
+            T tA1j = -(gj.c11 * rx + gj.c12 * ry + gj.c13 * rz) * Wj;
+            T tA2j = -(gj.c12 * rx + gj.c22 * ry + gj.c23 * rz) * Wj;
+            T tA3j = -(gj.c13 * rx + gj.c23 * ry + gj.c33 * rz) * Wj;
+
+            T mj     = T(pj.w);
+            T cj     = hj.c;
+            T xmassj = hj.xm;
+            T rhoj   = hj.kx * mj / xmassj;
+
+            T rv  = rx * vxij + ry * vyij + rz * vzij;
+            T wij = rv / dist;
+            T visc = T(0);
+            if (wij < T(0))
+            {
+                T vijSignal = (alphaI + gj.alpha) * T(0.25) * (ci + cj) - T(2) * wij;
+                visc        = -vijSignal * wij;
+            }
+            T vijsignal  = T(0.5) * (ci + cj) - T(2) * wij;
+            maxvsignalI  = vijsignal > maxvsignalI ? vijsignal : maxvsignalI;
+
+            T aMom, bMom;
+            T atwood = fabs(rhoi - rhoj) / (rhoi + rhoj);
+            if (atwood < k.Atmin)
+            {
+                aMom = xmassi * xmassi;
+                bMom = xmassj * xmassj;
+            }
+            else if (atwood > k.Atmax)
+            {
+                aMom = xmassi * xmassj;
+                bMom = aMom;
+            }
+            else
+            {
+                T sigma = k.ramp * (atwood - k.Atmin);
+                aMom    = powT(xmassi, T(2) - sigma) * powT(xmassj, sigma);
+                bMom    = powT(xmassj, T(2) - sigma) * powT(xmassi, sigma);
+            }
+
+            T aVisc  = mj / rhoi * visc;
+            T bVisc  = mj / rhoj * visc;
+            T aViscX = T(0.5) * (aVisc * tA1i + bVisc * tA1j);
+            T aViscY = T(0.5) * (aVisc * tA2i + bVisc * tA2j);
+            T aViscZ = T(0.5) * (aVisc * tA3i + bVisc * tA3j);
+            aViscE.add(aViscX * vxij + aViscY * vyij + aViscZ * vzij);
+            energyS.add(mj * aMom * (vxij * tA1i + vyij * tA2i + vzij * tA3i));
+            T momI = mj * prhoi * aMom;
+            T momJ = mj * hj.prho * bMom;
+            momX.add(momI * tA1i + momJ * tA1j + aViscX);
+            momY.add(momI * tA2i + momJ * tA2j + aViscY);
+            momZ.add(momI * tA3i + momJ * tA3j + aViscZ);
+        }
+        T aViscEnergy = aViscE.get() > T(0) ? aViscE.get() : T(0);
+        a.du[t.i] = double(k.K * (prhoi * energyS.get() + T(0.5) * aViscEnergy));
+        a.ax[t.i] = -k.K * momX.get();
+        a.ay[t.i] = -k.K * momY.get();
+        a.az[t.i] = -k.K * momZ.get();
+
+        double v = maxvsignalI > T(0) ? double(maxvsignalI) : double(ci);
+        dtMin    = hiD > 0.0 ? k.Kcour * hiD / v : INFINITY;
+    }
+    double m = dtMin;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
+    }
+    __shared__ double warpMin[kChainThreads / 32];
+    if ((threadIdx.x & 31) == 0) { warpMin[threadIdx.x >> 5] = m; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double b = warpMin[0];
+        for (int w = 1; w < kChainThreads / 32; ++w)
+        {
+            b = fmin(b, warpMin[w]);
+        }
+        atomicMin(a.reduce + 1, orderedBits(b));
+    }
+}
+
+template<class T>
+unsigned chainBlocks(const ChainArrays<T>& a)
+{
+    return ceilDiv(a.n, kChainThreads);
+}
+
+} // namespace
+
+template<class T>
+int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
+{
+    if (a.n == 0) { return kOk; }
+    xmassKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template<class T>
+int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
+{
+    if (a.n == 0) { return kOk; }
+    veDefGradhEosKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template<class T>
+int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
+{
+    if (a.n == 0) { return kOk; }
+    iadDivvCurlvKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template<class T>
+int launchAVswitches(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, double dt, cudaStream_t s)
+{
+    if (a.n == 0) { return kOk; }
+    avSwitchesKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box, dt);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template<class T>
+int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
+{
+    if (a.n == 0) { return kOk; }
+    momentumEnergyKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+#define SPHB_INSTANTIATE(T)                                                                                            \
+    template int launchXMass<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);          \
+    template int launchVeDefGradhEos<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);  \
+    template int launchIadDivvCurlv<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);   \
+    template int launchAVswitches<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, double,            \
+                                     cudaStream_t);                                                                  \
+    template int launchMomentumEnergy<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);
+
+SPHB_INSTANTIATE(double)
+SPHB_INSTANTIATE(float)
+
+} // namespace sphb

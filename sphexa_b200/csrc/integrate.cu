@@ -1,0 +1,221 @@
+// Per-particle FP64 kernels around the neighbour sums: position packing, kick-drift + energy integration,
+// smoothing-length update, coordinate min/max and the conservation reductions.
+#include "hydro.cuh"
+#include "integrate.cuh"
+#include "primitives.cuh"
+
+namespace sphb
+{
+
+namespace
+{
+
+__global__ void packPosKernel(const double* x, const double* y, const double* z, const double* m, size_t n,
+                              double4* pos)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i < n) { pos[i] = make_double4(x[i], y[i], z[i], m[i]); }
+}
+
+//! fold a coordinate back into a periodic box once (cstone/sfc/box.hpp putInBox)
+__device__ inline double putInBox(double v, int k, const DevBox& box)
+{
+    if (!box.periodic[k]) { return v; }
+    if (v > box.hi[k]) { return v - box.len[k]; }
+    if (v < box.lo[k]) { return v + box.len[k]; }
+    return v;
+}
+
+/*! Press kick-drift (sph/include/sph/positions.hpp:100-111) and the Adams-Bashforth energy update of temp
+ *  (positions.hpp:77-84,139-160), in FP64, with the operation order of the reference expressions. */
+template<class T>
+__global__ void positionsKernel(size_t n, IntegrateArrays<T> a, DevBox box, double dt, double dtm1, double cv)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    double X[3]  = {a.x[i], a.y[i], a.z[i]};
+    double A[3]  = {double(a.ax[i]), double(a.ay[i]), double(a.az[i])};
+    double dX[3] = {a.xm1[i], a.ym1[i], a.zm1[i]};
+    double* V[3] = {a.vx, a.vy, a.vz};
+    double* P[3] = {a.x, a.y, a.z};
+    double* M[3] = {a.xm1, a.ym1, a.zm1};
+    double invDtm1 = 1.0 / dtm1;
+    double adt     = fabs(dt);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        double vHalf = dX[k] * invDtm1;
+        double vn    = vHalf + (0.5 * dtm1) * A[k];
+        double vnp1  = vn + A[k] * dt;
+        double dXn1  = (vn + (0.5 * A[k]) * adt) * dt;
+        P[k][i]      = putInBox(X[k] + dXn1, k, box);
+        M[k][i]      = dXn1;
+        V[k][i]      = vnp1;
+    }
+    double uOld = cv * a.temp[i];
+    double du   = a.du[i];
+    double duM1 = a.duM1[i];
+    double uNew = uOld + du * dt + 0.5 * (du - duM1) / dtm1 * adt * dt;
+    if (uNew < 0.0) { uNew = uOld * exp(uNew * dt / uOld); }
+    a.temp[i] = uNew / cv;
+    a.duM1[i] = du;
+}
+
+/*! end-of-step smoothing length: h * 0.5 (1 + 1023 ng0/nc)^(1/10); nc <= 1 flags the particle for removal
+ *  (sph/include/sph/update_h.hpp:12-33) */
+__global__ void updateHKernel(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    unsigned c = nc[i];
+    if (c <= 1)
+    {
+        keys[i] = kRemoveKey;
+        atomicOr(flag, 1u);
+    }
+    double ratio = __ddiv_rn(__dmul_rn(1023.0, double(ng0)), double(c));
+    h[i]         = __dmul_rn(__dmul_rn(h[i], 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
+}
+
+constexpr int kRedThreads = 256;
+
+//! per-block partial sums of the conserved quantities: eKin, eInt, P(3), L(3), sum nc (9 doubles)
+__global__ void __launch_bounds__(kRedThreads) conservedPartialKernel(size_t n, const double* x, const double* y,
+                                                                      const double* z, const double* vx,
+                                                                      const double* vy, const double* vz,
+                                                                      const double* m, const double* temp,
+                                                                      const unsigned* nc, double cv, double* partial)
+{
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        double mi = m[i];
+        double X[3] = {x[i], y[i], z[i]};
+        double V[3] = {vx[i], vy[i], vz[i]};
+        acc[0] += mi * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+        acc[1] += cv * temp[i] * mi;
+        acc[2] += mi * V[0];
+        acc[3] += mi * V[1];
+        acc[4] += mi * V[2];
+        acc[5] += mi * (X[1] * V[2] - X[2] * V[1]);
+        acc[6] += mi * (X[2] * V[0] - X[0] * V[2]);
+        acc[7] += mi * (X[0] * V[1] - X[1] * V[0]);
+        acc[8] += double(nc[i]);
+    }
+    __shared__ double sh[kRedThreads / 32][9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q)
+    {
+        double v = acc[q];
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            v += __shfl_xor_sync(0xffffffffu, v, off);
+        }
+        if ((threadIdx.x & 31) == 0) { sh[threadIdx.x >> 5][q] = v; }
+    }
+    __syncthreads();
+    if (threadIdx.x < 9)
+    {
+        double s = 0;
+        for (int w = 0; w < kRedThreads / 32; ++w)
+        {
+            s += sh[w][threadIdx.x];
+        }
+        partial[blockIdx.x * 9 + threadIdx.x] = s;
+    }
+}
+
+__global__ void conservedFinalKernel(const double* partial, int numBlocks, double* out)
+{
+    int q = threadIdx.x;
+    if (q >= 9) { return; }
+    double s = 0;
+    for (int b = 0; b < numBlocks; ++b)
+    {
+        s += partial[b * 9 + q];
+    }
+    out[q] = s;
+}
+
+__global__ void minMaxKernel(const double* v, size_t n, unsigned long long* out)
+{
+    double lo = INFINITY, hi = -INFINITY;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        lo = fmin(lo, v[i]);
+        hi = fmax(hi, v[i]);
+    }
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, off));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, off));
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomicMin(out, orderedBits(lo));
+        atomicMax(out + 1, orderedBits(hi));
+    }
+}
+
+} // namespace
+
+int packPositions(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
+                  cudaStream_t s)
+{
+    if (n == 0) { return kOk; }
+    packPosKernel<<<ceilDiv(n, 256), 256, 0, s>>>(x, y, z, m, n, pos);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template<class T>
+int launchPositions(size_t n, const IntegrateArrays<T>& a, const DevBox& box, double dt, double dtm1, double cv,
+                    cudaStream_t s)
+{
+    if (n == 0) { return kOk; }
+    positionsKernel<T><<<ceilDiv(n, 256), 256, 0, s>>>(n, a, box, dt, dtm1, cv);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int launchUpdateH(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag,
+                  cudaStream_t s)
+{
+    if (n == 0) { return kOk; }
+    updateHKernel<<<ceilDiv(n, 256), 256, 0, s>>>(n, ng0, nc, h, keys, flag);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int conservedSums(size_t n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
+                  const double* vz, const double* m, const double* temp, const unsigned* nc, double cv,
+                  double* partial, int maxBlocks, double* out9, cudaStream_t s)
+{
+    int blocks = int(std::min<size_t>(std::max<size_t>(ceilDiv(n, kRedThreads), 1), size_t(maxBlocks)));
+    conservedPartialKernel<<<blocks, kRedThreads, 0, s>>>(n, x, y, z, vx, vy, vz, m, temp, nc, cv, partial);
+    conservedFinalKernel<<<1, 32, 0, s>>>(partial, blocks, out9);
+    countLaunch(2);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s)
+{
+    unsigned long long init[2] = {orderedBits(INFINITY), orderedBits(-INFINITY)};
+    SPHB_CUDA_TRY(cudaMemcpyAsync(out2, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    int blocks = int(std::min<size_t>(std::max<size_t>(ceilDiv(n, 256), 1), size_t(smCount()) * 4));
+    minMaxKernel<<<blocks, 256, 0, s>>>(v, n, out2);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template int launchPositions<double>(size_t, const IntegrateArrays<double>&, const DevBox&, double, double, double,
+                                     cudaStream_t);
+template int launchPositions<float>(size_t, const IntegrateArrays<float>&, const DevBox&, double, double, double,
+                                    cudaStream_t);
+
+} // namespace sphb

@@ -1,0 +1,39 @@
+// Per-particle FP64 kernels around the neighbour sums (see integrate.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace sphb
+{
+
+template<class T>
+struct IntegrateArrays
+{
+    double *x, *y, *z;
+    double *vx, *vy, *vz;
+    double *xm1, *ym1, *zm1;
+    double* temp;
+    double* duM1;
+    const double* du;
+    const T *ax, *ay, *az;
+};
+
+int packPositions(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
+                  cudaStream_t s);
+
+template<class T>
+int launchPositions(size_t n, const IntegrateArrays<T>& a, const DevBox& box, double dt, double dtm1, double cv,
+                    cudaStream_t s);
+
+int launchUpdateH(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag,
+                  cudaStream_t s);
+
+//! eKin (sum m v^2), eInt, linear momentum (3), angular momentum (3), sum nc -> out9 (device)
+int conservedSums(size_t n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
+                  const double* vz, const double* m, const double* temp, const unsigned* nc, double cv,
+                  double* partial, int maxBlocks, double* out9, cudaStream_t s);
+
+//! out2 = ordered bits of (min, max) of v
+int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s);
+
+} // namespace sphb

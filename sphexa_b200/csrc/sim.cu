@@ -1,0 +1,720 @@
+// The simulation object: particle dataset in HBM and the whole HydroVeProp step
+// (main/src/propagator/ve_hydro.hpp:126-220) at one rank, driven from the host.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "hydro.cuh"
+#include "integrate.cuh"
+#include "neighbors.cuh"
+#include "octree.cuh"
+#include "primitives.cuh"
+#include "sfc.cuh"
+#include "sort.cuh"
+#include "tables.hpp"
+
+namespace sphb
+{
+
+//! conserved fields, in the order of the upload ABI
+enum Field : int
+{
+    fX, fY, fZ, fH, fM, fTemp, fVx, fVy, fVz, fXm1, fYm1, fZm1, fDuM1, fAlpha, kNumConserved
+};
+static const char* const kConservedNames[kNumConserved] = {"x",  "y",    "z",    "h",    "m",     "temp", "vx",
+                                                           "vy", "vz",   "x_m1", "y_m1", "z_m1", "du_m1", "alpha"};
+
+//! derived fields stored in the J-loop type
+enum Derived : int
+{
+    dXm, dKx, dGradh, dPrho, dC, dC11, dC12, dC13, dC22, dC23, dC33, dDivv, dCurlv, dAx, dAy, dAz, kNumDerived
+};
+static const char* const kDerivedNames[kNumDerived] = {"xm",  "kx",  "gradh", "prho", "c",     "c11", "c12", "c13",
+                                                       "c22", "c23", "c33",   "divv", "curlv", "ax",  "ay",  "az"};
+
+enum Stage : int
+{
+    sSync, sNeighbors, sXMass, sVeDefGradh, sIad, sAV, sMomentum, sConserved, sIntegrate, kNumStages
+};
+
+} // namespace sphb
+
+using namespace sphb;
+
+struct sphb_sim
+{
+    size_t n{0};
+    sphb_params p{};
+    sphb_box hbox{};
+    DevBox box{};
+    bool mixed{false};
+    cudaStream_t stream{nullptr};
+
+    DeviceBuffer<double> f[kNumConserved];
+    DeviceBuffer<double> fAlt[kNumConserved];
+    DeviceBuffer<uint64_t> id, idAlt, keys;
+    DeviceBuffer<uint32_t> order;
+    DeviceBuffer<char> sortScratch;
+    DeviceBuffer<double4> pos;
+    DeviceBuffer<uint32_t> nidx;
+    DeviceBuffer<unsigned> nc;
+    DeviceBuffer<char> derived[kNumDerived];
+    DeviceBuffer<double> du;
+    DeviceBuffer<char> hrec, grec;
+    DeviceBuffer<double> whD, whdD;
+    DeviceBuffer<float> whF, whdF;
+    DeviceBuffer<unsigned long long> reduce;
+    DeviceBuffer<unsigned> status;
+    DeviceBuffer<double> partial, cons;
+    double K{0};
+
+    GlobalTree gtree;
+    FocusTree ftree;
+    TreeScratch ts;
+    bool boxFirstCall{true};
+
+    double minDt{0}, minDt_m1{0}, minDtCourant{INFINITY}, minDtRho{INFINITY}, ttot{0};
+    double etot{0}, ecin{0}, eint{0}, linmom{0}, angmom{0};
+    double totalNeighbors{0};
+    uint64_t iteration{1};
+    bool uploaded{false};
+    bool forcesDone{false};
+
+    cudaEvent_t ev[kNumStages + 1]{};
+    float stageMs[kNumStages]{};
+
+    size_t elemBytes() const { return mixed ? sizeof(float) : sizeof(double); }
+    size_t numGroups() const { return (n + kWarp - 1) / kWarp; }
+
+    template<class T>
+    T* dptr(int d) const
+    {
+        return reinterpret_cast<T*>(derived[d].data());
+    }
+};
+
+namespace
+{
+
+int allocateSim(sphb_sim& s)
+{
+    size_t n = s.n;
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        SPHB_TRY(s.f[k].reserve(n));
+        SPHB_TRY(s.fAlt[k].reserve(n));
+    }
+    SPHB_TRY(s.id.reserve(n));
+    SPHB_TRY(s.idAlt.reserve(n));
+    SPHB_TRY(s.keys.reserve(n));
+    SPHB_TRY(s.order.reserve(n));
+    SPHB_TRY(s.sortScratch.reserve(sortScratchBytes(n)));
+    SPHB_TRY(s.pos.reserve(n));
+    SPHB_TRY(s.nidx.reserve(s.numGroups() * size_t(s.p.ngmax) * kWarp));
+    SPHB_TRY(s.nc.reserve(n));
+    for (int d = 0; d < kNumDerived; ++d)
+    {
+        SPHB_TRY(s.derived[d].reserve(n * s.elemBytes()));
+    }
+    SPHB_TRY(s.du.reserve(n));
+    SPHB_TRY(s.hrec.reserve(n * 8 * s.elemBytes()));
+    SPHB_TRY(s.grec.reserve(n * 8 * s.elemBytes()));
+    SPHB_TRY(s.reduce.reserve(4));
+    SPHB_TRY(s.status.reserve(4));
+    SPHB_TRY(s.partial.reserve(9 * 1024));
+    SPHB_TRY(s.cons.reserve(16));
+
+    std::vector<double> wh(kTableSize), whd(kTableSize);
+    s.K = sincKernelTables(s.p.sinc_index, wh.data(), whd.data(), kTableSize);
+    SPHB_TRY(s.whD.reserve(kTableSize));
+    SPHB_TRY(s.whdD.reserve(kTableSize));
+    SPHB_CUDA_TRY(cudaMemcpy(s.whD.data(), wh.data(), kTableSize * sizeof(double), cudaMemcpyHostToDevice));
+    SPHB_CUDA_TRY(cudaMemcpy(s.whdD.data(), whd.data(), kTableSize * sizeof(double), cudaMemcpyHostToDevice));
+    std::vector<float> whf(wh.begin(), wh.end()), whdf(whd.begin(), whd.end());
+    SPHB_TRY(s.whF.reserve(kTableSize));
+    SPHB_TRY(s.whdF.reserve(kTableSize));
+    SPHB_CUDA_TRY(cudaMemcpy(s.whF.data(), whf.data(), kTableSize * sizeof(float), cudaMemcpyHostToDevice));
+    SPHB_CUDA_TRY(cudaMemcpy(s.whdF.data(), whdf.data(), kTableSize * sizeof(float), cudaMemcpyHostToDevice));
+    for (auto& e : s.ev)
+    {
+        SPHB_CUDA_TRY(cudaEventCreate(&e));
+    }
+    return kOk;
+}
+
+double idealGasCv(double mui, double gamma) { return 8.317e7 / mui / (gamma - 1.0); }
+
+//! limitBoxShrinking (cstone/sfc/box.hpp:398-414) and makeGlobalBox (cstone/sfc/box_mpi.hpp:69-107) for open axes
+int updateBox(sphb_sim& s)
+{
+    bool anyOpen = !s.hbox.periodic[0] || !s.hbox.periodic[1] || !s.hbox.periodic[2];
+    if (!anyOpen) { return kOk; }
+    double fit[6];
+    for (int k = 0; k < 3; ++k)
+    {
+        fit[2 * k]     = s.hbox.lo[k];
+        fit[2 * k + 1] = s.hbox.hi[k];
+        if (!s.hbox.periodic[k])
+        {
+            SPHB_TRY(minMax(s.f[fX + k].data(), s.n, s.reduce.data() + 2, s.stream));
+            unsigned long long mm[2];
+            SPHB_CUDA_TRY(cudaMemcpyAsync(mm, s.reduce.data() + 2, sizeof(mm), cudaMemcpyDeviceToHost, s.stream));
+            SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
+            fit[2 * k]     = fromOrderedBits(mm[0]);
+            fit[2 * k + 1] = fromOrderedBits(mm[1]);
+        }
+    }
+    if (!s.boxFirstCall)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            if (s.hbox.periodic[k]) { continue; }
+            double len = s.hbox.hi[k] - s.hbox.lo[k];
+            fit[2 * k]     = std::min(fit[2 * k], s.hbox.lo[k] + 0.05 * len);
+            fit[2 * k + 1] = std::max(fit[2 * k + 1], s.hbox.hi[k] - 0.05 * len);
+        }
+    }
+    for (int k = 0; k < 3; ++k)
+    {
+        s.hbox.lo[k] = fit[2 * k];
+        s.hbox.hi[k] = fit[2 * k + 1];
+    }
+    s.box = makeDevBox(s.hbox);
+    return kOk;
+}
+
+//! Domain::sync at one rank (cstone/domain/domain.hpp:165-213 with assign, assignment.hpp:91-142)
+int syncDomain(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    SPHB_TRY(updateBox(s));
+    s.boxFirstCall = false;
+    SPHB_TRY(launchSfcKeys(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.keys.data(), s.n, s.box, st));
+    SPHB_TRY(sortByKey(s.keys.data(), s.order.data(), s.n, true, s.sortScratch.data(), s.sortScratch.capacity(), st));
+    SPHB_TRY(updateGlobalTree(s.gtree, s.keys.data(), s.n, s.ts, st));
+
+    // reorder every conserved field and the ids into SFC order
+    const void* src[kNumConserved + 1];
+    void* dst[kNumConserved + 1];
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        src[k] = s.f[k].data();
+        dst[k] = s.fAlt[k].data();
+    }
+    src[kNumConserved] = s.id.data();
+    dst[kNumConserved] = s.idAlt.data();
+    SPHB_TRY(gather8(s.order.data(), s.n, kNumConserved + 1, src, dst, st));
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        s.f[k].swap(s.fAlt[k]);
+    }
+    s.id.swap(s.idAlt);
+
+    bool converged = false;
+    if (s.ftree.firstCall)
+    {
+        int guard = 0;
+        while (!converged)
+        {
+            SPHB_TRY(focusUpdateTree(s.ftree, s.gtree, s.ts, st, &converged));
+            SPHB_TRY(focusUpdateCounts(s.ftree, s.keys.data(), s.n, s.ts, st));
+            if (++guard > 100) { return kErrNotConverged; }
+        }
+        s.ftree.firstCall = false;
+    }
+    SPHB_TRY(focusUpdateTree(s.ftree, s.gtree, s.ts, st, &converged));
+    SPHB_TRY(focusUpdateCounts(s.ftree, s.keys.data(), s.n, s.ts, st));
+    SPHB_TRY(computeGeoCenters(s.ftree.tree, s.box, st));
+    SPHB_TRY(packPositions(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n, s.pos.data(), st));
+    return kOk;
+}
+
+template<class T>
+ChainArrays<T> chainArrays(sphb_sim& s)
+{
+    ChainArrays<T> a;
+    a.n     = s.n;
+    a.pos   = s.pos.data();
+    a.h     = s.f[fH].data();
+    a.vx    = s.f[fVx].data();
+    a.vy    = s.f[fVy].data();
+    a.vz    = s.f[fVz].data();
+    a.temp  = s.f[fTemp].data();
+    a.alpha = s.f[fAlpha].data();
+    a.nidx  = s.nidx.data();
+    a.nc    = s.nc.data();
+    if constexpr (sizeof(T) == 8)
+    {
+        a.wh  = reinterpret_cast<const T*>(s.whD.data());
+        a.whd = reinterpret_cast<const T*>(s.whdD.data());
+    }
+    else
+    {
+        a.wh  = reinterpret_cast<const T*>(s.whF.data());
+        a.whd = reinterpret_cast<const T*>(s.whdF.data());
+    }
+    a.xm    = s.dptr<T>(dXm);
+    a.kx    = s.dptr<T>(dKx);
+    a.gradh = s.dptr<T>(dGradh);
+    a.prho  = s.dptr<T>(dPrho);
+    a.c     = s.dptr<T>(dC);
+    for (int q = 0; q < 6; ++q)
+    {
+        a.cij[q] = s.dptr<T>(dC11 + q);
+    }
+    a.divv   = s.dptr<T>(dDivv);
+    a.curlv  = s.dptr<T>(dCurlv);
+    a.ax     = s.dptr<T>(dAx);
+    a.ay     = s.dptr<T>(dAy);
+    a.az     = s.dptr<T>(dAz);
+    a.du     = s.du.data();
+    a.hrec   = reinterpret_cast<HydroRec<T>*>(s.hrec.data());
+    a.grec   = reinterpret_cast<GradRec<T>*>(s.grec.data());
+    a.reduce = s.reduce.data();
+    return a;
+}
+
+template<class T>
+HydroConsts<T> hydroConsts(const sphb_sim& s)
+{
+    HydroConsts<T> k;
+    k.K        = T(s.K);
+    k.alphamin = T(s.p.alphamin);
+    k.alphamax = T(s.p.alphamax);
+    k.decay    = T(s.p.decay_constant);
+    // Atwood ramp of the crossed/uncrossed momentum weights (sph/include/sph/particles_data.hpp:128-133)
+    k.Atmin = T(0.1);
+    k.Atmax = T(0.2);
+    k.ramp  = T(1.0) / (k.Atmax - k.Atmin);
+    k.Kcour = double(float(s.p.Kcour));
+    k.gamma = s.p.gamma;
+    k.cv    = idealGasCv(s.p.mui, s.p.gamma);
+    k.ngmax = s.p.ngmax;
+    return k;
+}
+
+template<class T>
+int runChain(sphb_sim& s)
+{
+    cudaStream_t st     = s.stream;
+    ChainArrays<T> a    = chainArrays<T>(s);
+    HydroConsts<T> k    = hydroConsts<T>(s);
+    SPHB_TRY(launchXMass(a, k, s.box, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sVeDefGradh], st));
+    SPHB_TRY(launchVeDefGradhEos(a, k, s.box, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIad], st));
+    SPHB_TRY(launchIadDivvCurlv(a, k, s.box, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sAV], st));
+    SPHB_TRY(launchAVswitches(a, k, s.box, s.minDt, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sMomentum], st));
+    SPHB_TRY(launchMomentumEnergy(a, k, s.box, st));
+    return kOk;
+}
+
+int computeForces(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sSync], st));
+    SPHB_TRY(syncDomain(s));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sNeighbors], st));
+
+    unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
+
+    TreeView tv;
+    tv.childOffsets = s.ftree.tree.childOffsets.data();
+    tv.nodeToLeaf   = s.ftree.tree.nodeToLeaf.data();
+    tv.centers      = s.ftree.tree.centers.data();
+    tv.sizes        = s.ftree.tree.sizes.data();
+    tv.layout       = s.ftree.layout.data();
+    tv.numNodes     = s.ftree.tree.numNodes;
+    NeighborParams np{s.p.ng0, s.p.ngmax, 10};
+    SPHB_TRY(findNeighbors(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fH].data(), s.n, tv, s.box, np,
+                           s.nidx.data(), s.nc.data(), s.status.data(), st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
+
+    if (s.mixed) { SPHB_TRY(runChain<float>(s)); }
+    else { SPHB_TRY(runChain<double>(s)); }
+
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sConserved], st));
+    double cv = idealGasCv(s.p.mui, s.p.gamma);
+    SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
+                           s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
+                           s.cons.data(), st));
+    double cons[9];
+    unsigned long long red[2];
+    unsigned status = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(red, s.reduce.data(), sizeof(red), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIntegrate], st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (status) { return kErrCapacity; }
+
+    double maxDivv = fromOrderedBits(red[0]);
+    s.minDtRho     = s.p.Krho / std::abs(maxDivv);
+    s.minDtCourant = fromOrderedBits(red[1]);
+    s.ecin         = 0.5 * cons[0];
+    s.eint         = cons[1];
+    s.etot         = s.ecin + s.eint;
+    s.linmom       = std::sqrt(cons[2] * cons[2] + cons[3] * cons[3] + cons[4] * cons[4]);
+    s.angmom       = std::sqrt(cons[5] * cons[5] + cons[6] * cons[6] + cons[7] * cons[7]);
+    s.totalNeighbors = cons[8];
+    s.forcesDone     = true;
+    return kOk;
+}
+
+template<class T>
+int runPositions(sphb_sim& s, double cv)
+{
+    IntegrateArrays<T> a;
+    a.x    = s.f[fX].data();
+    a.y    = s.f[fY].data();
+    a.z    = s.f[fZ].data();
+    a.vx   = s.f[fVx].data();
+    a.vy   = s.f[fVy].data();
+    a.vz   = s.f[fVz].data();
+    a.xm1  = s.f[fXm1].data();
+    a.ym1  = s.f[fYm1].data();
+    a.zm1  = s.f[fZm1].data();
+    a.temp = s.f[fTemp].data();
+    a.duM1 = s.f[fDuM1].data();
+    a.du   = s.du.data();
+    a.ax   = s.dptr<T>(dAx);
+    a.ay   = s.dptr<T>(dAy);
+    a.az   = s.dptr<T>(dAz);
+    return launchPositions(s.n, a, s.box, s.minDt, s.minDt_m1, cv, s.stream);
+}
+
+//! HydroVeProp::integrate (ve_hydro.hpp:205-220): computeTimestep (ts_global.hpp:100-128), positions, h update
+int integrateStep(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    double dtNew    = std::min({s.minDtCourant, s.minDtRho, 1.1 * s.minDt});
+    s.ttot += dtNew;
+    s.minDt_m1 = s.minDt;
+    s.minDt    = dtNew;
+
+    double cv = idealGasCv(s.p.mui, s.p.gamma);
+    if (s.mixed) { SPHB_TRY(runPositions<float>(s, cv)); }
+    else { SPHB_TRY(runPositions<double>(s, cv)); }
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 1, 0, sizeof(unsigned), st));
+    SPHB_TRY(launchUpdateH(s.n, s.p.ng0, s.nc.data(), s.f[fH].data(), s.keys.data(), s.status.data() + 1, st));
+    unsigned flag = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&flag, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[kNumStages], st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int k = 0; k < kNumStages; ++k)
+    {
+        cudaEventElapsedTime(&s.stageMs[k], s.ev[k], s.ev[k + 1]);
+    }
+    s.iteration++;
+    s.forcesDone = false;
+    return flag ? kErrNotConverged : kOk;
+}
+
+} // namespace
+
+// -------------------------------------------------------------------------------------------------------------------
+// C ABI
+// -------------------------------------------------------------------------------------------------------------------
+
+extern "C" void sphb_default_params(sphb_params* p)
+{
+    if (!p) { return; }
+    p->ng0            = 100;
+    p->ngmax          = 150;
+    p->gamma          = 5.0 / 3.0;
+    p->mui            = 10.0;
+    p->Kcour          = 0.2;
+    p->Krho           = 0.06;
+    p->alphamin       = 0.05;
+    p->alphamax       = 1.0;
+    p->decay_constant = 0.2;
+    p->sinc_index     = 6.0;
+    p->minDt          = 1e-12;
+    p->minDt_m1       = 1e-12;
+    p->precision      = SPHB_FP64;
+    p->bucket_focus   = 64;
+}
+
+extern "C" const char* sphb_version(void) { return "sphb200 0.1 (sm_100a)"; }
+
+extern "C" int sphb_sim_create(sphb_sim** out, size_t n, const sphb_box* box, const sphb_params* params)
+{
+    if (!out || !box || !params || n == 0 || n >= (size_t(1) << 30)) { return SPHB_ERR_ARG; }
+    if (params->ng0 > params->ngmax || params->ngmax == 0 || params->bucket_focus == 0) { return SPHB_ERR_ARG; }
+    if (params->precision != SPHB_FP64 && params->precision != SPHB_MIXED) { return SPHB_ERR_ARG; }
+    for (int k = 0; k < 3; ++k)
+    {
+        if (!(box->hi[k] > box->lo[k])) { return SPHB_ERR_ARG; }
+    }
+    auto* s     = new sphb_sim;
+    s->n        = n;
+    s->p        = *params;
+    s->hbox     = *box;
+    s->box      = makeDevBox(*box);
+    s->mixed    = params->precision == SPHB_MIXED;
+    s->minDt    = params->minDt;
+    s->minDt_m1 = params->minDt_m1;
+    int rc      = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess ? kOk : kErrCuda;
+    if (rc == kOk) { rc = allocateSim(*s); }
+    if (rc != kOk)
+    {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_destroy(sphb_sim* s)
+{
+    if (!s) { return SPHB_ERR_ARG; }
+    if (s->stream) { cudaStreamSynchronize(s->stream); }
+    for (auto& e : s->ev)
+    {
+        if (e) { cudaEventDestroy(e); }
+    }
+    if (s->stream) { cudaStreamDestroy(s->stream); }
+    delete s;
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const uint64_t* id, int on_device)
+{
+    if (!s || !fields || !id) { return SPHB_ERR_ARG; }
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        if (!fields[k]) { return SPHB_ERR_ARG; }
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s->f[k].data(), fields[k], s->n * sizeof(double), kind, s->stream));
+    }
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s->id.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s->keys.data(), 0, s->n * sizeof(uint64_t), s->stream));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s->du.data(), 0, s->n * sizeof(double), s->stream));
+    SPHB_TRY(initGlobalTree(s->gtree, std::max<unsigned>(s->p.bucket_focus, unsigned(s->n / 100)), s->stream));
+    SPHB_TRY(initFocusTree(s->ftree, s->p.bucket_focus, s->ts, s->stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->boxFirstCall = true;
+    s->minDt        = s->p.minDt;
+    s->minDt_m1     = s->p.minDt_m1;
+    s->ttot         = 0;
+    s->iteration    = 1;
+    s->uploaded     = true;
+    s->forcesDone   = false;
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_initial_sync(sphb_sim* s)
+{
+    if (!s) { return SPHB_ERR_ARG; }
+    if (!s->uploaded) { return SPHB_ERR_STATE; }
+    SPHB_TRY(syncDomain(*s));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_compute_forces(sphb_sim* s)
+{
+    if (!s) { return SPHB_ERR_ARG; }
+    if (!s->uploaded) { return SPHB_ERR_STATE; }
+    return computeForces(*s);
+}
+
+extern "C" int sphb_sim_integrate(sphb_sim* s)
+{
+    if (!s) { return SPHB_ERR_ARG; }
+    if (!s->forcesDone) { return SPHB_ERR_STATE; }
+    return integrateStep(*s);
+}
+
+extern "C" int sphb_sim_step(sphb_sim* s)
+{
+    int rc = sphb_sim_compute_forces(s);
+    if (rc != SPHB_OK) { return rc; }
+    return sphb_sim_integrate(s);
+}
+
+extern "C" size_t sphb_sim_size(const sphb_sim* s) { return s ? s->n : 0; }
+
+namespace
+{
+
+//! locate a field by name: returns device pointer and element kind (0 double, 1 T, 2 uint32, 3 uint64)
+bool findField(sphb_sim* s, const char* name, void** ptr, int* kind)
+{
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        if (std::strcmp(name, kConservedNames[k]) == 0)
+        {
+            *ptr  = s->f[k].data();
+            *kind = 0;
+            return true;
+        }
+    }
+    for (int d = 0; d < kNumDerived; ++d)
+    {
+        if (std::strcmp(name, kDerivedNames[d]) == 0)
+        {
+            *ptr  = s->derived[d].data();
+            *kind = 1;
+            return true;
+        }
+    }
+    if (std::strcmp(name, "du") == 0)
+    {
+        *ptr  = s->du.data();
+        *kind = 0;
+        return true;
+    }
+    if (std::strcmp(name, "nc") == 0)
+    {
+        *ptr  = s->nc.data();
+        *kind = 2;
+        return true;
+    }
+    if (std::strcmp(name, "keys") == 0)
+    {
+        *ptr  = s->keys.data();
+        *kind = 3;
+        return true;
+    }
+    if (std::strcmp(name, "id") == 0)
+    {
+        *ptr  = s->id.data();
+        *kind = 3;
+        return true;
+    }
+    return false;
+}
+
+} // namespace
+
+extern "C" int sphb_sim_get_field(sphb_sim* s, const char* name, double* out, int on_device)
+{
+    if (!s || !name || !out) { return SPHB_ERR_ARG; }
+    void* ptr = nullptr;
+    int kind  = 0;
+    if (!findField(s, name, &ptr, &kind)) { return SPHB_ERR_ARG; }
+    size_t n = s->n;
+    size_t elem = kind == 0 || kind == 3 ? 8 : kind == 2 ? 4 : s->elemBytes();
+    std::vector<char> host(n * elem);
+    SPHB_CUDA_TRY(cudaMemcpyAsync(host.data(), ptr, n * elem, cudaMemcpyDeviceToHost, s->stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    std::vector<double> conv;
+    double* dst = out;
+    if (on_device)
+    {
+        conv.resize(n);
+        dst = conv.data();
+    }
+    for (size_t i = 0; i < n; ++i)
+    {
+        double v;
+        if (kind == 0 || (kind == 1 && elem == 8)) { std::memcpy(&v, host.data() + 8 * i, 8); }
+        else if (kind == 1) { v = double(reinterpret_cast<const float*>(host.data())[i]); }
+        else if (kind == 2) { v = double(reinterpret_cast<const uint32_t*>(host.data())[i]); }
+        else { std::memcpy(&v, host.data() + 8 * i, 8); } // uint64 bits
+        dst[i] = v;
+    }
+    if (on_device) { SPHB_CUDA_TRY(cudaMemcpy(out, conv.data(), n * sizeof(double), cudaMemcpyHostToDevice)); }
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_set_field(sphb_sim* s, const char* name, const double* in, int on_device)
+{
+    if (!s || !name || !in) { return SPHB_ERR_ARG; }
+    void* ptr = nullptr;
+    int kind  = 0;
+    if (!findField(s, name, &ptr, &kind)) { return SPHB_ERR_ARG; }
+    size_t n = s->n;
+    std::vector<double> src(n);
+    SPHB_CUDA_TRY(cudaMemcpy(src.data(), in, n * sizeof(double),
+                             on_device ? cudaMemcpyDeviceToHost : cudaMemcpyHostToHost));
+    if (kind == 0 || kind == 3 || (kind == 1 && s->elemBytes() == 8))
+    {
+        SPHB_CUDA_TRY(cudaMemcpy(ptr, src.data(), n * 8, cudaMemcpyHostToDevice));
+    }
+    else if (kind == 1)
+    {
+        std::vector<float> f(src.begin(), src.end());
+        SPHB_CUDA_TRY(cudaMemcpy(ptr, f.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+    else
+    {
+        std::vector<uint32_t> u(n);
+        for (size_t i = 0; i < n; ++i)
+        {
+            u[i] = uint32_t(src[i]);
+        }
+        SPHB_CUDA_TRY(cudaMemcpy(ptr, u.data(), n * 4, cudaMemcpyHostToDevice));
+    }
+    if (std::strcmp(name, "x") == 0 || std::strcmp(name, "y") == 0 || std::strcmp(name, "z") == 0 ||
+        std::strcmp(name, "m") == 0)
+    {
+        SPHB_TRY(packPositions(s->f[fX].data(), s->f[fY].data(), s->f[fZ].data(), s->f[fM].data(), s->n,
+                               s->pos.data(), s->stream));
+        SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    }
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_scalars(sphb_sim* s, double* out)
+{
+    if (!s || !out) { return SPHB_ERR_ARG; }
+    double v[18] = {s->minDt,  s->minDt_m1,          s->minDtCourant,     s->minDtRho,  s->ttot,     s->etot,
+                    s->ecin,   s->eint,              s->linmom,           s->angmom,    s->totalNeighbors,
+                    double(s->iteration), s->hbox.lo[0], s->hbox.hi[0], s->hbox.lo[1], s->hbox.hi[1], s->hbox.lo[2],
+                    s->hbox.hi[2]};
+    std::memcpy(out, v, sizeof(v));
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_tree(sphb_sim* s, size_t* num_leaves, uint64_t* leaves, uint32_t* counts, uint32_t* layout)
+{
+    if (!s || !num_leaves) { return SPHB_ERR_ARG; }
+    int L       = s->ftree.numLeaves;
+    *num_leaves = size_t(L);
+    if (leaves)
+    {
+        SPHB_CUDA_TRY(cudaMemcpy(leaves, s->ftree.leaves.data(), (L + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+    }
+    if (counts)
+    {
+        SPHB_CUDA_TRY(cudaMemcpy(counts, s->ftree.leafCounts.data(), L * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
+    if (layout)
+    {
+        SPHB_CUDA_TRY(cudaMemcpy(layout, s->ftree.layout.data(), (L + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    }
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_neighbors(sphb_sim* s, uint32_t* out)
+{
+    if (!s || !out) { return SPHB_ERR_ARG; }
+    size_t ng = s->p.ngmax;
+    std::vector<uint32_t> raw(s->numGroups() * ng * kWarp);
+    SPHB_CUDA_TRY(cudaMemcpy(raw.data(), s->nidx.data(), raw.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < s->n; ++i)
+    {
+        size_t g = i / kWarp, lane = i % kWarp;
+        for (size_t k = 0; k < ng; ++k)
+        {
+            out[i * ng + k] = raw[nidxSlot(g, unsigned(ng), unsigned(k), unsigned(lane))];
+        }
+    }
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_stage_times(sphb_sim* s, float* out)
+{
+    if (!s || !out) { return SPHB_ERR_ARG; }
+    std::memcpy(out, s->stageMs, sizeof(s->stageMs));
+    return SPHB_OK;
+}
+
+extern "C" uint64_t sphb_sim_kernel_launches(const sphb_sim*) { return launchCounter(); }

@@ -1,0 +1,324 @@
+// Stable LSD radix sort of (uint64 key, uint32 value) pairs: one histogram sweep for all digits, then one
+// "onesweep" pass per 8-bit digit in which each tile ranks its keys, resolves its global digit offsets through a
+// decoupled look-back over the preceding tiles, and scatters. Passes whose digit is identical for every key are
+// skipped. Replaces the reference's CUB DeviceRadixSort::SortPairs (cstone/primitives/primitives_gpu.cu:308-339).
+//
+// Tile = 8 warps x 16 keys x 32 lanes = 4096 keys. Within a warp, key k of lane l is element warpBase + k*32 + l, and
+// ranking walks k then l, so ranks follow input order (stability). The look-back status word per (tile, digit) is
+// 32 bits: 2 flag bits (0 = empty, 1 = tile aggregate, 2 = inclusive prefix) and a 30-bit count, so n < 2^30.
+// Every spin on a predecessor's status is bounded; on timeout the pass records an error word that the host reads.
+#include "common.cuh"
+#include "sort.cuh"
+
+namespace sphb
+{
+
+namespace
+{
+
+constexpr int kRadixBits   = 8;
+constexpr int kRadix       = 1 << kRadixBits;
+constexpr int kSortWarps   = 8;
+constexpr int kSortThreads = kSortWarps * kWarp;
+constexpr int kItems       = 16;
+constexpr int kTile        = kSortThreads * kItems;
+constexpr int kPasses      = 8;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagInc = 2u << 30;
+constexpr uint32_t kValMask = (1u << 30) - 1;
+constexpr long kSpinLimit   = 1L << 24;
+
+struct SortScratch
+{
+    uint64_t* keysAlt;
+    uint32_t* valsAlt;
+    uint32_t* hist;       // [kPasses][kRadix] counts, then exclusive offsets
+    uint32_t* status;     // [numTiles][kRadix]
+    uint32_t* counters;   // [0] tile counter, [1] error word
+};
+
+size_t alignUp(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+size_t numTilesOf(size_t n) { return (n + kTile - 1) / kTile; }
+
+SortScratch carve(void* base, size_t n)
+{
+    char* p = static_cast<char*>(base);
+    SortScratch s;
+    s.keysAlt = reinterpret_cast<uint64_t*>(p);
+    p += alignUp(n * sizeof(uint64_t), 256);
+    s.valsAlt = reinterpret_cast<uint32_t*>(p);
+    p += alignUp(n * sizeof(uint32_t), 256);
+    s.hist = reinterpret_cast<uint32_t*>(p);
+    p += alignUp(kPasses * kRadix * sizeof(uint32_t), 256);
+    s.status = reinterpret_cast<uint32_t*>(p);
+    p += alignUp(numTilesOf(n) * kRadix * sizeof(uint32_t), 256);
+    s.counters = reinterpret_cast<uint32_t*>(p);
+    return s;
+}
+
+//! digit histograms of all 8 byte positions in one sweep over the keys
+__global__ void __launch_bounds__(256) histogramKernel(const uint64_t* __restrict__ keys, size_t n,
+                                                       uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t sh[kPasses][kRadix];
+    for (int t = threadIdx.x; t < kPasses * kRadix; t += blockDim.x)
+    {
+        (&sh[0][0])[t] = 0;
+    }
+    __syncthreads();
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        uint64_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < kPasses; ++p)
+        {
+            atomicAdd(&sh[p][(k >> (p * kRadixBits)) & (kRadix - 1)], 1u);
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < kPasses * kRadix; t += blockDim.x)
+    {
+        uint32_t c = (&sh[0][0])[t];
+        if (c) { atomicAdd(hist + t, c); }
+    }
+}
+
+//! exclusive scan of each pass's 256 digit counts, in place (one block per pass)
+__global__ void histScanKernel(uint32_t* hist)
+{
+    __shared__ uint32_t sh[kRadix];
+    uint32_t* h = hist + blockIdx.x * kRadix;
+    int t       = threadIdx.x;
+    uint32_t v  = h[t];
+    sh[t]       = v;
+    __syncthreads();
+    for (int off = 1; off < kRadix; off <<= 1)
+    {
+        uint32_t add = t >= off ? sh[t - off] : 0;
+        __syncthreads();
+        sh[t] += add;
+        __syncthreads();
+    }
+    h[t] = sh[t] - v;
+}
+
+__global__ void iotaKernel(uint32_t* v, size_t n)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i < n) { v[i] = uint32_t(i); }
+}
+
+/*! One onesweep pass over bits [shift, shift+8).
+ *
+ * Shared memory: per-warp digit counters (8 x 256), the tile's exclusive digit prefix (256) and the tile index.
+ */
+__global__ void __launch_bounds__(kSortThreads) onesweepKernel(const uint64_t* __restrict__ keysIn,
+                                                               const uint32_t* __restrict__ valsIn,
+                                                               uint64_t* __restrict__ keysOut,
+                                                               uint32_t* __restrict__ valsOut, size_t n, int shift,
+                                                               const uint32_t* __restrict__ digitOffsets,
+                                                               uint32_t* status, uint32_t* counters)
+{
+    __shared__ uint32_t warpCount[kSortWarps][kRadix];
+    __shared__ uint32_t tilePrefix[kRadix];
+    __shared__ uint32_t tileIdxSh;
+
+    const int lane = threadIdx.x & (kWarp - 1);
+    const int warp = threadIdx.x / kWarp;
+
+    if (threadIdx.x == 0) { tileIdxSh = atomicAdd(counters, 1u); }
+    for (int t = threadIdx.x; t < kSortWarps * kRadix; t += kSortThreads)
+    {
+        (&warpCount[0][0])[t] = 0;
+    }
+    __syncthreads();
+    const size_t tile     = tileIdxSh;
+    const size_t tileBase = tile * kTile;
+    const size_t warpBase = tileBase + size_t(warp) * kItems * kWarp;
+
+    uint64_t key[kItems];
+    uint32_t val[kItems];
+    uint32_t rank[kItems];
+#pragma unroll
+    for (int k = 0; k < kItems; ++k)
+    {
+        size_t idx = warpBase + size_t(k) * kWarp + lane;
+        bool valid = idx < n;
+        key[k]     = valid ? keysIn[idx] : ~uint64_t(0);
+        val[k]     = valid ? valsIn[idx] : 0u;
+    }
+
+    // warp-local stable ranking: peers with equal digits are found with match.any
+#pragma unroll
+    for (int k = 0; k < kItems; ++k)
+    {
+        size_t idx      = warpBase + size_t(k) * kWarp + lane;
+        bool valid      = idx < n;
+        uint32_t digit  = uint32_t(key[k] >> shift) & (kRadix - 1);
+        uint32_t active = __ballot_sync(0xffffffffu, valid);
+        uint32_t peers  = __match_any_sync(0xffffffffu, valid ? digit : 0xffffffffu);
+        peers &= active;
+        uint32_t before = 0;
+        if (valid)
+        {
+            before = warpCount[warp][digit];
+        }
+        __syncwarp();
+        if (valid)
+        {
+            uint32_t lowerPeers = peers & ((1u << lane) - 1u);
+            rank[k]             = before + __popc(lowerPeers);
+            if (lowerPeers == 0) { warpCount[warp][digit] = before + __popc(peers); }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // per digit: exclusive scan over warps, tile total, then look-back across tiles (thread t owns digit t)
+    {
+        const int d    = threadIdx.x;
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w)
+        {
+            uint32_t c     = warpCount[w][d];
+            warpCount[w][d] = total;
+            total += c;
+        }
+        uint32_t* myStatus = status + tile * kRadix + d;
+        if (tile == 0) { atomicExch(myStatus, kFlagInc | total); }
+        else { atomicExch(myStatus, kFlagAgg | total); }
+        __threadfence();
+
+        uint32_t exclusive = 0;
+        if (tile > 0)
+        {
+            long pred = long(tile) - 1;
+            long spins = 0;
+            while (pred >= 0)
+            {
+                uint32_t s = *((volatile uint32_t*)(status + size_t(pred) * kRadix + d));
+                uint32_t flag = s & ~kValMask;
+                if (flag == 0)
+                {
+                    if (++spins > kSpinLimit)
+                    {
+                        atomicExch(counters + 1, 1u);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                exclusive += s & kValMask;
+                if (flag == kFlagInc) { break; }
+                --pred;
+            }
+            atomicExch(myStatus, kFlagInc | ((exclusive + total) & kValMask));
+        }
+        tilePrefix[d] = digitOffsets[d] + exclusive;
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int k = 0; k < kItems; ++k)
+    {
+        size_t idx = warpBase + size_t(k) * kWarp + lane;
+        if (idx < n)
+        {
+            uint32_t digit = uint32_t(key[k] >> shift) & (kRadix - 1);
+            uint32_t pos   = tilePrefix[digit] + warpCount[warp][digit] + rank[k];
+            if (pos < n)
+            {
+                keysOut[pos] = key[k];
+                valsOut[pos] = val[k];
+            }
+            else { atomicExch(counters + 1, 2u); } // inconsistent offsets: report instead of writing
+        }
+    }
+}
+
+} // namespace
+
+size_t sortScratchBytes(size_t n)
+{
+    return alignUp(n * sizeof(uint64_t), 256) + alignUp(n * sizeof(uint32_t), 256) +
+           alignUp(kPasses * kRadix * sizeof(uint32_t), 256) + alignUp(numTilesOf(n) * kRadix * sizeof(uint32_t), 256) +
+           256;
+}
+
+int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,
+              cudaStream_t stream)
+{
+    if (n == 0) { return kOk; }
+    if (n >= (size_t(1) << 30)) { return kErrArg; }
+    if (!scratch || scratchBytes < sortScratchBytes(n)) { return kErrCapacity; }
+    SortScratch s = carve(scratch, n);
+
+    if (initValues)
+    {
+        iotaKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(values, n);
+        SPHB_CUDA_TRY(cudaGetLastError());
+    }
+
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.hist, 0, kPasses * kRadix * sizeof(uint32_t), stream));
+    unsigned histBlocks = unsigned(std::min<size_t>(ceilDiv(n, 256 * 16), size_t(smCount()) * 4));
+    histogramKernel<<<histBlocks, 256, 0, stream>>>(keys, n, s.hist);
+    SPHB_CUDA_TRY(cudaGetLastError());
+
+    // decide on the host which passes are trivial (one digit holds every key)
+    uint32_t h[kPasses * kRadix];
+    SPHB_CUDA_TRY(cudaMemcpyAsync(h, s.hist, sizeof(h), cudaMemcpyDeviceToHost, stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    bool doPass[kPasses];
+    for (int p = 0; p < kPasses; ++p)
+    {
+        doPass[p] = true;
+        for (int d = 0; d < kRadix; ++d)
+        {
+            if (h[p * kRadix + d] == n) { doPass[p] = false; }
+        }
+    }
+
+    histScanKernel<<<kPasses, kRadix, 0, stream>>>(s.hist);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.counters + 1, 0, sizeof(uint32_t), stream));
+
+    size_t tiles      = numTilesOf(n);
+    uint64_t* kIn     = keys;
+    uint32_t* vIn     = values;
+    uint64_t* kOut    = s.keysAlt;
+    uint32_t* vOut    = s.valsAlt;
+    for (int p = 0; p < kPasses; ++p)
+    {
+        if (!doPass[p]) { continue; }
+        SPHB_CUDA_TRY(cudaMemsetAsync(s.status, 0, tiles * kRadix * sizeof(uint32_t), stream));
+        SPHB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(uint32_t), stream));
+        onesweepKernel<<<unsigned(tiles), kSortThreads, 0, stream>>>(kIn, vIn, kOut, vOut, n, p * kRadixBits,
+                                                                      s.hist + p * kRadix, s.status, s.counters);
+        SPHB_CUDA_TRY(cudaGetLastError());
+        std::swap(kIn, kOut);
+        std::swap(vIn, vOut);
+    }
+    if (kIn != keys)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(keys, kIn, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(values, vIn, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
+    }
+    uint32_t err = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    return err ? kErrCapacity : kOk;
+}
+
+} // namespace sphb
+
+extern "C" size_t sphb_sort_by_key_scratch_bytes(size_t n) { return sphb::sortScratchBytes(n); }
+
+extern "C" int sphb_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* scratch,
+                                size_t scratch_bytes, void* stream)
+{
+    if (n && (!keys || !values)) { return SPHB_ERR_ARG; }
+    return sphb::sortByKey(keys, values, n, init_values != 0, scratch, scratch_bytes,
+                           static_cast<cudaStream_t>(stream));
+}

@@ -1,0 +1,129 @@
+"""ctypes binding of libsphb200.so (the C ABI declared in include/sphb200.h).
+
+The library is the only compute path: importing this module fails loudly if it has not been built
+(python -m sphexa_b200.build), and every call checks its status code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsphb200.so")
+
+SPHB_OK = 0
+ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "capacity exhausted", 4: "smoothing length not converged",
+          5: "call out of order"}
+SPHB_FP64 = 0
+SPHB_MIXED = 1
+
+
+class SphbError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {ERRORS.get(code, code)} (status {code})")
+        self.code = code
+
+
+class Box(C.Structure):
+    _fields_ = [("lo", C.c_double * 3), ("hi", C.c_double * 3), ("periodic", C.c_int * 3)]
+
+
+class Params(C.Structure):
+    _fields_ = [("ng0", C.c_uint32), ("ngmax", C.c_uint32), ("gamma", C.c_double), ("mui", C.c_double),
+                ("Kcour", C.c_double), ("Krho", C.c_double), ("alphamin", C.c_double), ("alphamax", C.c_double),
+                ("decay_constant", C.c_double), ("sinc_index", C.c_double), ("minDt", C.c_double),
+                ("minDt_m1", C.c_double), ("precision", C.c_int), ("bucket_focus", C.c_uint32)]
+
+
+#: every extern "C" symbol of include/sphb200.h
+EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sphb_sort_by_key_scratch_bytes",
+            "sphb_sort_by_key", "sphb_gather8", "sphb_compute_octree", "sphb_sim_create", "sphb_sim_destroy",
+            "sphb_sim_upload", "sphb_sim_initial_sync", "sphb_sim_compute_forces", "sphb_sim_integrate",
+            "sphb_sim_step", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
+            "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches")
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m sphexa_b200.build`")
+    lib = C.CDLL(LIB_PATH)
+    P, S = C.c_void_p, C.c_size_t
+    sig = {
+        "sphb_default_params": (None, [C.POINTER(Params)]),
+        "sphb_version": (C.c_char_p, []),
+        "sphb_compute_sfc_keys": (C.c_int, [P, P, P, P, S, C.POINTER(Box), P]),
+        "sphb_sort_by_key_scratch_bytes": (S, [S]),
+        "sphb_sort_by_key": (C.c_int, [P, P, S, C.c_int, P, S, P]),
+        "sphb_gather8": (C.c_int, [P, S, C.c_int, P, P, P]),
+        "sphb_compute_octree": (C.c_int, [P, S, C.c_uint, P, P, S, C.POINTER(S), P]),
+        "sphb_sim_create": (C.c_int, [C.POINTER(P), S, C.POINTER(Box), C.POINTER(Params)]),
+        "sphb_sim_destroy": (C.c_int, [P]),
+        "sphb_sim_upload": (C.c_int, [P, P, P, C.c_int]),
+        "sphb_sim_initial_sync": (C.c_int, [P]),
+        "sphb_sim_compute_forces": (C.c_int, [P]),
+        "sphb_sim_integrate": (C.c_int, [P]),
+        "sphb_sim_step": (C.c_int, [P]),
+        "sphb_sim_size": (S, [P]),
+        "sphb_sim_get_field": (C.c_int, [P, C.c_char_p, P, C.c_int]),
+        "sphb_sim_set_field": (C.c_int, [P, C.c_char_p, P, C.c_int]),
+        "sphb_sim_scalars": (C.c_int, [P, P]),
+        "sphb_sim_tree": (C.c_int, [P, C.POINTER(S), P, P, P]),
+        "sphb_sim_neighbors": (C.c_int, [P, P]),
+        "sphb_sim_stage_times": (C.c_int, [P, P]),
+        "sphb_sim_kernel_launches": (C.c_uint64, [P]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int, what: str):
+    if rc != SPHB_OK:
+        raise SphbError(rc, what)
+
+
+def ptr(a) -> C.c_void_p:
+    """Address of a numpy array or torch tensor."""
+    if isinstance(a, np.ndarray):
+        return C.c_void_p(a.ctypes.data)
+    return C.c_void_p(a.data_ptr())
+
+
+def make_box(limits, periodic) -> Box:
+    b = Box()
+    for k in range(3):
+        b.lo[k] = float(limits[2 * k])
+        b.hi[k] = float(limits[2 * k + 1])
+        b.periodic[k] = int(bool(periodic[k] if hasattr(periodic, "__len__") else periodic))
+    return b
+
+
+def make_params(p: dict, precision: int = SPHB_FP64, bucket: int = 64) -> Params:
+    lib = load()
+    prm = Params()
+    lib.sphb_default_params(C.byref(prm))
+    prm.ng0 = int(p["ng0"])
+    prm.ngmax = int(p["ngmax"])
+    prm.gamma = float(p["gamma"])
+    prm.mui = float(p["mui"])
+    prm.Kcour = float(p["Kcour"])
+    prm.Krho = float(p["Krho"])
+    prm.alphamin = float(p["alphamin"])
+    prm.alphamax = float(p["alphamax"])
+    prm.decay_constant = float(p["decay_constant"])
+    prm.sinc_index = float(p.get("sincIndex", 6.0))
+    prm.minDt = float(p["minDt"])
+    prm.minDt_m1 = float(p["minDt_m1"])
+    prm.precision = int(precision)
+    prm.bucket_focus = int(bucket)
+    return prm

@@ -1,0 +1,124 @@
+"""Host-side mirror of the reference's propagator interface for the VE hydro step.
+
+`Simulation` owns one sphb_sim (the particle dataset in HBM) and exposes the calls of HydroVeProp
+(main/src/propagator/ve_hydro.hpp): sync, computeForces, integrate, plus field access by the reference's field names
+(sph/include/sph/particles_data.hpp:262-266).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import lib as L
+from .ic import CONSERVED_FIELDS
+
+SCALAR_NAMES = ("minDt", "minDt_m1", "minDtCourant", "minDtRho", "ttot", "etot", "ecin", "eint", "linmom", "angmom",
+                "totalNeighbors", "iteration", "xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
+STAGE_NAMES = ("sync", "neighbors", "xmass", "ve_def_gradh_eos", "iad_divv_curlv", "av_switches", "momentum_energy",
+               "conserved", "integrate")
+
+
+class Simulation:
+    """One SPH-VE simulation on the current CUDA device.
+
+    ic: dict from sphexa_b200.ic (fields, "box", "periodic", "params"); precision: "fp64" or "mixed".
+    """
+
+    def __init__(self, ic: dict, precision: str = "fp64", initial_sync: bool = True):
+        self.lib = L.load()
+        self.n = int(ic["x"].size)
+        self.params = dict(ic["params"])
+        self.precision = precision
+        prec = L.SPHB_MIXED if precision == "mixed" else L.SPHB_FP64
+        box = L.make_box(ic["box"], [ic["periodic"]] * 3)
+        prm = L.make_params(self.params, prec)
+        h = C.c_void_p()
+        L.check(self.lib.sphb_sim_create(C.byref(h), self.n, C.byref(box), C.byref(prm)), "sphb_sim_create")
+        self.h = h
+        self.upload(ic)
+        if initial_sync:
+            self.initial_sync()
+
+    def upload(self, ic: dict, on_device: bool = False):
+        """Copy the 14 conserved fields and ids in (host numpy arrays, or device tensors with on_device)."""
+        if on_device:
+            arrs = [ic[f] for f in CONSERVED_FIELDS]
+            ids = ic["id"]
+        else:
+            arrs = [np.ascontiguousarray(ic[f], dtype=np.float64) for f in CONSERVED_FIELDS]
+            ids = np.ascontiguousarray(ic["id"], dtype=np.uint64)
+        table = (C.c_void_p * len(arrs))(*[L.ptr(a).value for a in arrs])
+        L.check(self.lib.sphb_sim_upload(self.h, table, L.ptr(ids), int(on_device)), "sphb_sim_upload")
+
+    def initial_sync(self):
+        L.check(self.lib.sphb_sim_initial_sync(self.h), "sphb_sim_initial_sync")
+
+    def compute_forces(self):
+        L.check(self.lib.sphb_sim_compute_forces(self.h), "sphb_sim_compute_forces")
+
+    def integrate(self) -> int:
+        rc = self.lib.sphb_sim_integrate(self.h)
+        if rc not in (L.SPHB_OK, 4):
+            L.check(rc, "sphb_sim_integrate")
+        return rc
+
+    def step(self) -> int:
+        self.compute_forces()
+        return self.integrate()
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.n, dtype=np.float64)
+        L.check(self.lib.sphb_sim_get_field(self.h, name.encode(), L.ptr(out), 0), f"get_field({name})")
+        if name in ("keys", "id"):
+            return out.view(np.uint64)
+        return out
+
+    def get_device(self, name: str, out) -> None:
+        """Copy a field as doubles into a device buffer (torch tensor)."""
+        L.check(self.lib.sphb_sim_get_field(self.h, name.encode(), L.ptr(out), 1), f"get_field({name})")
+
+    def set(self, name: str, values: np.ndarray):
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        L.check(self.lib.sphb_sim_set_field(self.h, name.encode(), L.ptr(v), 0), f"set_field({name})")
+
+    def keys(self) -> np.ndarray:
+        return self.get("keys")
+
+    def scalars(self) -> dict:
+        out = np.empty(len(SCALAR_NAMES))
+        L.check(self.lib.sphb_sim_scalars(self.h, L.ptr(out)), "scalars")
+        return dict(zip(SCALAR_NAMES, out.tolist()))
+
+    def tree(self):
+        nl = C.c_size_t()
+        L.check(self.lib.sphb_sim_tree(self.h, C.byref(nl), None, None, None), "tree")
+        leaves = np.empty(nl.value + 1, dtype=np.uint64)
+        counts = np.empty(nl.value, dtype=np.uint32)
+        layout = np.empty(nl.value + 1, dtype=np.uint32)
+        L.check(self.lib.sphb_sim_tree(self.h, C.byref(nl), L.ptr(leaves), L.ptr(counts), L.ptr(layout)), "tree")
+        return leaves, counts, layout
+
+    def neighbors(self) -> np.ndarray:
+        out = np.empty((self.n, int(self.params["ngmax"])), dtype=np.uint32)
+        L.check(self.lib.sphb_sim_neighbors(self.h, L.ptr(out)), "neighbors")
+        return out
+
+    def stage_times(self) -> dict:
+        out = np.empty(len(STAGE_NAMES), dtype=np.float32)
+        L.check(self.lib.sphb_sim_stage_times(self.h, L.ptr(out)), "stage_times")
+        return dict(zip(STAGE_NAMES, out.tolist()))
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.sphb_sim_kernel_launches(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sphb_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
