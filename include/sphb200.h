@@ -162,8 +162,28 @@ int sphb_sim_neighbors(sphb_sim* sim, uint32_t* out);
  *  eos, iad_divv_curlv, av_switches, momentum_energy, integrate (9 floats). */
 int sphb_sim_stage_times(sphb_sim* sim, float* out);
 
-/*! Number of kernels this library launched since the simulation was created (for launch accounting). */
+/*! Number of kernels this library has launched in this process (for launch accounting). */
 uint64_t sphb_sim_kernel_launches(const sphb_sim* sim);
+
+/*! The CUDA stream (a cudaStream_t) on which the simulation issues all its work. */
+void* sphb_sim_stream(sphb_sim* sim);
+
+/*! Replace the 14 conserved fields and the ids of the current particles (same count, same layout as
+ *  sphb_sim_upload) without resetting the domain state (trees, time step, iteration): the per-step host round trip of
+ *  a caller that keeps the particle state in its own host buffers. */
+int sphb_sim_load_state(sphb_sim* sim, const double* const* fields, const uint64_t* id, int on_device);
+
+/*! Copy the 14 conserved fields and the ids out (current SFC order), host memory if on_device == 0. */
+int sphb_sim_store_state(sphb_sim* sim, double* const* fields, uint64_t* id, int on_device);
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* 3. Measurement helper                                                                                            */
+/* ---------------------------------------------------------------------------------------------------------------- */
+
+/*! Measure the CUDA-core FMA throughput of the current device: which = 0 for FP32, 1 for FP64. Runs a short
+ *  register-resident FMA kernel over all SMs and returns the achieved TFLOP/s (2 flops per FMA) in *tflops.
+ *  No counterpart in the reference: it supplies the roofline denominator of the FP32/FP64-bound neighbour sums. */
+int sphb_probe_fma_peak(int which, double* tflops);
 
 #ifdef __cplusplus
 }

@@ -718,3 +718,33 @@ extern "C" int sphb_sim_stage_times(sphb_sim* s, float* out)
 }
 
 extern "C" uint64_t sphb_sim_kernel_launches(const sphb_sim*) { return launchCounter(); }
+
+extern "C" void* sphb_sim_stream(sphb_sim* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
+
+extern "C" int sphb_sim_load_state(sphb_sim* s, const double* const* fields, const uint64_t* id, int on_device)
+{
+    if (!s || !fields || !id) { return SPHB_ERR_ARG; }
+    if (!s->uploaded) { return SPHB_ERR_STATE; }
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        if (!fields[k]) { return SPHB_ERR_ARG; }
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s->f[k].data(), fields[k], s->n * sizeof(double), kind, s->stream));
+    }
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s->id.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_store_state(sphb_sim* s, double* const* fields, uint64_t* id, int on_device)
+{
+    if (!s || !fields || !id) { return SPHB_ERR_ARG; }
+    cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        if (!fields[k]) { return SPHB_ERR_ARG; }
+        SPHB_CUDA_TRY(cudaMemcpyAsync(fields[k], s->f[k].data(), s->n * sizeof(double), kind, s->stream));
+    }
+    SPHB_CUDA_TRY(cudaMemcpyAsync(id, s->id.data(), s->n * sizeof(uint64_t), kind, s->stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SPHB_OK;
+}

@@ -42,7 +42,8 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sort_by_key", "sphb_gather8", "sphb_compute_octree", "sphb_sim_create", "sphb_sim_destroy",
             "sphb_sim_upload", "sphb_sim_initial_sync", "sphb_sim_compute_forces", "sphb_sim_integrate",
             "sphb_sim_step", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
-            "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches")
+            "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches",
+            "sphb_sim_stream", "sphb_sim_load_state", "sphb_sim_store_state", "sphb_probe_fma_peak")
 
 _lib = None
 
@@ -78,6 +79,10 @@ def load() -> C.CDLL:
         "sphb_sim_neighbors": (C.c_int, [P, P]),
         "sphb_sim_stage_times": (C.c_int, [P, P]),
         "sphb_sim_kernel_launches": (C.c_uint64, [P]),
+        "sphb_sim_stream": (C.c_void_p, [P]),
+        "sphb_sim_load_state": (C.c_int, [P, P, P, C.c_int]),
+        "sphb_sim_store_state": (C.c_int, [P, P, P, C.c_int]),
+        "sphb_probe_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
