@@ -6,6 +6,9 @@
 namespace sphb
 {
 
+//! number of coefficients of the FP32 polynomial kernel (degree 12 in t)
+constexpr int kPolyTerms = 13;
+
 //! physics constants of one simulation, in the J-loop type T
 template<class T>
 struct HydroConsts
@@ -16,17 +19,21 @@ struct HydroConsts
     double Kcour;  // stored as the float the reference passes to tsKCourant (sph/include/sph/kernels.hpp:10-17)
     double gamma, cv;
     unsigned ngmax;
+    // FP32 path only: polynomial kernel W(v) = P(t), dW/dv = v Q(t), t = v^2/2 - 1 (instead of table lookups)
+    int usePoly;
+    float wpoly[kPolyTerms];
+    float dwpoly[kPolyTerms];
 };
 
 /*! Per-particle neighbour-side records, written by the stage that produces the values and gathered once per
  *  neighbour by the next stages (one 16-byte-aligned record instead of one scattered load per field).
  *  pos:   x, y, z, m            (double, every stage)
- *  hydro: vx, vy, vz, h, xm, kx, c, prho   (T; written by VeDefGradh+EOS)
+ *  hydro: vx, vy, vz, 1/h, xm, xm/kx, c, prho   (T; written by VeDefGradh+EOS)
  *  grad:  c11, c12, c13, c22, c23, c33, divv, alpha   (T; c_ij and divv by IAD, alpha by the AV switches) */
 template<class T>
 struct alignas(8 * sizeof(T)) HydroRec
 {
-    T vx, vy, vz, h, xm, kx, c, prho;
+    T vx, vy, vz, hInv, xm, vol, c, prho; // hInv = 1/h, vol = xm/kx
 };
 
 template<class T>

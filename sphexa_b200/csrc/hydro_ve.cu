@@ -71,6 +71,41 @@ __device__ __forceinline__ T tableLookup(const T* __restrict__ table, T v)
     return t0 + derivative * (v - T(idx) * dx);
 }
 
+//! Horner evaluation of the FP32 kernel polynomial in t = v^2/2 - 1
+__device__ __forceinline__ float polyEval(const float (&c)[kPolyTerms], float v)
+{
+    float t   = fmaf(0.5f * v, v, -1.0f);
+    float acc = c[kPolyTerms - 1];
+#pragma unroll
+    for (int p = kPolyTerms - 2; p >= 0; --p)
+    {
+        acc = fmaf(acc, t, c[p]);
+    }
+    return acc;
+}
+
+//! the smoothing kernel W(v), zero from v = 2 on: FP64 by table lookup (as the reference), FP32 by polynomial
+template<class T>
+__device__ __forceinline__ T kernelW(const T* __restrict__ table, const HydroConsts<T>& k, T v)
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        if (k.usePoly) { return v < T(2) ? polyEval(k.wpoly, v) : T(0); }
+    }
+    return tableLookup(table, v);
+}
+
+//! dW/dv, zero from v = 2 on
+template<class T>
+__device__ __forceinline__ T kernelDW(const T* __restrict__ table, const HydroConsts<T>& k, T v)
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        if (k.usePoly) { return v < T(2) ? v * polyEval(k.dwpoly, v) : T(0); }
+    }
+    return tableLookup(table, v);
+}
+
 //! periodic shift of a pair separation by one box length if it exceeds r (cstone/sfc/box.hpp applyPBC, legacy form)
 __device__ __forceinline__ void shiftPbc(double& rx, double& ry, double& rz, double r, const DevBox& box)
 {
@@ -185,7 +220,7 @@ __global__ void __launch_bounds__(kChainThreads) xmassKernel(ChainArrays<T> a, H
         shiftPbc(rx, ry, rz, 2.0 * hiD, box);
         T fx = T(rx), fy = T(ry), fz = T(rz);
         T dist = sqrt(fx * fx + fy * fy + fz * fz);
-        T w    = tableLookup(a.wh, dist * hInv);
+        T w    = kernelW(a.wh, k, dist * hInv);
         rho0.add(w * T(pj.w));
     }
     a.xm[t.i] = mi / (rho0.get() * k.K * h3Inv);
@@ -219,8 +254,8 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays
         T fx = T(rx), fy = T(ry), fz = T(rz);
         T dist   = sqrt(fx * fx + fy * fy + fz * fz);
         T vloc   = dist * hInv;
-        T w      = tableLookup(a.wh, vloc);
-        T dw     = tableLookup(a.whd, vloc);
+        T w      = kernelW(a.wh, k, vloc);
+        T dw     = kernelDW(a.whd, k, vloc);
         T dterh  = -(T(3) * w + vloc * dw);
         T xmassj = __ldg(a.xm + j);
         kxS.add(w * xmassj);
@@ -247,7 +282,7 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays
     a.gradh[t.i] = gradhi;
     a.prho[t.i]  = T(prho);
     a.c[t.i]     = T(c);
-    a.hrec[t.i]  = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), hi, xmassi, kxi, T(c), T(prho)};
+    a.hrec[t.i]  = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), T(1) / hi, xmassi, xmassi / kxi, T(c), T(prho)};
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -284,8 +319,8 @@ __global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<
             shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
             T rx = T(rxD), ry = T(ryD), rz = T(rzD);
             T dist   = sqrt(rx * rx + ry * ry + rz * rz);
-            T w      = tableLookup(a.wh, dist * hiInv);
-            T voljW  = hj.xm / hj.kx * w;
+            T w      = kernelW(a.wh, k, dist * hiInv);
+            T voljW  = hj.vol * w;
             s11.add(rx * rx * voljW);
             s12.add(rx * ry * voljW);
             s13.add(rx * rz * voljW);
@@ -316,7 +351,7 @@ __global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<
 
         HydroRec<T> hrI = a.hrec[t.i];
         T vxi = hrI.vx, vyi = hrI.vy, vzi = hrI.vz;
-        T kxi = hrI.kx;
+        T kxi = a.kx[t.i];
         Sum<T> dVxx, dVxy, dVxz, dVyx, dVyy, dVyz, dVzx, dVzy, dVzz;
 #pragma unroll 4
         for (unsigned q = 0; q < t.count; ++q)
@@ -332,7 +367,7 @@ __global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<
             T vxji  = hj.vx - vxi;
             T vyji  = hj.vy - vyi;
             T vzji  = hj.vz - vzi;
-            T Wi    = tableLookup(a.wh, dist * hiInv);
+            T Wi    = kernelW(a.wh, k, dist * hiInv);
             T tA0   = -(c11i * rx + c12i * ry + c13i * rz) * Wi;
             T tA1   = -(c12i * rx + c22i * ry + c23i * rz) * Wi;
             T tA2   = -(c13i * rx + c23i * ry + c33i * rz) * Wi;
@@ -429,11 +464,11 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
         T vsig = T(0);
         if (rv < T(0)) { vsig = ci + hj.c - T(3) * rv / dist; }
         vijsignalI = vijsignalI > vsig ? vijsignalI : vsig;
-        T Wi   = k.K * hiInv3 * tableLookup(a.wh, dist * hiInv);
+        T Wi   = k.K * hiInv3 * kernelW(a.wh, k, dist * hiInv);
         T tA1  = -(gr.c11 * rx + gr.c12 * ry + gr.c13 * rz) * Wi;
         T tA2  = -(gr.c12 * rx + gr.c22 * ry + gr.c23 * rz) * Wi;
         T tA3  = -(gr.c13 * rx + gr.c23 * ry + gr.c33 * rz) * Wi;
-        T volj = hj.xm / hj.kx;
+        T volj = hj.vol;
         T fac  = volj * (divvI - gj.divv);
         gx.add(fac * tA1);
         gy.add(fac * tA2);
@@ -485,7 +520,7 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArray
         T hi      = T(hiD);
         T mi      = T(pi.w);
         T ci      = hr.c;
-        T kxi     = hr.kx;
+        T kxi     = a.kx[t.i];
         T alphaI  = gr.alpha;
         T xmassi  = hr.xm;
         T rhoi    = kxi * mi / xmassi;
@@ -510,12 +545,12 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArray
             T vxij  = hr.vx - hj.vx;
             T vyij  = hr.vy - hj.vy;
             T vzij  = hr.vz - hj.vz;
-            T hjInv = T(1) / hj.h;
+            T hjInv = hj.hInv;
             T v1    = dist * hiInv;
             T v2    = dist * hjInv;
             T hjInv3 = hjInv * hjInv * hjInv;
-            T Wi    = hiInv3 * tableLookup(a.wh, v1);
-            T Wj    = hjInv3 * tableLookup(a.wh, v2);
+            T Wi    = hiInv3 * kernelW(a.wh, k, v1);
+            T Wj    = hjInv3 * kernelW(a.wh, k, v2);
 
             T tA1i = -(gr.c11 * rx + gr.c12 * ry + gr.c13 * rz) * Wi;
             T tA2i = -(gr.c12 * rx + gr.c22 * ry + gr.c23 * rz) * Wi;
@@ -527,7 +562,7 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArray
             T mj     = T(pj.w);
             T cj     = hj.c;
             T xmassj = hj.xm;
-            T rhoj   = hj.kx * mj / xmassj;
+            T rhoj   = mj / hj.vol;
 
             T rv  = rx * vxij + ry * vyij + rz * vzij;
             T wij = rv / dist;

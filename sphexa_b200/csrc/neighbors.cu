@@ -30,11 +30,15 @@ struct NbShared
     int leaf[kNbWarps][kLeafCap];
     int first[kNbWarps][kLeafCap];
     int prefix[kNbWarps][kLeafCap + 1];
-    double sx[kNbWarps][kWarp];
-    double sy[kNbWarps][kWarp];
-    double sz[kNbWarps][kWarp];
-    int sj[kNbWarps][kWarp];
+    float4 cand[kNbWarps][kWarp]; // candidate position relative to the group centre (FP32) and its index
 };
+
+/*! Half width of the band |d^2 - (2h)^2| < band * (2h)^2 in which the FP32 distance cannot decide and the exact FP64
+ *  test runs. Relative coordinates are formed in FP64 and rounded once to FP32, so each has an error of at most
+ *  2^-24 S, S = the largest distance from the group centre at which a neighbour of the group can lie. For a pair at
+ *  distance ~2h that bounds the FP32 squared-distance error by about 2^-21 (S / 2h + 1) (2h)^2 including the FP32
+ *  arithmetic; the band is four times that. */
+__device__ inline float bandOf(float S, float twoH) { return 2.0e-6f * (S / twoH + 1.0f); }
 
 __device__ inline double warpMin(double v)
 {
@@ -119,6 +123,21 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
             gc[k] = 0.5 * (blo[k] + bhi[k]);
             gs[k] = 0.5 * (bhi[k] - blo[k]) * (1.0 + 1e-12) + 1e-14 * box.len[k];
         }
+        // this particle relative to the group centre in FP32, and the FP32 acceptance band
+        const float rix = float(minImage(xi - gc[0], box.len[0], box.ilen[0], box.periodic[0]));
+        const float riy = float(minImage(yi - gc[1], box.len[1], box.ilen[1], box.periodic[1]));
+        const float riz = float(minImage(zi - gc[2], box.len[2], box.ilen[2], box.periodic[2]));
+        const float twoH = float(r);
+        const float r2f  = twoH * twoH;
+        float reach      = active ? sqrtf(rix * rix + riy * riy + riz * riz) * 1.001f + twoH : 0.f;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            reach = fmaxf(reach, __shfl_xor_sync(0xffffffffu, reach, off));
+        }
+        const float band = active ? bandOf(reach, twoH) : 0.f;
+        const float r2lo = r2f * (1.f - band);
+        const float r2hi = r2f * (1.f + band);
 
         if (active) { count = 0; }
         int numLeaves = 0;
@@ -175,22 +194,21 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
                         else { hiIdx = mid; }
                     }
                     int j = firsts[lo] + (t - prefix[lo]);
+                    float4 c;
                     if (j < 0 || size_t(j) >= n)
                     {
-                        // a layout that points outside the particle arrays: report, test a far-away point
+                        // a layout that points outside the particle arrays: report, stage a far-away point
                         atomicOr(status, 2u);
-                        j = 0;
-                        sh.sx[warp][lane] = INFINITY;
-                        sh.sy[warp][lane] = INFINITY;
-                        sh.sz[warp][lane] = INFINITY;
+                        c = make_float4(INFINITY, INFINITY, INFINITY, __int_as_float(0));
                     }
                     else
                     {
-                        sh.sx[warp][lane] = x[j];
-                        sh.sy[warp][lane] = y[j];
-                        sh.sz[warp][lane] = z[j];
+                        c = make_float4(float(minImage(x[j] - gc[0], box.len[0], box.ilen[0], box.periodic[0])),
+                                        float(minImage(y[j] - gc[1], box.len[1], box.ilen[1], box.periodic[1])),
+                                        float(minImage(z[j] - gc[2], box.len[2], box.ilen[2], box.periodic[2])),
+                                        __int_as_float(j));
                     }
-                    sh.sj[warp][lane] = j;
+                    sh.cand[warp][lane] = c;
                 }
                 __syncwarp();
                 int cnt = min(kWarp, total - base);
@@ -198,12 +216,24 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
                 {
                     for (int k = 0; k < cnt; ++k)
                     {
-                        double dx = minImage(sh.sx[warp][k] - xi, box.len[0], box.ilen[0], box.periodic[0]);
-                        double dy = minImage(sh.sy[warp][k] - yi, box.len[1], box.ilen[1], box.periodic[1]);
-                        double dz = minImage(sh.sz[warp][k] - zi, box.len[2], box.ilen[2], box.periodic[2]);
-                        double d2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-                        int j     = sh.sj[warp][k];
-                        if (d2 < radiusSq && size_t(j) != i)
+                        float4 c  = sh.cand[warp][k];
+                        float dx  = c.x - rix;
+                        float dy  = c.y - riy;
+                        float dz  = c.z - riz;
+                        float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        if (d2f >= r2hi) { continue; }
+                        int j   = __float_as_int(c.w);
+                        bool in = d2f < r2lo;
+                        if (!in)
+                        {
+                            // too close to the search radius for FP32: the exact test of the reference
+                            double ex = minImage(x[j] - xi, box.len[0], box.ilen[0], box.periodic[0]);
+                            double ey = minImage(y[j] - yi, box.len[1], box.ilen[1], box.periodic[1]);
+                            double ez = minImage(z[j] - zi, box.len[2], box.ilen[2], box.periodic[2]);
+                            double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+                            in        = d2 < radiusSq;
+                        }
+                        if (in && size_t(j) != i)
                         {
                             if (count < prm.ngmax) { nidx[nidxSlot(group, prm.ngmax, count, lane)] = uint32_t(j); }
                             ++count;

@@ -291,6 +291,19 @@ HydroConsts<T> hydroConsts(const sphb_sim& s)
     k.gamma = s.p.gamma;
     k.cv    = idealGasCv(s.p.mui, s.p.gamma);
     k.ngmax = s.p.ngmax;
+    k.usePoly = 0;
+    if constexpr (sizeof(T) == 4)
+    {
+        // the polynomial replaces the table only if it reproduces the kernel to well inside FP32 resolution
+        double cw[kPolyTerms], cdw[kPolyTerms];
+        double err = sincPolyCoeffs(s.p.sinc_index, kPolyTerms - 1, cw, cdw);
+        k.usePoly  = err < 1e-6 ? 1 : 0;
+        for (int q = 0; q < kPolyTerms; ++q)
+        {
+            k.wpoly[q]  = float(cw[q]);
+            k.dwpoly[q] = float(cdw[q]);
+        }
+    }
     return k;
 }
 
