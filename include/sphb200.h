@@ -90,6 +90,21 @@ size_t sphb_sort_by_key_scratch_bytes(size_t n);
 int sphb_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* scratch, size_t scratch_bytes,
                      void* stream);
 
+/*! Same sort as sphb_sort_by_key, for callers that cannot allocate device memory: for example code whose device
+ *  memory all belongs to another allocator (a framework's caching pool), or code running where cudaMalloc is not
+ *  allowed or would synchronise the device. It calls no cudaMalloc, cudaFree or other allocating routine; its
+ *  scratch is a fixed array of about 12.6 MB inside this library, which every GPU that loads the library keeps until
+ *  the process exits. n may be at most sphb_sort_by_key_static_max() (1,048,576); larger n returns
+ *  SPHB_ERR_CAPACITY and sorts nothing. The first call on a device looks up the array's device address (once per
+ *  device); make that first call before any stream capture. All calls share the one array: calls that overlap on
+ *  the GPU (on different streams or from different threads) race with each other, so run them one after another.
+ *  The array keeps the previous call's contents; every call clears what it needs before use.
+ *  No counterpart in the reference. */
+int sphb_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* stream);
+
+/*! Largest n accepted by sphb_sort_by_key_static. */
+size_t sphb_sort_by_key_static_max(void);
+
 /*! dst_f[i] = src_f[order[i]] for num_fields arrays of 8-byte elements (double or uint64).
  *  Replaces cstone::gatherGpu (domain/include/cstone/primitives/primitives_gpu.cu:73-88) applied per field by
  *  Domain::updateLayout (domain/include/cstone/domain/domain.hpp:491-537). */

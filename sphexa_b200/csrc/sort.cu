@@ -7,6 +7,8 @@
 // ranking walks k then l, so ranks follow input order (stability). The look-back status word per (tile, digit) is
 // 32 bits: 2 flag bits (0 = empty, 1 = tile aggregate, 2 = inclusive prefix) and a 30-bit count, so n < 2^30.
 // Every spin on a predecessor's status is bounded; on timeout the pass records an error word that the host reads.
+#include <mutex>
+
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -311,7 +313,71 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
     return err ? kErrCapacity : kOk;
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Allocation-free variant: the scratch lives in a fixed device array of this library (see sphb_sort_by_key_static)
+// ---------------------------------------------------------------------------------------------------------------
+
+//! largest n accepted by the allocation-free sort
+constexpr size_t kStaticSortMaxN = size_t(1) << 20;
+
+constexpr size_t alignUpC(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+constexpr size_t kStaticSortBytes = alignUpC(kStaticSortMaxN * sizeof(uint64_t), 256) +
+                                    alignUpC(kStaticSortMaxN * sizeof(uint32_t), 256) +
+                                    alignUpC(kPasses * kRadix * sizeof(uint32_t), 256) +
+                                    alignUpC((kStaticSortMaxN + kTile - 1) / kTile * kRadix * sizeof(uint32_t), 256) +
+                                    256;
+
+/*! Scratch of the allocation-free sort: ~12.6 MB of device memory that every GPU which loads this library holds until
+ *  the process exits. Host code must not use the symbol itself as a device address; it asks the runtime for the
+ *  device address of this array once per device (staticSortScratch below). */
+static __device__ __align__(256) unsigned char gStaticSortScratch[kStaticSortBytes];
+
+namespace
+{
+
+constexpr int kMaxDevices = 64;
+std::mutex gStaticScratchMutex;
+void* gStaticScratchAddr[kMaxDevices] = {};
+
+//! device address of gStaticSortScratch on the current device, looked up on the first call per device
+int staticSortScratch(void** ptr)
+{
+    int dev = 0;
+    SPHB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) { return kErrArg; }
+    std::lock_guard<std::mutex> lock(gStaticScratchMutex);
+    if (!gStaticScratchAddr[dev])
+    {
+        void* p = nullptr;
+        SPHB_CUDA_TRY(cudaGetSymbolAddress(&p, gStaticSortScratch));
+        gStaticScratchAddr[dev] = p;
+    }
+    *ptr = gStaticScratchAddr[dev];
+    return kOk;
+}
+
+} // namespace
+
 } // namespace sphb
+
+extern "C" size_t sphb_sort_by_key_static_max(void) { return sphb::kStaticSortMaxN; }
+
+extern "C" int sphb_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* stream)
+{
+    if (n && (!keys || !values)) { return SPHB_ERR_ARG; }
+    if (n > sphb::kStaticSortMaxN)
+    {
+        std::fprintf(stderr, "sphb_sort_by_key_static: n = %zu exceeds the fixed scratch capacity of %zu pairs\n", n,
+                     sphb::kStaticSortMaxN);
+        return SPHB_ERR_CAPACITY;
+    }
+    void* scratch = nullptr;
+    int rc        = sphb::staticSortScratch(&scratch);
+    if (rc != SPHB_OK) { return rc; }
+    return sphb::sortByKey(keys, values, n, init_values != 0, scratch, sphb::kStaticSortBytes,
+                           static_cast<cudaStream_t>(stream));
+}
 
 extern "C" size_t sphb_sort_by_key_scratch_bytes(size_t n) { return sphb::sortScratchBytes(n); }
 
