@@ -1,0 +1,272 @@
+"""CPU tests of the oracle: the C restatement (oracle/liboracle.so) pinned against the reference's own known answers
+(sph/test/ve.cpp on its example_data.txt fixture, committed under tests/golden/) and against the reference CPU code
+itself (oracle/_ref, and its recorded outputs in tests/golden/*_ref.npz)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+COLUMNS = ("x", "y", "z", "vx", "vy", "vz", "h", "c", "c11", "c12", "c13", "c22", "c23", "c33", "p", "gradh", "rho0",
+           "sumwhrho0", "sumwh", "dvxdx", "dvxdy", "dvxdz", "dvydx", "dvydy", "dvydz", "dvzdx", "dvzdy", "dvzdz",
+           "alpha", "u", "divv")
+
+
+@pytest.fixture(scope="module")
+def orc():
+    from oracle import restated
+    if not restated.available():
+        pytest.skip("oracle/liboracle.so not built")
+    restated.load()
+    return restated
+
+
+# ----------------------------------------------------------------------------------------------------------------
+# known answers of the reference's SPH kernel tests (sph/test/ve.cpp:52-249)
+# ----------------------------------------------------------------------------------------------------------------
+
+class VeFixture:
+    """The ve.cpp fixture: particle 0 with neighbours 1..98 in an open box of half size 1e9, FP64 sinc^6 tables and
+    K = sphynx_3D_k(6) (ve.cpp:52-110)."""
+
+    def __init__(self, orc):
+        import ctypes as C
+        d = np.load(os.path.join(GOLDEN, "ve_example_data.npy"))
+        self.f = {c: np.ascontiguousarray(d[:, k]) for k, c in enumerate(COLUMNS)}
+        self.n = d.shape[0]
+        self.lib = orc.load()
+        self.K = self.lib.orc_sphynx_3d_k(6.0)
+        _, self.wh, self.whd = orc.tables(6.0)
+        self.mpart = 3.781038064465603e26
+        f = self.f
+        f["m"] = np.full(self.n, self.mpart)
+        f["xm"] = self.mpart / f["rho0"]
+        f["kx"] = self.K * f["xm"] / f["h"] ** 3
+        f["prho"] = f["p"] / (f["kx"] * f["m"] * f["m"] * f["gradh"])
+        f["dV11"] = f["dvxdx"]
+        f["dV12"] = f["dvxdy"] + f["dvydx"]
+        f["dV13"] = f["dvxdz"] + f["dvzdx"]
+        f["dV22"] = f["dvydy"]
+        f["dV23"] = f["dvydz"] + f["dvzdy"]
+        f["dV33"] = f["dvzdz"]
+        self.nb = np.arange(1, self.n, dtype=np.uint32)
+        self.box = orc.box((-1e9, 1e9) * 3, False)
+        self.C = C
+        self.orc = orc
+
+    def p(self, name):
+        return self.orc.ptr(self.f[name])
+
+    def cij(self):
+        C = self.C
+        return (C.c_void_p * 6)(*[self.f[k].ctypes.data for k in ("c11", "c12", "c13", "c22", "c23", "c33")])
+
+    def dv(self):
+        C = self.C
+        return (C.c_void_p * 6)(*[self.f[k].ctypes.data for k in ("dV11", "dV12", "dV13", "dV22", "dV23", "dV33")])
+
+
+def _answers():
+    return json.load(open(os.path.join(GOLDEN, "ve_known_answers.json")))
+
+
+def _num(s):
+    return float(s)
+
+
+def test_ve_known_answers_restated(orc):
+    import ctypes as C
+    fx = VeFixture(orc)
+    lib, K, nb, box, cnt = fx.lib, fx.K, fx.nb, fx.box, fx.n - 1
+    ans = _answers()
+    ptr = orc.ptr
+
+    # XMass (ve.cpp:240-249)
+    xmass = lib.orc_xmass(0, K, C.byref(box), ptr(nb), cnt, fx.p("x"), fx.p("y"), fx.p("z"), fx.p("h"), fx.p("m"),
+                          ptr(fx.wh))
+    rho0i = fx.mpart / xmass
+    e = ans["XMass"]
+    assert abs(rho0i - _num(e[0]["expected"])) < _num(e[0]["tol"])
+    assert abs(xmass - fx.mpart / fx.f["rho0"][0]) < fx.mpart / fx.f["rho0"][0] * 1e-7
+
+    # VeDefGradh (ve.cpp:229-238)
+    kx, gradh = C.c_double(), C.c_double()
+    lib.orc_ve_def_gradh(0, K, C.byref(box), ptr(nb), cnt, fx.p("x"), fx.p("y"), fx.p("z"), fx.p("h"), fx.p("m"),
+                         ptr(fx.wh), ptr(fx.whd), fx.p("xm"), C.byref(kx), C.byref(gradh))
+    got = {"density": kx.value * fx.mpart / fx.f["xm"][0], "gradh": gradh.value, "kx": kx.value}
+    for e in ans["VeDefGradh"]:
+        assert abs(got[e["quantity"]] - _num(e["expected"])) < _num(e["tol"]), e
+
+    # IAD (ve.cpp:141-156)
+    c6 = (C.c_double * 6)()
+    lib.orc_iad(0, K, C.byref(box), ptr(nb), cnt, fx.p("x"), fx.p("y"), fx.p("z"), fx.p("h"), ptr(fx.wh), fx.p("xm"),
+                fx.p("kx"), c6)
+    for k, e in enumerate(ans["IAD"]):
+        assert abs(c6[k] - _num(e["expected"])) < _num(e["tol"]), e
+
+    # divv / curlv (ve.cpp:122-139)
+    dv = (C.c_double * 6)()
+    divv, curlv = C.c_double(), C.c_double()
+    lib.orc_divv_curlv(0, K, C.byref(box), ptr(nb), cnt, fx.p("x"), fx.p("y"), fx.p("z"), fx.p("vx"), fx.p("vy"),
+                       fx.p("vz"), fx.p("h"), fx.cij(), ptr(fx.wh), fx.p("kx"), fx.p("xm"), C.byref(divv),
+                       C.byref(curlv), dv)
+    got = {"divv": divv.value, "curlv": curlv.value, "dV11": dv[0], "dV12": dv[1], "dV13": dv[2], "dV22": dv[3],
+           "dV23": dv[4], "dV33": dv[5]}
+    for e in ans["Divv_Curlv"]:
+        assert abs(got[e["quantity"]] - _num(e["expected"])) < _num(e["tol"]), e
+
+    # AV switches (ve.cpp:112-120), dt 0.3
+    alpha = lib.orc_av_switches(0, K, C.byref(box), ptr(nb), cnt, fx.p("x"), fx.p("y"), fx.p("z"), fx.p("vx"),
+                                fx.p("vy"), fx.p("vz"), fx.p("h"), fx.p("c"), fx.cij(), ptr(fx.wh), fx.p("kx"),
+                                fx.p("xm"), fx.p("divv"), 0.3, 0.05, 1.0, 0.2, fx.f["alpha"][0])
+    e = ans["AVSwitches"][0]
+    assert abs(alpha - _num(e["expected"])) < _num(e["tol"])
+
+    # momentum-energy with and without AV cleaning, and without neighbours (ve.cpp:172-227)
+    for block, clean, count in ((1, 1, cnt), (2, 0, cnt), (3, 0, 0)):
+        out = (C.c_double * 5)()
+        lib.orc_momentum_energy(0, clean, K, C.byref(box), ptr(nb), count, fx.p("x"), fx.p("y"), fx.p("z"),
+                                fx.p("vx"), fx.p("vy"), fx.p("vz"), fx.p("h"), fx.p("m"), fx.p("prho"), fx.p("c"),
+                                fx.cij(), 0.1, 0.2, 1.0 / (0.2 - 0.1), ptr(fx.wh), fx.p("kx"), fx.p("xm"),
+                                fx.p("alpha"), fx.dv(), out)
+        got = {"grad_Px": out[0], "grad_Py": out[1], "grad_Pz": out[2], "du": out[3], "maxvsignal": out[4]}
+        for e in (e for e in ans["MomentumEnergy"] if e["block"] == block):
+            tol = _num(e["tol"])
+            if tol == 0:
+                assert got[e["quantity"]] == _num(e["expected"]), e
+            else:
+                assert abs(got[e["quantity"]] - _num(e["expected"])) < tol, (e, got[e["quantity"]])
+
+
+def test_kernel_tables_normalisation(orc):
+    """K by Simpson integration lies close to the SPHYNX fit (sph/test/table_creation.cpp:17-40 compares both)."""
+    K, wh, whd = orc.tables(6.0)
+    K_fit = orc.load().orc_sphynx_3d_k(6.0)
+    assert abs(K - K_fit) / K_fit < 2e-3
+    assert wh[0] == 1.0 and abs(wh[-1]) < 1e-30 and whd[0] == 0.0
+
+
+# ----------------------------------------------------------------------------------------------------------------
+# SFC keys, sort, tree, neighbours
+# ----------------------------------------------------------------------------------------------------------------
+
+def test_hilbert_roundtrip_and_continuity(orc):
+    import ctypes as C
+    lib = orc.load()
+    rng = np.random.default_rng(5)
+    for _ in range(2000):
+        x, y, z = (int(v) for v in rng.integers(0, 2 ** 21, 3))
+        k = lib.orc_hilbert(x, y, z)
+        a, b, c = C.c_uint(), C.c_uint(), C.c_uint()
+        lib.orc_hilbert_decode(k, C.byref(a), C.byref(b), C.byref(c))
+        assert (a.value, b.value, c.value) == (x, y, z)
+    # consecutive keys are face neighbours of the finest grid (hilbert.cpp continuity test)
+    start = int(rng.integers(0, 2 ** 60))
+    prev = None
+    for k in range(start, start + 4096):
+        a, b, c = C.c_uint(), C.c_uint(), C.c_uint()
+        lib.orc_hilbert_decode(k, C.byref(a), C.byref(b), C.byref(c))
+        p = np.array([a.value, b.value, c.value], dtype=np.int64)
+        if prev is not None:
+            assert np.abs(p - prev).sum() == 1
+        prev = p
+    # the eight level-1 octants follow the Hilbert order 0 1 3 2 7 6 4 5 of the Morton octants
+    order = [lib.orc_hilbert(((o >> 2) & 1) << 20, ((o >> 1) & 1) << 20, (o & 1) << 20) >> 60 for o in range(8)]
+    assert order == [0, 1, 3, 2, 7, 6, 4, 5]
+
+
+def _ref():
+    from oracle import refsim
+    if not refsim.available():
+        pytest.skip("reference oracle not built")
+    return refsim
+
+
+def test_keys_sort_tree_vs_reference(orc):
+    ref = _ref()
+    rng = np.random.default_rng(9)
+    n = 50_000
+    x = rng.normal(0, 0.2, n).clip(-0.5, 0.5)
+    y = rng.uniform(-0.5, 0.5, n)
+    z = rng.uniform(-0.5, 0.5, n)
+    lim = (-0.5, 0.5, -0.5, 0.5, -0.5, 0.5)
+    k_orc = orc.sfc_keys(x, y, z, lim, True)
+    assert np.array_equal(k_orc, ref.sfc_keys(x, y, z, lim, True))
+    ks, perm = orc.sort_by_key(k_orc)
+    assert np.array_equal(perm, np.argsort(k_orc, kind="stable").astype(np.uint32))
+    for bucket in (16, 64, 500):
+        lo, co = orc.compute_octree(ks, bucket)
+        lr, cr = ref.compute_octree(ks, bucket)
+        assert np.array_equal(lo, lr) and np.array_equal(co, cr)
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+def test_neighbors_vs_reference(orc, periodic):
+    ref = _ref()
+    rng = np.random.default_rng(2)
+    n = 4000
+    pts = rng.uniform(-0.5, 0.5, (3, n))
+    lim = (-0.5, 0.5, -0.5, 0.5, -0.5, 0.5)
+    keys = orc.sfc_keys(*pts, lim, periodic)
+    order = np.argsort(keys, kind="stable")
+    keys = keys[order]
+    x, y, z = (np.ascontiguousarray(p[order]) for p in pts)
+    h = rng.uniform(0.03, 0.07, n)
+    ngmax = 150
+    nr, cr = ref.find_neighbors(keys, x, y, z, h, lim, periodic, ngmax)
+    no, co, _ = orc.find_neighbors(x, y, z, h, lim, periodic, 100, ngmax, iterate=False)
+    assert np.array_equal(co - 1, cr)
+    for i in range(n):
+        k = min(int(cr[i]), ngmax)
+        assert np.array_equal(no[i, :k], nr[i, :k]), i
+
+
+# ----------------------------------------------------------------------------------------------------------------
+# whole steps against the recorded reference outputs
+# ----------------------------------------------------------------------------------------------------------------
+
+@pytest.mark.parametrize("case", ["sedov12", "noh14"])
+def test_oracle_step_vs_recorded_reference(orc, case):
+    from sphexa_b200 import ic as icm
+    g = np.load(os.path.join(GOLDEN, f"{case}_ref.npz"))
+    ic = icm.sedov(12) if case == "sedov12" else icm.noh(14)
+    s = orc.OracleSim(ic)
+    assert np.array_equal(s.keys(), g["init_keys"])
+    assert np.array_equal(s.get("id"), g["init_id"])
+    s.compute_forces()
+    assert np.array_equal(s.keys(), g["keys"])
+    assert np.array_equal(s.get("nc").astype(np.uint32), g["f_nc"].astype(np.uint32))
+    nb = s.neighbors()
+    nc = g["f_nc"].astype(np.int64)
+    flat = np.concatenate([nb[i, :min(nc[i] - 1, nb.shape[1])] for i in range(s.n)])
+    assert np.array_equal(flat, g["nbr"])
+    for f in ("h", "xm", "kx", "gradh", "prho", "c", "c11", "c22", "c33", "divv", "curlv", "alpha", "ax", "ay", "az",
+              "du"):
+        a, b = s.get(f), g["f_" + f]
+        scale = np.max(np.abs(b))
+        assert np.max(np.abs(a - b)) <= 1e-12 * scale + 1e-300, f
+    s.integrate()
+    for f in ("x", "y", "z", "h", "temp", "vx", "vy", "vz"):
+        a, b = s.get(f), g["s_" + f]
+        scale = max(np.max(np.abs(b)), 1e-300)
+        assert np.max(np.abs(a - b)) <= 1e-12 * scale, f
+
+
+def test_oracle_multi_step_vs_reference(orc):
+    ref = _ref()
+    from sphexa_b200 import ic as icm
+    ic = icm.sedov(14)
+    r = ref.RefSim(ic)
+    s = orc.OracleSim(ic)
+    for _ in range(3):
+        r.step()
+        s.step()
+    assert np.array_equal(s.keys(), r.keys())
+    for f in ("x", "y", "z", "h", "temp", "vx", "alpha"):
+        a, b = s.get(f), r.get(f)
+        assert np.max(np.abs(a - b)) <= 1e-12 * max(np.max(np.abs(b)), 1e-300), f
+    sr, so = r.scalars(), s.scalars()
+    for k in ("minDt", "ttot", "etot"):
+        assert abs(so[k] - sr[k]) <= 1e-12 * abs(sr[k]), k
