@@ -23,11 +23,16 @@ struct HydroConsts
     int usePoly;
     float wpoly[kPolyTerms];
     float dwpoly[kPolyTerms];
+    // FP32 path only: length of one unit of the 32-bit fixed-point coordinates, per axis (box length / 2^32)
+    float qscale[3];
 };
 
 /*! Per-particle neighbour-side records, written by the stage that produces the values and gathered once per
  *  neighbour by the next stages (one 16-byte-aligned record instead of one scattered load per field).
- *  pos:   x, y, z, m            (double, every stage)
+ *  pos:   x, y, z, m            (double; FP64 path)
+ *  posq:  qx, qy, qz, m         (FP32 path: coordinates as 32-bit fixed point over the box, q = (x - lo) 2^32 / L,
+ *                                m as float bits; the int32 difference of two q is the pair separation in units of
+ *                                L / 2^32, wrapped to the nearest periodic image by integer overflow)
  *  hydro: vx, vy, vz, 1/h, xm, xm/kx, c, prho   (T; written by VeDefGradh+EOS)
  *  grad:  c11, c12, c13, c22, c23, c33, divv, alpha   (T; c_ij and divv by IAD, alpha by the AV switches) */
 template<class T>
@@ -47,7 +52,8 @@ template<class T>
 struct ChainArrays
 {
     size_t n;
-    const double4* pos;       // x, y, z, m
+    const double4* pos;       // x, y, z, m (FP64 path)
+    const int4* posq;         // fixed-point x, y, z and float m (FP32 path)
     const double* h;          // smoothing length (FP64 state)
     const double* vx;
     const double* vy;

@@ -3,12 +3,13 @@
 // neighbour lists are read slot-major (one coalesced line per slot). Each J-loop walks the list in stored (ascending)
 // order, like the reference CPU loops, and reads neighbour data through the packed records of hydro.cuh.
 //
-// T = double: plain FP64 drop-in. T = float: the mixed form — pair geometry is formed in FP64 (x_i - x_j with the
-// periodic shift) and then rounded to FP32, all pair arithmetic is FP32, and every neighbour sum is a compensated
-// (Kahan) FP32 sum.
+// T = double: the plain FP64 drop-in. Positions are FP64, the periodic shift is the reference's, sums run in list
+// order with the reference's expression order, so results differ from the reference CPU only by FMA contraction.
 //
-// Per-pair formulas follow the reference J-loops cited at each kernel; the order of operations inside each
-// expression is kept, so FP64 results differ from the reference CPU only by FMA contraction.
+// T = float: the mixed form. Pair separations come from 32-bit fixed-point coordinates (exact integer differences,
+// periodic wrap by overflow; one unit = L / 2^32), all pair arithmetic is FP32, the kernel W is a degree-12
+// polynomial instead of a table, and every neighbour sum is block-compensated: plain FP32 partial sums over blocks of
+// 8 neighbours, each added to a Kahan-compensated FP32 accumulator.
 #include "hydro.cuh"
 #include "neighbors.cuh"
 #include "primitives.cuh"
@@ -21,40 +22,51 @@ namespace
 
 constexpr int kChainThreads = 128;
 
+/*! Neighbour-sum accumulator. FP64: every term is added as it comes, in list order (the reference's order).
+ *  FP32: terms are summed plainly within one list chunk of 8 neighbours and each chunk sum is added to a
+ *  Kahan-compensated accumulator; explicit round-to-nearest intrinsics keep the compiler from fusing or reordering
+ *  the compensation. */
 template<class T>
-struct Sum;
+struct BlockSum;
 
 template<>
-struct Sum<double>
+struct BlockSum<double>
 {
     double s;
-    __device__ explicit Sum(double v = 0.0)
+    __device__ explicit BlockSum(double v = 0.0)
         : s(v)
     {
     }
     __device__ void add(double v) { s += v; }
+    __device__ void flush() {}
     __device__ double get() const { return s; }
 };
 
-//! Kahan-compensated FP32 sum; explicit round-to-nearest intrinsics keep the compiler from fusing or reordering
 template<>
-struct Sum<float>
+struct BlockSum<float>
 {
-    float s, comp;
-    __device__ explicit Sum(float v = 0.f)
+    float s, comp, part;
+    __device__ explicit BlockSum(float v = 0.f)
         : s(v)
         , comp(0.f)
+        , part(0.f)
     {
     }
-    __device__ void add(float v)
+    __device__ void add(float v) { part += v; }
+    __device__ void flush()
     {
-        float y = __fsub_rn(v, comp);
+        float y = __fsub_rn(part, comp);
         float t = __fadd_rn(s, y);
         comp    = __fsub_rn(__fsub_rn(t, s), y);
         s       = t;
+        part    = 0.f;
     }
     __device__ float get() const { return s; }
 };
+
+//! a / b: IEEE division in FP64 (the reference's rounding), the fast 2-ulp reciprocal-multiply in FP32
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
 //! linear interpolation in a 20000-entry table on [0, 2] (sph/include/sph/table_lookup.hpp:14-26)
 template<class T>
@@ -134,6 +146,64 @@ __device__ __forceinline__ double4 ldg4(const double4* p)
     return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// positions and pair separations per precision
+// ---------------------------------------------------------------------------------------------------------------
+
+template<class T>
+struct Pos;
+
+template<>
+struct Pos<double>
+{
+    double x, y, z, m;
+};
+
+template<>
+struct Pos<float>
+{
+    int x, y, z;
+    float m;
+};
+
+__device__ __forceinline__ Pos<double> posOf(const ChainArrays<double>& a, size_t j)
+{
+    double4 v = ldg4(a.pos + j);
+    return {v.x, v.y, v.z, v.w};
+}
+
+__device__ __forceinline__ Pos<float> posOf(const ChainArrays<float>& a, size_t j)
+{
+    int4 v = __ldg(a.posq + j);
+    return {v.x, v.y, v.z, __int_as_float(v.w)};
+}
+
+template<class T>
+struct Sep
+{
+    T rx, ry, rz;
+};
+
+//! x_i - x_j with the reference's periodic shift (threshold r = 2 h_i), FP64
+__device__ __forceinline__ Sep<double> separation(const Pos<double>& pi, const Pos<double>& pj, double r,
+                                                  const DevBox& box, const HydroConsts<double>&)
+{
+    double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
+    shiftPbc(rx, ry, rz, r, box);
+    return {rx, ry, rz};
+}
+
+//! x_i - x_j from fixed-point coordinates: an exact integer difference, wrapped to the nearest image on periodic
+//! axes, rounded once to FP32
+__device__ __forceinline__ Sep<float> separation(const Pos<float>& pi, const Pos<float>& pj, double,
+                                                 const DevBox&, const HydroConsts<float>& k)
+{
+    int dx = int(unsigned(pi.x) - unsigned(pj.x));
+    int dy = int(unsigned(pi.y) - unsigned(pj.y));
+    int dz = int(unsigned(pi.z) - unsigned(pj.z));
+    return {float(dx) * k.qscale[0], float(dy) * k.qscale[1], float(dz) * k.qscale[2]};
+}
+
 template<class T>
 __device__ __forceinline__ HydroRec<T> loadHydro(const HydroRec<T>* p)
 {
@@ -178,6 +248,7 @@ struct Target
     size_t group;
     unsigned lane;
     unsigned count;
+    unsigned ngPad;
 };
 
 __device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned ngmax, Target& t)
@@ -187,12 +258,24 @@ __device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned 
     t.group = t.i >> 5;
     t.lane  = unsigned(t.i & 31);
     t.count = min(nc[t.i] - 1u, ngmax);
+    t.ngPad = paddedNgmax(ngmax);
     return true;
 }
 
-__device__ __forceinline__ uint32_t neighborAt(const uint32_t* nidx, const Target& t, unsigned ngmax, unsigned k)
+//! the 8 neighbour indices of list chunk q0 / 8 of the target (two 16-byte loads of one sector)
+__device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t, unsigned ngPad, unsigned q0,
+                                          uint32_t (&js)[kNbChunk])
 {
-    return __ldg(nidx + nidxSlot(t.group, ngmax, k, t.lane));
+    const uint4* p = reinterpret_cast<const uint4*>(nidx + nidxAt(t.group, ngPad, q0, t.lane));
+    uint4 a = __ldg(p), b = __ldg(p + 1);
+    js[0] = a.x;
+    js[1] = a.y;
+    js[2] = a.z;
+    js[3] = a.w;
+    js[4] = b.x;
+    js[5] = b.y;
+    js[6] = b.z;
+    js[7] = b.w;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -203,25 +286,30 @@ __global__ void __launch_bounds__(kChainThreads) xmassKernel(ChainArrays<T> a, H
 {
     Target t;
     if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
-    double4 pi = a.pos[t.i];
+    Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
-    T mi       = T(pi.w);
+    T mi       = T(pi.m);
     T hInv     = T(1.0) / hi;
     T h3Inv    = hInv * hInv * hInv;
 
-    Sum<T> rho0(mi);
-#pragma unroll 4
-    for (unsigned q = 0; q < t.count; ++q)
+    BlockSum<T> rho0(mi);
+    for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
     {
-        uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
-        double4 pj = ldg4(a.pos + j);
-        double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
-        shiftPbc(rx, ry, rz, 2.0 * hiD, box);
-        T fx = T(rx), fy = T(ry), fz = T(rz);
-        T dist = sqrt(fx * fx + fy * fy + fz * fz);
-        T w    = kernelW(a.wh, k, dist * hInv);
-        rho0.add(w * T(pj.w));
+        uint32_t js[kNbChunk];
+        loadChunk(a.nidx, t, t.ngPad, q0, js);
+        unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+        for (unsigned q = 0; q < kNbChunk; ++q)
+        {
+            if (q >= qn) { break; }
+            uint32_t j = js[q];
+            Pos<T> pj  = posOf(a, j);
+            Sep<T> r   = separation(pi, pj, 2.0 * hiD, box, k);
+            T dist     = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+            rho0.add(kernelW(a.wh, k, dist * hInv) * T(pj.m));
+        }
+        rho0.flush();
     }
     a.xm[t.i] = mi / (rho0.get() * k.K * h3Inv);
 }
@@ -235,32 +323,40 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays
 {
     Target t;
     if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
-    double4 pi  = a.pos[t.i];
-    double hiD  = a.h[t.i];
-    T hi        = T(hiD);
-    T mi        = T(pi.w);
-    T xmassi    = a.xm[t.i];
-    T hInv      = T(1) / hi;
-    T h3Inv     = hInv * hInv * hInv;
+    Pos<T> pi  = posOf(a, t.i);
+    double hiD = a.h[t.i];
+    T hi       = T(hiD);
+    T mi       = T(pi.m);
+    T xmassi   = a.xm[t.i];
+    T hInv     = T(1) / hi;
+    T h3Inv    = hInv * hInv * hInv;
 
-    Sum<T> kxS(xmassi), whomegaS(-T(3) * xmassi), wrho0S(-T(3) * mi);
-#pragma unroll 4
-    for (unsigned q = 0; q < t.count; ++q)
+    BlockSum<T> kxS(xmassi), whomegaS(-T(3) * xmassi), wrho0S(-T(3) * mi);
+    for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
     {
-        uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
-        double4 pj = ldg4(a.pos + j);
-        double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
-        shiftPbc(rx, ry, rz, 2.0 * hiD, box);
-        T fx = T(rx), fy = T(ry), fz = T(rz);
-        T dist   = sqrt(fx * fx + fy * fy + fz * fz);
-        T vloc   = dist * hInv;
-        T w      = kernelW(a.wh, k, vloc);
-        T dw     = kernelDW(a.whd, k, vloc);
-        T dterh  = -(T(3) * w + vloc * dw);
-        T xmassj = __ldg(a.xm + j);
-        kxS.add(w * xmassj);
-        whomegaS.add(dterh * xmassj);
-        wrho0S.add(dterh * T(pj.w));
+        uint32_t js[kNbChunk];
+        loadChunk(a.nidx, t, t.ngPad, q0, js);
+        unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+        for (unsigned q = 0; q < kNbChunk; ++q)
+        {
+            if (q >= qn) { break; }
+            uint32_t j = js[q];
+            Pos<T> pj  = posOf(a, j);
+            Sep<T> r   = separation(pi, pj, 2.0 * hiD, box, k);
+            T dist     = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+            T vloc     = dist * hInv;
+            T w        = kernelW(a.wh, k, vloc);
+            T dw       = kernelDW(a.whd, k, vloc);
+            T dterh    = -(T(3) * w + vloc * dw);
+            T xmassj   = __ldg(a.xm + j);
+            kxS.add(w * xmassj);
+            whomegaS.add(dterh * xmassj);
+            wrho0S.add(dterh * T(pj.m));
+        }
+        kxS.flush();
+        whomegaS.flush();
+        wrho0S.flush();
     }
     T kxi      = kxS.get() * (k.K * h3Inv);
     T whomegai = whomegaS.get() * (k.K * h3Inv * hInv);
@@ -282,7 +378,8 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays
     a.gradh[t.i] = gradhi;
     a.prho[t.i]  = T(prho);
     a.c[t.i]     = T(c);
-    a.hrec[t.i]  = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), T(1) / hi, xmassi, xmassi / kxi, T(c), T(prho)};
+    a.hrec[t.i]  = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), T(1) / hi, xmassi, xmassi / kxi, T(c),
+                              T(prho)};
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -299,34 +396,45 @@ template<class T>
 __global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid = targetOf(a.n, a.nc, k.ngmax, t);
+    bool valid     = targetOf(a.n, a.nc, k.ngmax, t);
     double divvOut = -INFINITY;
     if (valid)
     {
-        double4 pi = a.pos[t.i];
+        Pos<T> pi  = posOf(a, t.i);
         double hiD = a.h[t.i];
         T hi       = T(hiD);
         T hiInv    = T(1) / hi;
 
-        Sum<T> s11, s12, s13, s22, s23, s33;
-#pragma unroll 4
-        for (unsigned q = 0; q < t.count; ++q)
+        BlockSum<T> s11, s12, s13, s22, s23, s33;
+        for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
         {
-            uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
-            double4 pj = ldg4(a.pos + j);
-            HydroRec<T> hj = loadHydro(a.hrec + j);
-            double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
-            shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
-            T rx = T(rxD), ry = T(ryD), rz = T(rzD);
-            T dist   = sqrt(rx * rx + ry * ry + rz * rz);
-            T w      = kernelW(a.wh, k, dist * hiInv);
-            T voljW  = hj.vol * w;
-            s11.add(rx * rx * voljW);
-            s12.add(rx * ry * voljW);
-            s13.add(rx * rz * voljW);
-            s22.add(ry * ry * voljW);
-            s23.add(ry * rz * voljW);
-            s33.add(rz * rz * voljW);
+            uint32_t js[kNbChunk];
+            loadChunk(a.nidx, t, t.ngPad, q0, js);
+            unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+            for (unsigned q = 0; q < kNbChunk; ++q)
+            {
+                if (q >= qn) { break; }
+                uint32_t j = js[q];
+                Pos<T> pj      = posOf(a, j);
+                HydroRec<T> hj = loadHydro(a.hrec + j);
+                Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+                T dist         = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+                T w            = kernelW(a.wh, k, dist * hiInv);
+                T voljW        = hj.vol * w;
+                s11.add(r.rx * r.rx * voljW);
+                s12.add(r.rx * r.ry * voljW);
+                s13.add(r.rx * r.rz * voljW);
+                s22.add(r.ry * r.ry * voljW);
+                s23.add(r.ry * r.rz * voljW);
+                s33.add(r.rz * r.rz * voljW);
+            }
+            s11.flush();
+            s12.flush();
+            s13.flush();
+            s22.flush();
+            s23.flush();
+            s33.flush();
         }
         T tau11 = s11.get(), tau12 = s12.get(), tau13 = s13.get();
         T tau22 = s22.get(), tau23 = s23.get(), tau33 = s33.get();
@@ -352,45 +460,55 @@ __global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<
         HydroRec<T> hrI = a.hrec[t.i];
         T vxi = hrI.vx, vyi = hrI.vy, vzi = hrI.vz;
         T kxi = a.kx[t.i];
-        Sum<T> dVxx, dVxy, dVxz, dVyx, dVyy, dVyz, dVzx, dVzy, dVzz;
-#pragma unroll 4
-        for (unsigned q = 0; q < t.count; ++q)
+        BlockSum<T> dVxx, dVxy, dVxz, dVyx, dVyy, dVyz, dVzx, dVzy, dVzz;
+        for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
         {
-            uint32_t j = neighborAt(a.nidx, t, k.ngmax, q);
-            double4 pj = ldg4(a.pos + j);
-            HydroRec<T> hj = loadHydro(a.hrec + j);
-            double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
-            shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
-            T rx = T(rxD), ry = T(ryD), rz = T(rzD);
-            T r2    = rx * rx + ry * ry + rz * rz;
-            T dist  = sqrt(r2);
-            T vxji  = hj.vx - vxi;
-            T vyji  = hj.vy - vyi;
-            T vzji  = hj.vz - vzi;
-            T Wi    = kernelW(a.wh, k, dist * hiInv);
-            T tA0   = -(c11i * rx + c12i * ry + c13i * rz) * Wi;
-            T tA1   = -(c12i * rx + c22i * ry + c23i * rz) * Wi;
-            T tA2   = -(c13i * rx + c23i * ry + c33i * rz) * Wi;
-            T fx    = vxji * hj.xm;
-            T fy    = vyji * hj.xm;
-            T fz    = vzji * hj.xm;
-            dVxx.add(fx * tA0);
-            dVxy.add(fx * tA1);
-            dVxz.add(fx * tA2);
-            dVyx.add(fy * tA0);
-            dVyy.add(fy * tA1);
-            dVyz.add(fy * tA2);
-            dVzx.add(fz * tA0);
-            dVzy.add(fz * tA1);
-            dVzz.add(fz * tA2);
+            uint32_t js[kNbChunk];
+            loadChunk(a.nidx, t, t.ngPad, q0, js);
+            unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+            for (unsigned q = 0; q < kNbChunk; ++q)
+            {
+                if (q >= qn) { break; }
+                uint32_t j = js[q];
+                Pos<T> pj      = posOf(a, j);
+                HydroRec<T> hj = loadHydro(a.hrec + j);
+                Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+                T dist         = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+                T Wi           = kernelW(a.wh, k, dist * hiInv);
+                T tA0          = -(c11i * r.rx + c12i * r.ry + c13i * r.rz) * Wi;
+                T tA1          = -(c12i * r.rx + c22i * r.ry + c23i * r.rz) * Wi;
+                T tA2          = -(c13i * r.rx + c23i * r.ry + c33i * r.rz) * Wi;
+                T fx           = (hj.vx - vxi) * hj.xm;
+                T fy           = (hj.vy - vyi) * hj.xm;
+                T fz           = (hj.vz - vzi) * hj.xm;
+                dVxx.add(fx * tA0);
+                dVxy.add(fx * tA1);
+                dVxz.add(fx * tA2);
+                dVyx.add(fy * tA0);
+                dVyy.add(fy * tA1);
+                dVyz.add(fy * tA2);
+                dVzx.add(fz * tA0);
+                dVzy.add(fz * tA1);
+                dVzz.add(fz * tA2);
+            }
+            dVxx.flush();
+            dVxy.flush();
+            dVxz.flush();
+            dVyx.flush();
+            dVyy.flush();
+            dVyz.flush();
+            dVzx.flush();
+            dVzy.flush();
+            dVzz.flush();
         }
-        T hiInv3  = hiInv * hiInv * hiInv;
-        T normKx  = k.K * hiInv3 / kxi;
-        T divv    = normKx * (dVxx.get() + dVyy.get() + dVzz.get());
-        T cx      = dVzy.get() - dVyz.get();
-        T cy      = dVxz.get() - dVzx.get();
-        T cz      = dVyx.get() - dVxy.get();
-        T curlv   = normKx * sqrt(cx * cx + cy * cy + cz * cz);
+        T hiInv3 = hiInv * hiInv * hiInv;
+        T normKx = k.K * hiInv3 / kxi;
+        T divv   = normKx * (dVxx.get() + dVyy.get() + dVzz.get());
+        T cx     = dVzy.get() - dVyz.get();
+        T cy     = dVxz.get() - dVzx.get();
+        T cz     = dVyx.get() - dVxy.get();
+        T curlv  = normKx * sqrt(cx * cx + cy * cy + cz * cz);
 
         a.cij[0][t.i] = c11i;
         a.cij[1][t.i] = c12i;
@@ -433,7 +551,7 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
 {
     Target t;
     if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
-    double4 pi     = a.pos[t.i];
+    Pos<T> pi      = posOf(a, t.i);
     double hiD     = a.h[t.i];
     HydroRec<T> hr = a.hrec[t.i];
     GradRec<T> gr  = a.grec[t.i];
@@ -442,37 +560,41 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
     T vijsignalI   = T(1.e-40) * ci;
     T hiInv        = T(1) / hi;
     T hiInv3       = hiInv * hiInv * hiInv;
+    T KhiInv3      = k.K * hiInv3;
     T divvI        = gr.divv;
 
-    Sum<T> gx, gy, gz;
-#pragma unroll 4
-    for (unsigned q = 0; q < t.count; ++q)
+    BlockSum<T> gx, gy, gz;
+    for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
     {
-        uint32_t j     = neighborAt(a.nidx, t, k.ngmax, q);
-        double4 pj     = ldg4(a.pos + j);
-        HydroRec<T> hj = loadHydro(a.hrec + j);
-        GradRec<T> gj  = loadGrad(a.grec + j);
-        double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
-        shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
-        T rx = T(rxD), ry = T(ryD), rz = T(rzD);
-        T r2   = rx * rx + ry * ry + rz * rz;
-        T dist = sqrt(r2);
-        T vxij = hr.vx - hj.vx;
-        T vyij = hr.vy - hj.vy;
-        T vzij = hr.vz - hj.vz;
-        T rv   = rx * vxij + ry * vyij + rz * vzij;
-        T vsig = T(0);
-        if (rv < T(0)) { vsig = ci + hj.c - T(3) * rv / dist; }
-        vijsignalI = vijsignalI > vsig ? vijsignalI : vsig;
-        T Wi   = k.K * hiInv3 * kernelW(a.wh, k, dist * hiInv);
-        T tA1  = -(gr.c11 * rx + gr.c12 * ry + gr.c13 * rz) * Wi;
-        T tA2  = -(gr.c12 * rx + gr.c22 * ry + gr.c23 * rz) * Wi;
-        T tA3  = -(gr.c13 * rx + gr.c23 * ry + gr.c33 * rz) * Wi;
-        T volj = hj.vol;
-        T fac  = volj * (divvI - gj.divv);
-        gx.add(fac * tA1);
-        gy.add(fac * tA2);
-        gz.add(fac * tA3);
+        uint32_t js[kNbChunk];
+        loadChunk(a.nidx, t, t.ngPad, q0, js);
+        unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+        for (unsigned q = 0; q < kNbChunk; ++q)
+        {
+            if (q >= qn) { break; }
+            uint32_t j = js[q];
+            Pos<T> pj      = posOf(a, j);
+            HydroRec<T> hj = loadHydro(a.hrec + j);
+            T divvJ        = __ldg(reinterpret_cast<const T*>(a.grec + j) + 6); // the divv slot of the record
+            Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+            T dist         = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+            T rv           = r.rx * (hr.vx - hj.vx) + r.ry * (hr.vy - hj.vy) + r.rz * (hr.vz - hj.vz);
+            T vsig         = T(0);
+            if (rv < T(0)) { vsig = ci + hj.c - fdiv(T(3) * rv, dist); }
+            vijsignalI = vijsignalI > vsig ? vijsignalI : vsig;
+            T Wi       = KhiInv3 * kernelW(a.wh, k, dist * hiInv);
+            T tA1      = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
+            T tA2      = -(gr.c12 * r.rx + gr.c22 * r.ry + gr.c23 * r.rz) * Wi;
+            T tA3      = -(gr.c13 * r.rx + gr.c23 * r.ry + gr.c33 * r.rz) * Wi;
+            T fac      = hj.vol * (divvI - divvJ);
+            gx.add(fac * tA1);
+            gy.add(fac * tA2);
+            gz.add(fac * tA3);
+        }
+        gx.flush();
+        gy.flush();
+        gz.flush();
     }
     T gdx      = gx.get(), gdy = gy.get(), gdz = gz.get();
     T graddivv = sqrt(gdx * gdx + gdy * gdy + gdz * gdz);
@@ -500,12 +622,6 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
 // (tsKCourant, kernels.hpp:10-17) reduced to the minimum.
 // ---------------------------------------------------------------------------------------------------------------
 template<class T>
-__device__ __forceinline__ T powT(T b, T e)
-{
-    return pow(b, e);
-}
-
-template<class T>
 __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
@@ -513,99 +629,107 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArray
     double dtMin = INFINITY;
     if (valid)
     {
-        double4 pi     = a.pos[t.i];
+        Pos<T> pi      = posOf(a, t.i);
         double hiD     = a.h[t.i];
         HydroRec<T> hr = a.hrec[t.i];
         GradRec<T> gr  = a.grec[t.i];
-        T hi      = T(hiD);
-        T mi      = T(pi.w);
-        T ci      = hr.c;
-        T kxi     = a.kx[t.i];
-        T alphaI  = gr.alpha;
-        T xmassi  = hr.xm;
-        T rhoi    = kxi * mi / xmassi;
-        T prhoi   = hr.prho;
-        T hiInv   = T(1) / hi;
-        T hiInv3  = hiInv * hiInv * hiInv;
+        T hi          = T(hiD);
+        T mi          = T(pi.m);
+        T ci          = hr.c;
+        T kxi         = a.kx[t.i];
+        T alphaI      = gr.alpha;
+        T xmassi      = hr.xm;
+        T rhoi        = kxi * mi / xmassi;
+        T prhoi       = hr.prho;
+        T hiInv       = T(1) / hi;
+        T hiInv3      = hiInv * hiInv * hiInv;
         T maxvsignalI = T(0);
-        Sum<T> momX, momY, momZ, energyS, aViscE;
+        BlockSum<T> momX, momY, momZ, energyS, aViscE;
 
-#pragma unroll 2
-        for (unsigned q = 0; q < t.count; ++q)
+        for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
         {
-            uint32_t j     = neighborAt(a.nidx, t, k.ngmax, q);
-            double4 pj     = ldg4(a.pos + j);
-            HydroRec<T> hj = loadHydro(a.hrec + j);
-            GradRec<T> gj  = loadGrad(a.grec + j);
-            double rxD = pi.x - pj.x, ryD = pi.y - pj.y, rzD = pi.z - pj.z;
-            shiftPbc(rxD, ryD, rzD, 2.0 * hiD, box);
-            T rx = T(rxD), ry = T(ryD), rz = T(rzD);
-            T r2    = rx * rx + ry * ry + rz * rz;
-            T dist  = sqrt(r2);
-            T vxij  = hr.vx - hj.vx;
-            T vyij  = hr.vy - hj.vy;
-            T vzij  = hr.vz - hj.vz;
-            T hjInv = hj.hInv;
-            T v1    = dist * hiInv;
-            T v2    = dist * hjInv;
-            T hjInv3 = hjInv * hjInv * hjInv;
-            T Wi    = hiInv3 * kernelW(a.wh, k, v1);
-            T Wj    = hjInv3 * kernelW(a.wh, k, v2);
-
-            T tA1i = -(gr.c11 * rx + gr.c12 * ry + gr.c13 * rz) * Wi;
-            T tA2i = -(gr.c12 * rx + gr.c22 * ry + gr.c23 * rz) * Wi;
-            T tA3i = -(gr.c13 * rx + gr.c23 * ry + gr.c33 * rz) * Wi;
-            T tA1j = -(gj.c11 * rx + gj.c12 * ry + gj.c13 * rz) * Wj;
-            T tA2j = -(gj.c12 * rx + gj.c22 * ry + gj.c23 * rz) * Wj;
-            T tA3j = -(gj.c13 * rx + gj.c23 * ry + gj.c33 * rz) * Wj;
-
-            T mj     = T(pj.w);
-            T cj     = hj.c;
-            T xmassj = hj.xm;
-            T rhoj   = mj / hj.vol;
-
-            T rv  = rx * vxij + ry * vyij + rz * vzij;
-            T wij = rv / dist;
-            T visc = T(0);
-            if (wij < T(0))
+            uint32_t js[kNbChunk];
+            loadChunk(a.nidx, t, t.ngPad, q0, js);
+            unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+            for (unsigned q = 0; q < kNbChunk; ++q)
             {
-                T vijSignal = (alphaI + gj.alpha) * T(0.25) * (ci + cj) - T(2) * wij;
-                visc        = -vijSignal * wij;
-            }
-            T vijsignal  = T(0.5) * (ci + cj) - T(2) * wij;
-            maxvsignalI  = vijsignal > maxvsignalI ? vijsignal : maxvsignalI;
+                if (q >= qn) { break; }
+                uint32_t j = js[q];
+                Pos<T> pj      = posOf(a, j);
+                HydroRec<T> hj = loadHydro(a.hrec + j);
+                GradRec<T> gj  = loadGrad(a.grec + j);
+                Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+                T dist         = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+                T vxij         = hr.vx - hj.vx;
+                T vyij         = hr.vy - hj.vy;
+                T vzij         = hr.vz - hj.vz;
+                T v1           = dist * hiInv;
+                T v2           = dist * hj.hInv;
+                T hjInv3       = hj.hInv * hj.hInv * hj.hInv;
+                T Wi           = hiInv3 * kernelW(a.wh, k, v1);
+                T Wj           = hjInv3 * kernelW(a.wh, k, v2);
 
-            T aMom, bMom;
-            T atwood = fabs(rhoi - rhoj) / (rhoi + rhoj);
-            if (atwood < k.Atmin)
-            {
-                aMom = xmassi * xmassi;
-                bMom = xmassj * xmassj;
-            }
-            else if (atwood > k.Atmax)
-            {
-                aMom = xmassi * xmassj;
-                bMom = aMom;
-            }
-            else
-            {
-                T sigma = k.ramp * (atwood - k.Atmin);
-                aMom    = powT(xmassi, T(2) - sigma) * powT(xmassj, sigma);
-                bMom    = powT(xmassj, T(2) - sigma) * powT(xmassi, sigma);
-            }
+                T tA1i = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
+                T tA2i = -(gr.c12 * r.rx + gr.c22 * r.ry + gr.c23 * r.rz) * Wi;
+                T tA3i = -(gr.c13 * r.rx + gr.c23 * r.ry + gr.c33 * r.rz) * Wi;
+                T tA1j = -(gj.c11 * r.rx + gj.c12 * r.ry + gj.c13 * r.rz) * Wj;
+                T tA2j = -(gj.c12 * r.rx + gj.c22 * r.ry + gj.c23 * r.rz) * Wj;
+                T tA3j = -(gj.c13 * r.rx + gj.c23 * r.ry + gj.c33 * r.rz) * Wj;
 
-            T aVisc  = mj / rhoi * visc;
-            T bVisc  = mj / rhoj * visc;
-            T aViscX = T(0.5) * (aVisc * tA1i + bVisc * tA1j);
-            T aViscY = T(0.5) * (aVisc * tA2i + bVisc * tA2j);
-            T aViscZ = T(0.5) * (aVisc * tA3i + bVisc * tA3j);
-            aViscE.add(aViscX * vxij + aViscY * vyij + aViscZ * vzij);
-            energyS.add(mj * aMom * (vxij * tA1i + vyij * tA2i + vzij * tA3i));
-            T momI = mj * prhoi * aMom;
-            T momJ = mj * hj.prho * bMom;
-            momX.add(momI * tA1i + momJ * tA1j + aViscX);
-            momY.add(momI * tA2i + momJ * tA2j + aViscY);
-            momZ.add(momI * tA3i + momJ * tA3j + aViscZ);
+                T mj     = T(pj.m);
+                T cj     = hj.c;
+                T xmassj = hj.xm;
+                T rhoj   = fdiv(mj, hj.vol);
+
+                T rv   = r.rx * vxij + r.ry * vyij + r.rz * vzij;
+                T wij  = fdiv(rv, dist);
+                T visc = T(0);
+                if (wij < T(0))
+                {
+                    T vijSignal = (alphaI + gj.alpha) * T(0.25) * (ci + cj) - T(2) * wij;
+                    visc        = -vijSignal * wij;
+                }
+                T vijsignal = T(0.5) * (ci + cj) - T(2) * wij;
+                maxvsignalI = vijsignal > maxvsignalI ? vijsignal : maxvsignalI;
+
+                T aMom, bMom;
+                T atwood = fdiv(fabs(rhoi - rhoj), rhoi + rhoj);
+                if (atwood < k.Atmin)
+                {
+                    aMom = xmassi * xmassi;
+                    bMom = xmassj * xmassj;
+                }
+                else if (atwood > k.Atmax)
+                {
+                    aMom = xmassi * xmassj;
+                    bMom = aMom;
+                }
+                else
+                {
+                    T sigma = k.ramp * (atwood - k.Atmin);
+                    aMom    = pow(xmassi, T(2) - sigma) * pow(xmassj, sigma);
+                    bMom    = pow(xmassj, T(2) - sigma) * pow(xmassi, sigma);
+                }
+
+                T aVisc  = fdiv(mj, rhoi) * visc;
+                T bVisc  = fdiv(mj, rhoj) * visc;
+                T aViscX = T(0.5) * (aVisc * tA1i + bVisc * tA1j);
+                T aViscY = T(0.5) * (aVisc * tA2i + bVisc * tA2j);
+                T aViscZ = T(0.5) * (aVisc * tA3i + bVisc * tA3j);
+                aViscE.add(aViscX * vxij + aViscY * vyij + aViscZ * vzij);
+                energyS.add(mj * aMom * (vxij * tA1i + vyij * tA2i + vzij * tA3i));
+                T momI = mj * prhoi * aMom;
+                T momJ = mj * hj.prho * bMom;
+                momX.add(momI * tA1i + momJ * tA1j + aViscX);
+                momY.add(momI * tA2i + momJ * tA2j + aViscY);
+                momZ.add(momI * tA3i + momJ * tA3j + aViscZ);
+            }
+            momX.flush();
+            momY.flush();
+            momZ.flush();
+            energyS.flush();
+            aViscE.flush();
         }
         T aViscEnergy = aViscE.get() > T(0) ? aViscE.get() : T(0);
         a.du[t.i] = double(k.K * (prhoi * energyS.get() + T(0.5) * aViscEnergy));

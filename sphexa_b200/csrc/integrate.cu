@@ -10,11 +10,27 @@ namespace sphb
 namespace
 {
 
+//! one coordinate as 32-bit fixed point over [lo, lo + 2^32 unit), unit = span / 2^32 (periodic: span = L, the value
+//! L wraps to 0; open: span = 2 L so that differences of up to L stay below half the range and never wrap)
+__device__ inline int quantiseFixed(double v, double lo, double invUnit)
+{
+    double q = (v - lo) * invUnit;
+    q        = q < 0.0 ? 0.0 : q;
+    unsigned long long u = (unsigned long long)(q + 0.5);
+    return int(unsigned(u & 0xffffffffull));
+}
+
 __global__ void packPosKernel(const double* x, const double* y, const double* z, const double* m, size_t n,
-                              double4* pos)
+                              double4* pos, int4* posq, FixedFrame fr)
 {
     size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-    if (i < n) { pos[i] = make_double4(x[i], y[i], z[i], m[i]); }
+    if (i >= n) { return; }
+    if (pos) { pos[i] = make_double4(x[i], y[i], z[i], m[i]); }
+    if (posq)
+    {
+        posq[i] = make_int4(quantiseFixed(x[i], fr.lo[0], fr.invUnit[0]), quantiseFixed(y[i], fr.lo[1], fr.invUnit[1]),
+                            quantiseFixed(z[i], fr.lo[2], fr.invUnit[2]), __float_as_int(float(m[i])));
+    }
 }
 
 //! fold a coordinate back into a periodic box once (cstone/sfc/box.hpp putInBox)
@@ -159,11 +175,24 @@ __global__ void minMaxKernel(const double* v, size_t n, unsigned long long* out)
 
 } // namespace
 
+FixedFrame fixedFrameOf(const DevBox& box)
+{
+    FixedFrame fr;
+    for (int k = 0; k < 3; ++k)
+    {
+        double span   = box.periodic[k] ? box.len[k] : 2.0 * box.len[k];
+        fr.lo[k]      = box.lo[k];
+        fr.invUnit[k] = 4294967296.0 / span;
+        fr.unit[k]    = span / 4294967296.0;
+    }
+    return fr;
+}
+
 int packPositions(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
-                  cudaStream_t s)
+                  int4* posq, const DevBox& box, cudaStream_t s)
 {
     if (n == 0) { return kOk; }
-    packPosKernel<<<ceilDiv(n, 256), 256, 0, s>>>(x, y, z, m, n, pos);
+    packPosKernel<<<ceilDiv(n, 256), 256, 0, s>>>(x, y, z, m, n, pos, posq, fixedFrameOf(box));
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

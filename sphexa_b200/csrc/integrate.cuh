@@ -18,8 +18,19 @@ struct IntegrateArrays
     const T *ax, *ay, *az;
 };
 
+//! the fixed-point frame of the FP32 J-loops: q = (x - lo) * invUnit, x - lo = q * unit
+struct FixedFrame
+{
+    double lo[3];
+    double invUnit[3];
+    double unit[3];
+};
+
+FixedFrame fixedFrameOf(const DevBox& box);
+
+//! pos = (x, y, z, m) in FP64 and/or posq = fixed-point (x, y, z) + float m; either pointer may be null
 int packPositions(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
-                  cudaStream_t s);
+                  int4* posq, const DevBox& box, cudaStream_t s);
 
 template<class T>
 int launchPositions(size_t n, const IntegrateArrays<T>& a, const DevBox& box, double dt, double dtm1, double cv,

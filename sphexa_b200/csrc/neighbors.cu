@@ -3,9 +3,12 @@
 // Per group: (1) the search box = union over the group's still-active particles of [x - 2h, x + 2h];
 // (2) a depth-first traversal of the focus octree in child (= SFC) order, warp-cooperative with 8 lanes testing the
 // 8 children of a node against the box (periodic axes use the minimum image), collecting overlapping leaves in
-// ascending order in shared memory; (3) the particles of those leaves are streamed 32 at a time through shared
-// memory and every lane tests them against its own particle with the exact FP64 distance of the reference
-// (cstone/findneighbors.hpp:33-51,77-147: squared minimum-image distance < (2h)^2, j != i).
+// ascending order in shared memory; (3) each buffered leaf is cut into the 8-particle SFC blocks it covers, every
+// block's bounding box (precomputed once per step) is tested against the search box 32 blocks at a time, and the
+// particles of surviving blocks are streamed 32 at a time through shared memory; (4) every lane tests the staged
+// candidates against its own particle, two candidates per packed FP32x2 instruction on coordinates relative to the
+// group centre, and runs the exact FP64 test of the reference (cstone/findneighbors.hpp:33-51,77-147: squared
+// minimum-image distance < (2h)^2, j != i) only for candidates within a narrow band around the radius.
 // Candidates arrive in ascending particle order, so each list equals the reference CPU list, which is also ascending
 // (depth-first octree traversal over SFC-ordered leaves), including which neighbours are kept when more than ngmax
 // qualify. The smoothing-length iteration of sph/include/sph/find_neighbors.hpp:10-41 is fused: lanes whose count
@@ -27,10 +30,18 @@ constexpr int kLeafCap   = 256; // candidate leaves buffered before they are str
 struct NbShared
 {
     int stack[kNbWarps][kStackCap];
-    int leaf[kNbWarps][kLeafCap];
-    int first[kNbWarps][kLeafCap];
-    int prefix[kNbWarps][kLeafCap + 1];
-    float4 cand[kNbWarps][kWarp]; // candidate position relative to the group centre (FP32) and its index
+    int leafFirst[kNbWarps][kLeafCap]; // first particle of each buffered leaf
+    int leafEnd[kNbWarps][kLeafCap];   // one past its last particle
+    int blkPre[kNbWarps][kLeafCap + 1]; // exclusive prefix of the number of blocks per buffered leaf
+    int pStart[kNbWarps][kWarp];       // surviving pieces (block and leaf intersections) of one round
+    int pPre[kNbWarps][kWarp + 1];     // exclusive prefix of their lengths
+    // staged candidates: position relative to the group centre (FP32, pairs loaded as float2) and index
+    alignas(16) float cx[kNbWarps][kWarp];
+    alignas(16) float cy[kNbWarps][kWarp];
+    alignas(16) float cz[kNbWarps][kWarp];
+    int cj[kNbWarps][kWarp];
+    // per lane: the neighbours of the list chunk being filled, written out as one 32-byte sector when full
+    alignas(16) uint32_t nbuf[kNbWarps][kWarp][kNbChunk];
 };
 
 /*! Half width of the band |d^2 - (2h)^2| < band * (2h)^2 in which the FP32 distance cannot decide and the exact FP64
@@ -60,6 +71,33 @@ __device__ inline double warpMax(double v)
     return v;
 }
 
+//! warp-wide exclusive prefix of one value per lane; *total receives the sum
+__device__ inline int warpExclusive(int v, int lane, int* total)
+{
+    int incl = v;
+#pragma unroll
+    for (int off = 1; off < kWarp; off <<= 1)
+    {
+        int t = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) { incl += t; }
+    }
+    *total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
+    return incl - v;
+}
+
+//! largest r in [0, n) with pre[r] <= t (pre ascending, pre[0] = 0 <= t)
+__device__ inline int findSlot(const int* pre, int n, int t)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 1)
+    {
+        int mid = (lo + hi) >> 1;
+        if (pre[mid] <= t) { lo = mid; }
+        else { hi = mid; }
+    }
+    return lo;
+}
+
 //! d folded to the nearest periodic image: d - L * rint(d / L), rounded like the reference's uncontracted CPU code
 __device__ inline double minImage(double d, double len, double ilen, int periodic)
 {
@@ -74,7 +112,7 @@ __device__ inline double updateH(unsigned ng0, unsigned nc, double h)
     return __dmul_rn(__dmul_rn(h, 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
 }
 
-__global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* __restrict__ x,
+__global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const double* __restrict__ x,
                                                                   const double* __restrict__ y,
                                                                   const double* __restrict__ z, double* h, size_t n,
                                                                   TreeView tree, DevBox box, NeighborParams prm,
@@ -82,29 +120,32 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
                                                                   unsigned* __restrict__ ncOut, unsigned* status)
 {
     __shared__ NbShared sh;
-    const int warp        = threadIdx.x / kWarp;
-    const int lane        = threadIdx.x & (kWarp - 1);
+    const int warp         = threadIdx.x / kWarp;
+    const int lane         = threadIdx.x & (kWarp - 1);
     const size_t numGroups = (n + kWarp - 1) / kWarp;
-    const size_t group    = size_t(blockIdx.x) * kNbWarps + warp;
+    const size_t group     = size_t(blockIdx.x) * kNbWarps + warp;
     if (group >= numGroups) { return; }
 
-    const size_t i  = group * kWarp + lane;
+    const size_t i   = group * kWarp + lane;
     const bool valid = i < n;
-    const double xi = valid ? x[i] : 0.0;
-    const double yi = valid ? y[i] : 0.0;
-    const double zi = valid ? z[i] : 0.0;
-    double hi       = valid ? h[i] : 0.0;
+    const double xi  = valid ? x[i] : 0.0;
+    const double yi  = valid ? y[i] : 0.0;
+    const double zi  = valid ? z[i] : 0.0;
+    double hi        = valid ? h[i] : 0.0;
 
     const unsigned ngmin = prm.ng0 / 4;
+    const unsigned ngPad = paddedNgmax(prm.ngmax);
     bool active          = valid;
     int updates          = 0;
     unsigned count       = 0;
     bool overflow        = false;
 
-    int* stack   = sh.stack[warp];
-    int* leaves  = sh.leaf[warp];
-    int* firsts  = sh.first[warp];
-    int* prefix  = sh.prefix[warp];
+    int* stack     = sh.stack[warp];
+    int* leafFirst = sh.leafFirst[warp];
+    int* leafEnd   = sh.leafEnd[warp];
+    int* blkPre    = sh.blkPre[warp];
+    int* pStart    = sh.pStart[warp];
+    int* pPre      = sh.pPre[warp];
 
     while (__ballot_sync(0xffffffffu, active) != 0u && !overflow)
     {
@@ -118,15 +159,20 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
         bhi[1] = warpMax(active ? yi + r : -INFINITY);
         bhi[2] = warpMax(active ? zi + r : -INFINITY);
         double gc[3], gs[3];
+        float gcb[3], gsb[3], lenf[3], ilenf[3]; // group box in the block-box frame (relative to the box corner)
         for (int k = 0; k < 3; ++k)
         {
-            gc[k] = 0.5 * (blo[k] + bhi[k]);
-            gs[k] = 0.5 * (bhi[k] - blo[k]) * (1.0 + 1e-12) + 1e-14 * box.len[k];
+            gc[k]    = 0.5 * (blo[k] + bhi[k]);
+            gs[k]    = 0.5 * (bhi[k] - blo[k]) * (1.0 + 1e-12) + 1e-14 * box.len[k];
+            gcb[k]   = float(gc[k] - box.lo[k]);
+            gsb[k]   = __double2float_ru(gs[k] + 4e-7 * box.len[k]);
+            lenf[k]  = float(box.len[k]);
+            ilenf[k] = float(box.ilen[k]);
         }
         // this particle relative to the group centre in FP32, and the FP32 acceptance band
-        const float rix = float(minImage(xi - gc[0], box.len[0], box.ilen[0], box.periodic[0]));
-        const float riy = float(minImage(yi - gc[1], box.len[1], box.ilen[1], box.periodic[1]));
-        const float riz = float(minImage(zi - gc[2], box.len[2], box.ilen[2], box.periodic[2]));
+        const float rix  = float(minImage(xi - gc[0], box.len[0], box.ilen[0], box.periodic[0]));
+        const float riy  = float(minImage(yi - gc[1], box.len[1], box.ilen[1], box.periodic[1]));
+        const float riz  = float(minImage(zi - gc[2], box.len[2], box.ilen[2], box.periodic[2]));
         const float twoH = float(r);
         const float r2f  = twoH * twoH;
         float reach      = active ? sqrtf(rix * rix + riy * riy + riz * riz) * 1.001f + twoH : 0.f;
@@ -142,105 +188,167 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
         if (active) { count = 0; }
         int numLeaves = 0;
 
-        // stream the buffered candidate leaves through the per-lane distance test
+        // this lane's chunk buffer and its store to the chunked list layout (nidxAt)
+        uint32_t* chunk = sh.nbuf[warp][lane];
+        auto storeChunk = [&](unsigned c) {
+            uint4* dst       = reinterpret_cast<uint4*>(nidx + nidxAt(group, ngPad, c * kNbChunk, lane));
+            const uint4* src = reinterpret_cast<const uint4*>(chunk);
+            dst[0]           = src[0];
+            dst[1]           = src[1];
+        };
+
+        // test the staged 32 candidates against this lane's particle and append the neighbours in index order
+        auto testStaged = [&]() {
+            if (!active) { return; }
+            // bit k: candidate k may lie inside the sphere (FP32 distance below the upper edge of the band)
+            unsigned maybe = 0u;
+            const float2 mx = make_float2(-rix, -rix), my = make_float2(-riy, -riy), mz = make_float2(-riz, -riz);
+#pragma unroll
+            for (int k = 0; k < kWarp; k += 2)
+            {
+                float2 X  = *reinterpret_cast<const float2*>(&sh.cx[warp][k]);
+                float2 Y  = *reinterpret_cast<const float2*>(&sh.cy[warp][k]);
+                float2 Z  = *reinterpret_cast<const float2*>(&sh.cz[warp][k]);
+                float2 dx = __fadd2_rn(X, mx);
+                float2 dy = __fadd2_rn(Y, my);
+                float2 dz = __fadd2_rn(Z, mz);
+                float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                maybe |= (unsigned(d2.x < r2hi) << k) | (unsigned(d2.y < r2hi) << (k + 1));
+            }
+            while (maybe)
+            {
+                int k = __ffs(maybe) - 1;
+                maybe &= maybe - 1u;
+                int j = sh.cj[warp][k];
+                if (size_t(j) == i) { continue; }
+                float dx = __fsub_rn(sh.cx[warp][k], rix);
+                float dy = __fsub_rn(sh.cy[warp][k], riy);
+                float dz = __fsub_rn(sh.cz[warp][k], riz);
+                bool in  = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))) < r2lo;
+                if (!in)
+                {
+                    // too close to the search radius for FP32: the exact test of the reference
+                    double ex = minImage(x[j] - xi, box.len[0], box.ilen[0], box.periodic[0]);
+                    double ey = minImage(y[j] - yi, box.len[1], box.ilen[1], box.periodic[1]);
+                    double ez = minImage(z[j] - zi, box.len[2], box.ilen[2], box.periodic[2]);
+                    double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+                    in        = d2 < radiusSq;
+                }
+                if (in)
+                {
+                    if (count < prm.ngmax)
+                    {
+                        chunk[count % kNbChunk] = uint32_t(j);
+                        if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
+                    }
+                    ++count;
+                }
+            }
+        };
+
+        // stream the buffered candidate leaves, pruned to the 8-particle blocks that meet the search box
         auto flush = [&]() {
-            // sizes and exclusive prefix of the buffered leaves (8 per lane at most)
             int local[kLeafCap / kWarp];
             int sum = 0;
 #pragma unroll
             for (int q = 0; q < kLeafCap / kWarp; ++q)
             {
-                int t    = lane * (kLeafCap / kWarp) + q;
-                int size = 0;
+                int t   = lane * (kLeafCap / kWarp) + q;
+                int nbk = 0;
                 if (t < numLeaves)
                 {
-                    int leaf  = leaves[t];
-                    int b     = tree.layout[leaf];
-                    size      = tree.layout[leaf + 1] - b;
-                    firsts[t] = b;
+                    int b = leafFirst[t], e = leafEnd[t];
+                    nbk   = e > b ? (e - 1) / kBlockSize - b / kBlockSize + 1 : 0;
                 }
-                local[q] = size;
-                sum += size;
+                local[q] = nbk;
+                sum += nbk;
             }
-            int incl = sum;
-#pragma unroll
-            for (int off = 1; off < kWarp; off <<= 1)
-            {
-                int v = __shfl_up_sync(0xffffffffu, incl, off);
-                if (lane >= off) { incl += v; }
-            }
-            int run = incl - sum;
+            int totalBlocks;
+            int run = warpExclusive(sum, lane, &totalBlocks);
 #pragma unroll
             for (int q = 0; q < kLeafCap / kWarp; ++q)
             {
                 int t = lane * (kLeafCap / kWarp) + q;
-                if (t < numLeaves) { prefix[t] = run; }
+                if (t < numLeaves) { blkPre[t] = run; }
                 run += local[q];
             }
-            int total = __shfl_sync(0xffffffffu, incl, kWarp - 1);
-            if (lane == 0) { prefix[numLeaves] = total; }
             __syncwarp();
 
-            for (int base = 0; base < total; base += kWarp)
+            for (int base = 0; base < totalBlocks; base += kWarp)
             {
-                int t = base + lane;
-                if (t < total)
+                int t     = base + lane;
+                bool keep = false;
+                int ps = 0, plen = 0;
+                if (t < totalBlocks)
                 {
-                    int lo = 0, hiIdx = numLeaves; // find the leaf r with prefix[r] <= t < prefix[r+1]
-                    while (hiIdx - lo > 1)
+                    int rr = findSlot(blkPre, numLeaves, t);
+                    int b = leafFirst[rr], e = leafEnd[rr];
+                    int c = b / kBlockSize + (t - blkPre[rr]);
+                    ps    = max(c * kBlockSize, b);
+                    plen  = min(c * kBlockSize + kBlockSize, e) - ps;
+                    float4 lo = __ldg(tree.blockLo + c);
+                    float4 hb = __ldg(tree.blockHi + c);
+                    float bl[3] = {lo.x, lo.y, lo.z};
+                    float bh[3] = {hb.x, hb.y, hb.z};
+                    keep = plen > 0;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
                     {
-                        int mid = (lo + hiIdx) >> 1;
-                        if (prefix[mid] <= t) { lo = mid; }
-                        else { hiIdx = mid; }
+                        float d = 0.5f * (bl[k] + bh[k]) - gcb[k];
+                        if (box.periodic[k]) { d -= lenf[k] * rintf(d * ilenf[k]); }
+                        keep = keep && fabsf(d) <= gsb[k] + 0.5f * (bh[k] - bl[k]) + 1e-6f * lenf[k];
                     }
-                    int j = firsts[lo] + (t - prefix[lo]);
-                    float4 c;
-                    if (j < 0 || size_t(j) >= n)
+                }
+                unsigned m = __ballot_sync(0xffffffffu, keep);
+                int numPieces = __popc(m);
+                int totalCand;
+                int ex = warpExclusive(keep ? plen : 0, lane, &totalCand);
+                if (keep)
+                {
+                    int pos     = __popc(m & ((1u << lane) - 1u));
+                    pStart[pos] = ps;
+                    pPre[pos]   = ex;
+                }
+                __syncwarp();
+                for (int cbase = 0; cbase < totalCand; cbase += kWarp)
+                {
+                    int tc = cbase + lane;
+                    if (tc < totalCand)
                     {
-                        // a layout that points outside the particle arrays: report, stage a far-away point
-                        atomicOr(status, 2u);
-                        c = make_float4(INFINITY, INFINITY, INFINITY, __int_as_float(0));
+                        int rr = findSlot(pPre, numPieces, tc);
+                        int j  = pStart[rr] + (tc - pPre[rr]);
+                        if (j < 0 || size_t(j) >= n)
+                        {
+                            // a layout that points outside the particle arrays: report, stage a far-away point
+                            atomicOr(status, 2u);
+                            sh.cx[warp][lane] = INFINITY;
+                            sh.cy[warp][lane] = INFINITY;
+                            sh.cz[warp][lane] = INFINITY;
+                            sh.cj[warp][lane] = -1;
+                        }
+                        else
+                        {
+                            sh.cx[warp][lane] =
+                                float(minImage(x[j] - gc[0], box.len[0], box.ilen[0], box.periodic[0]));
+                            sh.cy[warp][lane] =
+                                float(minImage(y[j] - gc[1], box.len[1], box.ilen[1], box.periodic[1]));
+                            sh.cz[warp][lane] =
+                                float(minImage(z[j] - gc[2], box.len[2], box.ilen[2], box.periodic[2]));
+                            sh.cj[warp][lane] = j;
+                        }
                     }
                     else
                     {
-                        c = make_float4(float(minImage(x[j] - gc[0], box.len[0], box.ilen[0], box.periodic[0])),
-                                        float(minImage(y[j] - gc[1], box.len[1], box.ilen[1], box.periodic[1])),
-                                        float(minImage(z[j] - gc[2], box.len[2], box.ilen[2], box.periodic[2])),
-                                        __int_as_float(j));
+                        // pad with points that no sphere reaches, so the test is branch-free
+                        sh.cx[warp][lane] = INFINITY;
+                        sh.cy[warp][lane] = INFINITY;
+                        sh.cz[warp][lane] = INFINITY;
+                        sh.cj[warp][lane] = -1;
                     }
-                    sh.cand[warp][lane] = c;
+                    __syncwarp();
+                    testStaged();
+                    __syncwarp();
                 }
-                __syncwarp();
-                int cnt = min(kWarp, total - base);
-                if (active)
-                {
-                    for (int k = 0; k < cnt; ++k)
-                    {
-                        float4 c  = sh.cand[warp][k];
-                        float dx  = c.x - rix;
-                        float dy  = c.y - riy;
-                        float dz  = c.z - riz;
-                        float d2f = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        if (d2f >= r2hi) { continue; }
-                        int j   = __float_as_int(c.w);
-                        bool in = d2f < r2lo;
-                        if (!in)
-                        {
-                            // too close to the search radius for FP32: the exact test of the reference
-                            double ex = minImage(x[j] - xi, box.len[0], box.ilen[0], box.periodic[0]);
-                            double ey = minImage(y[j] - yi, box.len[1], box.ilen[1], box.periodic[1]);
-                            double ez = minImage(z[j] - zi, box.len[2], box.ilen[2], box.periodic[2]);
-                            double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-                            in        = d2 < radiusSq;
-                        }
-                        if (in && size_t(j) != i)
-                        {
-                            if (count < prm.ngmax) { nidx[nidxSlot(group, prm.ngmax, count, lane)] = uint32_t(j); }
-                            ++count;
-                        }
-                    }
-                }
-                __syncwarp();
             }
             numLeaves = 0;
         };
@@ -258,7 +366,12 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
             if (child0 == 0)
             {
                 if (numLeaves == kLeafCap) { flush(); }
-                if (lane == 0) { leaves[numLeaves] = tree.nodeToLeaf[node]; }
+                if (lane == 0)
+                {
+                    int leaf             = tree.nodeToLeaf[node];
+                    leafFirst[numLeaves] = tree.layout[leaf];
+                    leafEnd[numLeaves]   = tree.layout[leaf + 1];
+                }
                 ++numLeaves;
                 __syncwarp();
                 continue;
@@ -287,14 +400,16 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
             if (ov)
             {
                 // children are pushed in reverse so that the lowest key is popped first
-                int pos                        = __popc(m >> (lane + 1));
-                stack[sp + pos]                = child0 + lane;
+                int pos         = __popc(m >> (lane + 1));
+                stack[sp + pos] = child0 + lane;
             }
             sp += pushes;
             __syncwarp();
         }
         if (overflow) { break; }
         if (numLeaves > 0) { flush(); }
+        // the last, partly filled chunk of the list (entries past the count are never read)
+        if (active && count % kNbChunk != 0 && count < prm.ngmax) { storeChunk(count / kNbChunk); }
 
         // smoothing-length iteration
         if (active)
@@ -322,7 +437,41 @@ __global__ void __launch_bounds__(kNbThreads) findNeighborsKernel(const double* 
     }
 }
 
+//! bounding box of each run of kBlockSize consecutive particles, relative to the box corner, rounded outwards
+__global__ void blockBoxesKernel(const double* __restrict__ x, const double* __restrict__ y,
+                                 const double* __restrict__ z, size_t n, DevBox box, float4* lo, float4* hi)
+{
+    size_t c = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    size_t b = c * kBlockSize;
+    if (b >= n) { return; }
+    size_t e  = min(b + kBlockSize, n);
+    double l[3] = {INFINITY, INFINITY, INFINITY}, u[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t j = b; j < e; ++j)
+    {
+        double p[3] = {x[j] - box.lo[0], y[j] - box.lo[1], z[j] - box.lo[2]};
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            l[k] = fmin(l[k], p[k]);
+            u[k] = fmax(u[k], p[k]);
+        }
+    }
+    lo[c] = make_float4(__double2float_rd(l[0]), __double2float_rd(l[1]), __double2float_rd(l[2]), 0.f);
+    hi[c] = make_float4(__double2float_ru(u[0]), __double2float_ru(u[1]), __double2float_ru(u[2]), 0.f);
+}
+
 } // namespace
+
+int computeBlockBoxes(const double* x, const double* y, const double* z, size_t n, const DevBox& box, float4* lo,
+                      float4* hi, cudaStream_t stream)
+{
+    if (n == 0) { return kOk; }
+    size_t blocks = (n + kBlockSize - 1) / kBlockSize;
+    blockBoxesKernel<<<ceilDiv(blocks, 256), 256, 0, stream>>>(x, y, z, n, box, lo, hi);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
 
 int findNeighbors(const double* x, const double* y, const double* z, double* h, size_t n, const TreeView& tree,
                   const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc, unsigned* status,

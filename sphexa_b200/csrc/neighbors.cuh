@@ -14,14 +14,31 @@ struct TreeView
     const double* centers; // 3 per node
     const double* sizes;   // 3 per node
     const int* layout;     // first particle per leaf, numLeaves+1
+    const float4* blockLo; // per run of kBlockSize consecutive particles: bounding box relative to the box corner
+    const float4* blockHi;
     int numNodes;
 };
 
-/*! Neighbour lists are stored per group of 32 consecutive particles, slot-major: the k-th neighbour of particle
- *  i = 32 g + lane sits at nidx[(g * ngmax + k) * 32 + lane], so one slot of a warp is one 128-byte line. */
-__host__ __device__ inline size_t nidxSlot(size_t group, unsigned ngmax, unsigned k, unsigned lane)
+//! particles per bounding-box block used to prune the candidates of the search below leaf resolution
+constexpr int kBlockSize = 8;
+
+//! bounding boxes of the runs of kBlockSize consecutive particles (ceil(n / kBlockSize) entries each)
+int computeBlockBoxes(const double* x, const double* y, const double* z, size_t n, const DevBox& box, float4* lo,
+                      float4* hi, cudaStream_t stream);
+
+//! neighbours per list chunk: one 32-byte sector of indices
+constexpr unsigned kNbChunk = 8;
+
+//! list capacity per particle rounded up to whole chunks
+__host__ __device__ inline unsigned paddedNgmax(unsigned ngmax) { return (ngmax + kNbChunk - 1) / kNbChunk * kNbChunk; }
+
+/*! Neighbour lists are stored per group of 32 consecutive particles in chunks of 8: the k-th neighbour of particle
+ *  i = 32 g + lane sits at nidx[((g * (P/8) + k/8) * 32 + lane) * 8 + k%8], P = paddedNgmax(ngmax). Each chunk of a
+ *  particle is one full 32-byte sector (written at once by the search, read with two 16-byte loads by the J-loops),
+ *  and chunk row k/8 of a warp is 1 KB of contiguous memory. */
+__host__ __device__ inline size_t nidxAt(size_t group, unsigned paddedNg, unsigned k, unsigned lane)
 {
-    return ((group * ngmax + k) << 5) + lane;
+    return (((group * (paddedNg / kNbChunk) + k / kNbChunk) << 5) + lane) * kNbChunk + (k % kNbChunk);
 }
 
 struct NeighborParams

@@ -57,6 +57,8 @@ struct sphb_sim
     DeviceBuffer<uint32_t> order;
     DeviceBuffer<char> sortScratch;
     DeviceBuffer<double4> pos;
+    DeviceBuffer<int4> posq;
+    DeviceBuffer<float4> blockLo, blockHi;
     DeviceBuffer<uint32_t> nidx;
     DeviceBuffer<unsigned> nc;
     DeviceBuffer<char> derived[kNumDerived];
@@ -68,6 +70,11 @@ struct sphb_sim
     DeviceBuffer<unsigned> status;
     DeviceBuffer<double> partial, cons;
     double K{0};
+    // FP32 polynomial kernel: fitted once per simulation (it depends only on the sinc index)
+    bool polyReady{false};
+    int polyOk{0};
+    float wpoly[kPolyTerms]{};
+    float dwpoly[kPolyTerms]{};
 
     GlobalTree gtree;
     FocusTree ftree;
@@ -111,7 +118,10 @@ int allocateSim(sphb_sim& s)
     SPHB_TRY(s.order.reserve(n));
     SPHB_TRY(s.sortScratch.reserve(sortScratchBytes(n)));
     SPHB_TRY(s.pos.reserve(n));
-    SPHB_TRY(s.nidx.reserve(s.numGroups() * size_t(s.p.ngmax) * kWarp));
+    if (s.mixed) { SPHB_TRY(s.posq.reserve(n)); }
+    SPHB_TRY(s.blockLo.reserve(n / kBlockSize + 1));
+    SPHB_TRY(s.blockHi.reserve(n / kBlockSize + 1));
+    SPHB_TRY(s.nidx.reserve(s.numGroups() * size_t(paddedNgmax(s.p.ngmax)) * kWarp));
     SPHB_TRY(s.nc.reserve(n));
     for (int d = 0; d < kNumDerived; ++d)
     {
@@ -127,6 +137,18 @@ int allocateSim(sphb_sim& s)
 
     std::vector<double> wh(kTableSize), whd(kTableSize);
     s.K = sincKernelTables(s.p.sinc_index, wh.data(), whd.data(), kTableSize);
+    {
+        // the polynomial replaces the table only if it reproduces the kernel to well inside FP32 resolution
+        double cw[kPolyTerms], cdw[kPolyTerms];
+        double err = sincPolyCoeffs(s.p.sinc_index, kPolyTerms - 1, cw, cdw);
+        s.polyOk   = err < 1e-6 ? 1 : 0;
+        for (int q = 0; q < kPolyTerms; ++q)
+        {
+            s.wpoly[q]  = float(cw[q]);
+            s.dwpoly[q] = float(cdw[q]);
+        }
+        s.polyReady = true;
+    }
     SPHB_TRY(s.whD.reserve(kTableSize));
     SPHB_TRY(s.whdD.reserve(kTableSize));
     SPHB_CUDA_TRY(cudaMemcpy(s.whD.data(), wh.data(), kTableSize * sizeof(double), cudaMemcpyHostToDevice));
@@ -226,7 +248,10 @@ int syncDomain(sphb_sim& s)
     SPHB_TRY(focusUpdateTree(s.ftree, s.gtree, s.ts, st, &converged));
     SPHB_TRY(focusUpdateCounts(s.ftree, s.keys.data(), s.n, s.ts, st));
     SPHB_TRY(computeGeoCenters(s.ftree.tree, s.box, st));
-    SPHB_TRY(packPositions(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n, s.pos.data(), st));
+    SPHB_TRY(packPositions(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n, s.pos.data(),
+                           s.mixed ? s.posq.data() : nullptr, s.box, st));
+    SPHB_TRY(computeBlockBoxes(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.n, s.box, s.blockLo.data(),
+                               s.blockHi.data(), st));
     return kOk;
 }
 
@@ -236,6 +261,7 @@ ChainArrays<T> chainArrays(sphb_sim& s)
     ChainArrays<T> a;
     a.n     = s.n;
     a.pos   = s.pos.data();
+    a.posq  = s.posq.data();
     a.h     = s.f[fH].data();
     a.vx    = s.f[fVx].data();
     a.vy    = s.f[fVy].data();
@@ -294,14 +320,16 @@ HydroConsts<T> hydroConsts(const sphb_sim& s)
     k.usePoly = 0;
     if constexpr (sizeof(T) == 4)
     {
-        // the polynomial replaces the table only if it reproduces the kernel to well inside FP32 resolution
-        double cw[kPolyTerms], cdw[kPolyTerms];
-        double err = sincPolyCoeffs(s.p.sinc_index, kPolyTerms - 1, cw, cdw);
-        k.usePoly  = err < 1e-6 ? 1 : 0;
+        k.usePoly = s.polyOk;
         for (int q = 0; q < kPolyTerms; ++q)
         {
-            k.wpoly[q]  = float(cw[q]);
-            k.dwpoly[q] = float(cdw[q]);
+            k.wpoly[q]  = s.wpoly[q];
+            k.dwpoly[q] = s.dwpoly[q];
+        }
+        FixedFrame fr = fixedFrameOf(s.box);
+        for (int d = 0; d < 3; ++d)
+        {
+            k.qscale[d] = float(fr.unit[d]);
         }
     }
     return k;
@@ -342,6 +370,8 @@ int computeForces(sphb_sim& s)
     tv.centers      = s.ftree.tree.centers.data();
     tv.sizes        = s.ftree.tree.sizes.data();
     tv.layout       = s.ftree.layout.data();
+    tv.blockLo      = s.blockLo.data();
+    tv.blockHi      = s.blockHi.data();
     tv.numNodes     = s.ftree.tree.numNodes;
     NeighborParams np{s.p.ng0, s.p.ngmax, 10};
     SPHB_TRY(findNeighbors(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fH].data(), s.n, tv, s.box, np,
@@ -669,7 +699,7 @@ extern "C" int sphb_sim_set_field(sphb_sim* s, const char* name, const double* i
         std::strcmp(name, "m") == 0)
     {
         SPHB_TRY(packPositions(s->f[fX].data(), s->f[fY].data(), s->f[fZ].data(), s->f[fM].data(), s->n,
-                               s->pos.data(), s->stream));
+                               s->pos.data(), s->mixed ? s->posq.data() : nullptr, s->box, s->stream));
         SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
     }
     return SPHB_OK;
@@ -709,15 +739,16 @@ extern "C" int sphb_sim_tree(sphb_sim* s, size_t* num_leaves, uint64_t* leaves, 
 extern "C" int sphb_sim_neighbors(sphb_sim* s, uint32_t* out)
 {
     if (!s || !out) { return SPHB_ERR_ARG; }
-    size_t ng = s->p.ngmax;
-    std::vector<uint32_t> raw(s->numGroups() * ng * kWarp);
+    size_t ng    = s->p.ngmax;
+    unsigned pad = paddedNgmax(s->p.ngmax);
+    std::vector<uint32_t> raw(s->numGroups() * pad * kWarp);
     SPHB_CUDA_TRY(cudaMemcpy(raw.data(), s->nidx.data(), raw.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     for (size_t i = 0; i < s->n; ++i)
     {
         size_t g = i / kWarp, lane = i % kWarp;
         for (size_t k = 0; k < ng; ++k)
         {
-            out[i * ng + k] = raw[nidxSlot(g, unsigned(ng), unsigned(k), unsigned(lane))];
+            out[i * ng + k] = raw[nidxAt(g, pad, unsigned(k), unsigned(lane))];
         }
     }
     return SPHB_OK;
