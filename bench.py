@@ -14,13 +14,14 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
-import math
 import os
 import statistics
 import subprocess
 import sys
 import tempfile
 import time
+
+import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -32,12 +33,15 @@ FLOPS_PER_PAIR = {"xmass": 18, "ve_def_gradh_eos": 31, "iad_divv_curlv": 88, "av
                   "momentum_energy": 140}
 KERNEL_STAGES = ("sync", "neighbors", "xmass", "ve_def_gradh_eos", "iad_divv_curlv", "av_switches",
                  "momentum_energy")
+#: DRAM bytes (read + write) per particle of one launch of a stage's kernel from an ncu capture, keyed by
+#: (stage, precision); scaled by the particle count of the run
+NCU_TRAFFIC = {}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--side", type=int, default=128)
@@ -63,57 +67,202 @@ def workload_config(side, n, precision):
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and throttle-reason samples taken every few milliseconds during the timed region (NVML, read only;
+    nvidia-smi polling as the fallback)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("sw_thermal_slowdown", 0x20), ("hw_thermal_slowdown", 0x40),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_s: float = 0.005):
         self.gpu = gpu_index
-        self.proc = None
+        self.period = period_s
+        self.samples = []
+        self.thread = None
+        self.stop_flag = None
+        self.smi = None
         self.path = None
+        self.max_mhz = None
+
+    def _nvml_loop(self, handle, nvml):
+        while not self.stop_flag.is_set():
+            try:
+                mhz = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                rs = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                self.samples.append((float(mhz), int(rs)))
+            except Exception:
+                pass
+            self.stop_flag.wait(self.period)
 
     def start(self):
         try:
+            import threading
+            import pynvml as nvml
+            nvml.nvmlInit()
+            handle = nvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = float(nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM))
+            self.stop_flag = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(handle, nvml), daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
+        try:
             fd, self.path = tempfile.mkstemp(suffix=".csv")
             os.close(fd)
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            fields = ("index,clocks.sm,clocks.max.sm,clocks_event_reasons.active")
+            self.smi = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={fields}",
+                                         "--format=csv,noheader,nounits", "-lms", "100"],
+                                        stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
-            self.proc = None
+            self.smi = None
 
     def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], [], set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    smax.append(float(parts[2]))
-                except ValueError:
-                    continue
-                for nm, v in zip(names, parts[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(nm)
-        os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            source = "nvml"
+        elif self.smi is not None:
+            self.smi.terminate()
+            try:
+                self.smi.wait(timeout=5)
+            except Exception:
+                self.smi.kill()
+            source = "nvidia-smi"
+            with open(self.path) as f:
+                for line in f:
+                    parts = [q.strip() for q in line.split(",")]
+                    try:
+                        self.samples.append((float(parts[1]), int(parts[3], 16)))
+                        self.max_mhz = float(parts[2])
+                    except (ValueError, IndexError):
+                        continue
+            os.unlink(self.path)
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": ["clock sampling unavailable"]}
+        mask = 0
+        for _, r in self.samples:
+            mask |= r
+        reasons = [name for name, bit in self.REASONS if mask & bit]
+        sm = [m for m, _ in self.samples]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "samples": len(sm), "source": source, "reasons": reasons}
+
+
+#: HBM bytes per particle that each stage must move at least: the reads and writes of the fields the reference's
+#: kernels take and produce (FP64 / mixed types). Sync: keys 32 (x, y, z in, key out) + sort 200 (8 radix passes
+#: over (key, index)) + gather 244 (15 fields in and out, permutation in) + tree 10. Neighbour search: x, y, z, h in,
+#: h, nc out. XMass: x, y, z, h, m in, xm out. VeDefGradh + EOS: x, y, z, h, m, xm, temp in, kx, gradh, prho, c out.
+#: IAD + divv/curlv: x, y, z, h, v, xm, kx in, c11..c33, divv, curlv out. AVswitches: x, y, z, h, v, c, c11..c33,
+#: divv, xm, kx, alpha in, alpha out. MomentumEnergy: x, y, z, h, v, m, c, prho, c11..c33, alpha, xm, kx in,
+#: ax, ay, az, du out. Conserved sums: x, y, z, v, m, temp, nc. Integrate: positions, x_m1, v, a, temp, du, du_m1 in,
+#: positions, x_m1, v, temp, du_m1 out, then h update (nc, h in, h out). Neighbour lists add 4 B per pair to the
+#: search (written) and to each J-loop (read).
+BYTES_PER_PARTICLE = {
+    "fp64": {"sync": 486, "neighbors": 44, "xmass": 48, "ve_def_gradh_eos": 88, "iad_divv_curlv": 136,
+             "av_switches": 152, "momentum_energy": 184, "conserved": 68, "integrate": 228},
+    "mixed": {"sync": 486, "neighbors": 44, "xmass": 40, "ve_def_gradh_eos": 64, "iad_divv_curlv": 96,
+              "av_switches": 112, "momentum_energy": 128, "conserved": 68, "integrate": 216},
+}
+LIST_BYTES_PER_PAIR = {"neighbors": 4, "xmass": 4, "ve_def_gradh_eos": 4, "iad_divv_curlv": 4, "av_switches": 4,
+                       "momentum_energy": 4}
+
+
+def stage_rooflines(stage_ms: dict, n: int, pairs: int, precision: str, fma_peak_tf: float, hbm_gbs: float):
+    """Per stage: algorithmic FLOPs and bytes, the time each would take at peak, and the achieved fraction of the
+    binding one. The whole-step figure is sum(max(F/P, B/BW)) over stages divided by the measured step time."""
+    out = {}
+    t_roof_total = 0.0
+    for st, ms in stage_ms.items():
+        flops = FLOPS_PER_PAIR.get(st, 0) * pairs
+        byts = BYTES_PER_PARTICLE[precision].get(st, 0) * n + LIST_BYTES_PER_PAIR.get(st, 0) * pairs
+        t_f = flops / (fma_peak_tf * 1e12)
+        t_b = byts / (hbm_gbs * 1e9)
+        bound = "fp32" if precision == "mixed" else "fp64"
+        if t_b >= t_f:
+            bound = "hbm"
+        t_roof = max(t_f, t_b)
+        t_roof_total += t_roof
+        entry = {"ms": round(ms, 4), "bound": bound, "flops": flops, "bytes": byts,
+                 "roof_ms": round(t_roof * 1e3, 4), "frac": (t_roof * 1e3 / ms) if ms > 0 else None}
+        out[st] = entry
+    return out, t_roof_total * 1e3
+
+
+def hbm_peak_gbs() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def align_by_id(snap: dict) -> dict:
+    order = np.argsort(snap["id"], kind="stable")
+    return {k: v[order] for k, v in snap.items()}
+
+
+def field_errors(mixed: dict, fp64: dict) -> dict:
+    """Max and RMS relative error of the mixed-precision state against the plain FP64 state of the same run.
+    rho, u (temp) and h: per particle |a - b| / |b|. Positions: |a - b| / box length. Velocities and accelerations:
+    |a - b| / max|b| of the field (they start at zero)."""
+    a, b = align_by_id(mixed), align_by_id(fp64)
+    res = {}
+
+    def put(name, d, s):
+        r = np.abs(d) / s
+        res[name] = {"max": float(np.max(r)), "rms": float(np.sqrt(np.mean(r * r)))}
+
+    rho_a = a["kx"] * a["m"] / a["xm"]
+    rho_b = b["kx"] * b["m"] / b["xm"]
+    put("rho", rho_a - rho_b, np.abs(rho_b))
+    put("u", a["temp"] - b["temp"], np.abs(b["temp"]))
+    put("u_field_normalised", a["temp"] - b["temp"], float(np.max(np.abs(b["temp"]))))
+    put("h", a["h"] - b["h"], np.abs(b["h"]))
+    for f in ("x", "y", "z"):
+        put(f, a[f] - b[f], 1.0)
+    for f in ("vx", "vy", "vz", "ax", "ay", "az"):
+        put(f, a[f] - b[f], max(float(np.max(np.abs(b[f]))), 1e-300))
+    return res
+
+
+def evaluation_errors(mixed_sim, fp64_sim, n) -> dict:
+    """Error of one force evaluation: the FP64 simulation's current state is loaded into the mixed one, both compute
+    forces on it, and the outputs are compared (max and RMS relative; rho per particle, the others normalised by the
+    field's largest magnitude)."""
+    import torch
+    from sphexa_b200 import lib as L
+    from sphexa_b200.ic import CONSERVED_FIELDS
+    host = [torch.empty(n, dtype=torch.float64) for _ in CONSERVED_FIELDS]
+    hid = torch.empty(n, dtype=torch.int64)
+    tbl = (C.c_void_p * len(host))(*[h.data_ptr() for h in host])
+    L.check(fp64_sim.lib.sphb_sim_store_state(fp64_sim.h, tbl, C.c_void_p(hid.data_ptr()), 0), "store_state")
+    L.check(mixed_sim.lib.sphb_sim_load_state(mixed_sim.h, tbl, C.c_void_p(hid.data_ptr()), 0), "load_state")
+    fp64_sim.compute_forces()
+    mixed_sim.compute_forces()
+    a = {f: mixed_sim.get(f) for f in EVAL_FIELDS}
+    b = {f: fp64_sim.get(f) for f in EVAL_FIELDS}
+    out = {"same_neighbor_counts": bool(np.array_equal(a["nc"], b["nc"]))}
+
+    def put(name, d, s):
+        r = np.abs(d) / s
+        out[name] = {"max": float(np.max(r)), "rms": float(np.sqrt(np.mean(r * r)))}
+
+    rho_a, rho_b = a["kx"] * a["m"] / a["xm"], b["kx"] * b["m"] / b["xm"]
+    put("rho", rho_a - rho_b, np.abs(rho_b))
+    for f in ("c", "prho", "gradh"):
+        put(f, a[f] - b[f], np.abs(b[f]))
+    for f in ("du", "ax", "ay", "az", "divv", "alpha"):
+        put(f, a[f] - b[f], max(float(np.max(np.abs(b[f]))), 1e-300))
+    return out
+
+
+EVAL_FIELDS = ("nc", "m", "kx", "xm", "c", "prho", "gradh", "du", "ax", "ay", "az", "divv", "alpha")
+SNAP_FIELDS = ("id", "x", "y", "z", "h", "m", "temp", "vx", "vy", "vz", "kx", "xm", "ax", "ay", "az")
 
 
 def run_ours(args, ws, rank, local):
-    import numpy as np
     import torch
 
     from sphexa_b200 import ic as icm
@@ -147,8 +296,10 @@ def run_ours(args, ws, rank, local):
     def timed_leg(precision: str, steps: int, warmup: int, with_e2e: bool, with_clocks: bool):
         sim = Simulation(ic, precision)
         stream = torch.cuda.ExternalStream(sim.lib.sphb_sim_stream(sim.h))
+        energy = []
         for _ in range(warmup):
             sim.step()
+            energy.append(sim.scalars()["etot"])
         stage_sum = {k: 0.0 for k in sim.stage_times()}
         clocks = ClockSampler(local)
         barrier_sync()
@@ -162,6 +313,7 @@ def run_ours(args, ws, rank, local):
             sim.step()
             for k, v in sim.stage_times().items():
                 stage_sum[k] += v
+            energy.append(sim.scalars()["etot"])
         e1.record(stream)
         barrier_sync()
         clk = clocks.stop() if with_clocks else None
@@ -170,8 +322,9 @@ def run_ours(args, ws, rank, local):
         ms = max_over_ranks(ms)
         nc = sim.get("nc").astype(np.int64)
         pairs = int(np.minimum(nc - 1, int(ic["params"]["ngmax"])).sum())
+        snap = {f: sim.get(f) for f in SNAP_FIELDS}
         res = {"ms_total": ms, "stage_ms": {k: v / steps for k, v in stage_sum.items()}, "launches": launches,
-               "pairs": pairs, "clocks": clk, "sim": sim}
+               "pairs": pairs, "clocks": clk, "snap": snap, "energy": energy, "ttot": sim.scalars()["ttot"]}
         if with_e2e:
             # per step: host->device copy of the whole particle state from pinned memory, the step, and the
             # device->host copy of the updated state (the C-ABI round trip of a caller holding host buffers)
@@ -192,54 +345,76 @@ def run_ours(args, ws, rank, local):
             res["e2e_ms"] = max_over_ranks(e0.elapsed_time(e1))
             res["h2d_bytes"] = (len(host) * 8 + 8) * n
             res["d2h_bytes"] = (len(host) * 8 + 8) * n
+        res["sim_obj"] = sim
         return res
 
-    main = timed_leg(args.precision, args.steps, args.warmup, with_e2e=True, with_clocks=True)
+    main_leg = timed_leg(args.precision, args.steps, args.warmup, with_e2e=True, with_clocks=True)
     fp64 = None
     if args.precision == "mixed" and not args.no_fp64_leg:
-        fp64 = timed_leg("fp64", max(2, args.steps // 2), max(1, args.warmup), with_e2e=False, with_clocks=False)
+        # the same number of steps as the mixed leg, so that the final states can be compared
+        fp64 = timed_leg("fp64", args.steps, args.warmup, with_e2e=False, with_clocks=False)
 
-    # roofline of the dominant kernel (stage times are CUDA events around each launch on the sim stream)
-    stages = main["stage_ms"]
-    dominant = max(KERNEL_STAGES, key=lambda k: stages.get(k, 0.0))
+    stages = main_leg["stage_ms"]
     which = 0 if args.precision == "mixed" else 1
     peak = C.c_double()
     L.check(L.load().sphb_probe_fma_peak(which, C.byref(peak)), "probe")
-    roofline = None
-    if dominant in FLOPS_PER_PAIR:
-        flops = FLOPS_PER_PAIR[dominant] * main["pairs"]
-        achieved = flops / (stages[dominant] * 1e-3) / 1e12
-        roofline = {"bound": "fp32" if which == 0 else "fp64", "kernel": dominant, "achieved": achieved,
-                    "peak": peak.value, "unit": "TFLOP/s", "frac": achieved / peak.value, "traffic": None,
-                    "peak_source": "measured on this GPU by sphb_probe_fma_peak (register FMA loop, all SMs)",
-                    "flops_per_launch": flops}
+    hbm, hbm_src = hbm_peak_gbs()
+    per_stage, t_roof = stage_rooflines(stages, n, main_leg["pairs"], args.precision, peak.value, hbm)
+    dominant = max(KERNEL_STAGES, key=lambda k: stages.get(k, 0.0))
+    d = per_stage[dominant]
+    if d["bound"] == "hbm":
+        achieved = d["bytes"] / (d["ms"] * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                    "frac": achieved / hbm, "traffic": NCU_TRAFFIC.get((dominant, args.precision)),
+                    "peak_source": f"{hbm_src} HBM copy bandwidth", "bytes_per_launch": d["bytes"]}
     else:
-        roofline = {"bound": "latency", "kernel": dominant, "achieved": None, "peak": peak.value,
-                    "unit": "TFLOP/s", "frac": None, "traffic": None}
+        achieved = d["flops"] / (d["ms"] * 1e-3) / 1e12
+        roofline = {"bound": d["bound"], "kernel": dominant, "achieved": achieved, "peak": peak.value,
+                    "unit": "TFLOP/s", "frac": achieved / peak.value,
+                    "traffic": NCU_TRAFFIC.get((dominant, args.precision)),
+                    "peak_source": "measured on this GPU by sphb_probe_fma_peak (register FMA loop, all SMs)",
+                    "flops_per_launch": d["flops"]}
+    if roofline["traffic"] is not None:
+        roofline["traffic"] = roofline["traffic"] * n
 
     steps = args.steps
-    value = n * ws * steps / (main["ms_total"] * 1e-3)
+    ms_step = main_leg["ms_total"] / steps
+    value = n * ws * steps / (main_leg["ms_total"] * 1e-3)
+    energy = main_leg["energy"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": args.warmup,
-        "ms_per_step": main["ms_total"] / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if args.precision == "mixed" else "f64", "data": "synthetic",
-        "precision": ("mixed: FP32 Kahan-compensated neighbour sums on FP64 relative coordinates; FP64 positions, "
+        "precision": ("mixed: FP32 block-compensated neighbour sums on relative coordinates; FP64 positions, "
                       "keys, integration, h update and reductions") if args.precision == "mixed" else "fp64",
         "config": workload_config(args.side, n, args.precision),
-        "e2e": {"value": n * ws * steps / (main["e2e_ms"] * 1e-3), "unit": UNIT,
-                "h2d_bytes_per_step": main["h2d_bytes"], "d2h_bytes_per_step": main["d2h_bytes"]},
-        "gpu_launches": main["launches"],
+        "e2e": {"value": n * ws * steps / (main_leg["e2e_ms"] * 1e-3), "unit": UNIT,
+                "h2d_bytes_per_step": main_leg["h2d_bytes"], "d2h_bytes_per_step": main_leg["d2h_bytes"]},
+        "gpu_launches": main_leg["launches"],
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
-        "neighbor_pairs_per_step": main["pairs"],
+        "neighbor_pairs_per_step": main_leg["pairs"],
         "roofline": roofline,
-        "clocks": main["clocks"],
+        "roofline_step": {"t_roof_ms": round(t_roof, 4), "t_measured_ms": round(ms_step, 4),
+                          "frac": t_roof / ms_step, "hbm_peak_gbs": hbm, "fma_peak_tflops": peak.value,
+                          "stages": per_stage},
+        "energy_drift": abs(energy[-1] - energy[0]) / abs(energy[0]),
+        "clocks": main_leg["clocks"],
     }
     if fp64 is not None:
-        fsteps = max(2, args.steps // 2)
-        v64 = n * ws * fsteps / (fp64["ms_total"] * 1e-3)
-        line["fp64_plain"] = {"value": v64, "unit": UNIT, "ms_per_step": fp64["ms_total"] / fsteps,
+        v64 = n * ws * steps / (fp64["ms_total"] * 1e-3)
+        line["fp64_plain"] = {"value": v64, "unit": UNIT, "ms_per_step": fp64["ms_total"] / steps,
                               "stage_ms": {k: round(v, 4) for k, v in fp64["stage_ms"].items()},
+                              "energy_drift": abs(fp64["energy"][-1] - fp64["energy"][0]) / abs(fp64["energy"][0]),
                               "mixed_over_fp64": value / v64}
+        line["mixed_vs_fp64_error"] = {
+            "per_evaluation": evaluation_errors(main_leg["sim_obj"], fp64["sim_obj"], n),
+            "trajectory": {
+                "after_steps": args.warmup + steps,
+                "same_time": abs(main_leg["ttot"] - fp64["ttot"]) <= 1e-6 * fp64["ttot"],
+                "total_energy": abs(main_leg["energy"][-1] - fp64["energy"][-1]) / abs(fp64["energy"][-1]),
+                "fields": field_errors(main_leg["snap"], fp64["snap"])}}
+        fp64["sim_obj"].close()
+    main_leg["sim_obj"].close()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ic, n)
     if dist is not None:
