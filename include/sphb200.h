@@ -192,7 +192,34 @@ int sphb_sim_load_state(sphb_sim* sim, const double* const* fields, const uint64
 int sphb_sim_store_state(sphb_sim* sim, double* const* fields, uint64_t* id, int on_device);
 
 /* ---------------------------------------------------------------------------------------------------------------- */
-/* 3. Measurement helper                                                                                            */
+/* 3. Differentiation of the step                                                                                   */
+/* ---------------------------------------------------------------------------------------------------------------- */
+
+/*! Use a fixed time step dt instead of computeTimestep (sph/include/sph/ts_global.hpp:100-128); dt = 0 restores the
+ *  adaptive step. With dt > 0, minDt and minDt_m1 are set to dt (the AV switches and the integration read them).
+ *  No counterpart in the reference (its propagators always compute the step); required by sphb_sim_step_vjp. */
+int sphb_sim_set_fixed_dt(sphb_sim* sim, double dt);
+
+/*! Replace the physics parameters of a simulation (gamma, mui, Kcour, Krho, alphamin, alphamax, decay_constant) as
+ *  between steps of the reference's propagator (ParticlesData members, particles_data.hpp:85-143). ng0, ngmax,
+ *  precision, sinc_index and bucket_focus must be unchanged (SPHB_ERR_ARG otherwise). */
+int sphb_sim_set_params(sphb_sim* sim, const sphb_params* params);
+
+/*! Adjoint (vector-Jacobian product) of one step of the VE propagator (main/src/propagator/ve_hydro.hpp:126-220)
+ *  with a fixed time step and the step's discrete structure held fixed (sort permutation, neighbour lists and
+ *  counts, smoothing-length iterations, branch choices). Precondition: the simulation holds the state the step
+ *  starts from (after sphb_sim_load_state of a stored state, or the state before an sphb_sim_step) and a fixed
+ *  time step is set. The call recomputes the step's forces (neighbour search and chain) with a tape, then maps
+ *  adj_post, the adjoint of the state after the step (14 device arrays of n doubles, conserved-field order,
+ *  indexed like the state sphb_sim_store_state returns after the step), to adj_pre, the adjoint of the state before
+ *  the step (indexed like the state the step starts from); *alphamax_bar (host) is incremented by the derivative
+ *  with respect to alphamax. The adjoint of m is passed through unchanged. Precision follows the simulation: FP64
+ *  adjoint for SPHB_FP64, FP32 J-loop adjoints for SPHB_MIXED. Afterwards the simulation holds the recomputed
+ *  post-force state, not the state after the step. No counterpart in the reference. */
+int sphb_sim_step_vjp(sphb_sim* sim, const double* const* adj_post, double* const* adj_pre, double* alphamax_bar);
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* 4. Measurement helper                                                                                            */
 /* ---------------------------------------------------------------------------------------------------------------- */
 
 /*! Measure the CUDA-core FMA throughput of the current device: which = 0 for FP32, 1 for FP64. Runs a short

@@ -1,0 +1,144 @@
+"""Gradients through K steps of the VE hydro propagator with the hand-written adjoint kernels (sphb_sim_step_vjp).
+
+The forward runs K steps at a fixed time step and keeps a checkpoint of the full particle state every
+`checkpoint_every` steps. The backward pass walks the checkpoints in reverse: it restores one, recomputes the forward
+steps of that segment to recover each step's starting state, then applies the step adjoints in reverse order. Each
+step adjoint recomputes the step's forces with the same sort, neighbour lists and branch choices as the forward
+(they are deterministic functions of the restored state), so neighbour lists are frozen per step by construction.
+
+Objective: the total kinetic energy sum_i m_i |v_i|^2 / 2 after K steps. Parameters: the initial internal energy per
+particle u0 = cv * temp0 (in the order of the initial conditions) and the artificial-viscosity alphamax
+(sph/include/sph/hydro_ve/av_switches_kern.hpp).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .ic import CONSERVED_FIELDS
+from .simulation import Simulation
+
+FIELD_INDEX = {f: k for k, f in enumerate(CONSERVED_FIELDS)}
+
+
+def ideal_gas_cv(mui: float, gamma: float) -> float:
+    """cv of the reference's ideal gas (sph/include/sph/eos.hpp:19-24)."""
+    return 8.317e7 / mui / (gamma - 1.0)
+
+
+class AdjointRun:
+    def __init__(self, ic: dict, precision: str = "fp64", dt: float = 1e-5, steps: int = 20,
+                 checkpoint_every: int = 5):
+        import torch
+        self.torch = torch
+        self.ic = ic
+        self.precision = precision
+        self.dt = float(dt)
+        self.steps = int(steps)
+        self.every = int(checkpoint_every)
+        self.n = int(ic["x"].size)
+        self.cv = ideal_gas_cv(ic["params"]["mui"], ic["params"]["gamma"])
+        self.sim = None
+        self.checkpoints = {}
+        self.forward_steps = 0
+
+    # state buffers on the device ------------------------------------------------------------------------------
+    def _state_buffers(self):
+        t = self.torch
+        fields = [t.empty(self.n, dtype=t.float64, device="cuda") for _ in CONSERVED_FIELDS]
+        ids = t.empty(self.n, dtype=t.int64, device="cuda")
+        return fields, ids
+
+    def _store(self):
+        fields, ids = self._state_buffers()
+        self.sim.store_state(fields, ids)
+        return fields, ids
+
+    def _make_sim(self, u0: np.ndarray, alphamax: float) -> Simulation:
+        ic = dict(self.ic)
+        ic["temp"] = np.asarray(u0, dtype=np.float64) / self.cv
+        ic["params"] = dict(self.ic["params"], alphamax=float(alphamax))
+        sim = Simulation(ic, self.precision)
+        sim.set_fixed_dt(self.dt)
+        return sim
+
+    def kinetic_energy(self) -> float:
+        t = self.torch
+        m = t.empty(self.n, dtype=t.float64, device="cuda")
+        self.sim.get_device("m", m)
+        e = t.zeros((), dtype=t.float64, device="cuda")
+        for f in ("vx", "vy", "vz"):
+            v = t.empty(self.n, dtype=t.float64, device="cuda")
+            self.sim.get_device(f, v)
+            e += 0.5 * (m * v * v).sum()
+        return float(e.item())
+
+    # forward and backward -------------------------------------------------------------------------------------
+    def forward(self, u0: np.ndarray, alphamax: float, checkpoints: bool = True) -> float:
+        if self.sim is not None:
+            self.sim.close()
+        self.sim = self._make_sim(u0, alphamax)
+        self.checkpoints = {}
+        for s in range(self.steps):
+            if checkpoints and s % self.every == 0:
+                self.checkpoints[s] = self._store()
+            self.sim.step()
+        self.forward_steps = self.steps
+        return self.kinetic_energy()
+
+    def backward(self):
+        """Returns (dL/du0 in initial-condition order, dL/dalphamax)."""
+        t = self.torch
+        if not self.checkpoints:
+            raise RuntimeError("backward needs a forward run with checkpoints")
+        n = self.n
+        adj = [t.zeros(n, dtype=t.float64, device="cuda") for _ in CONSERVED_FIELDS]
+        m = t.empty(n, dtype=t.float64, device="cuda")
+        self.sim.get_device("m", m)
+        for f in ("vx", "vy", "vz"):
+            v = t.empty(n, dtype=t.float64, device="cuda")
+            self.sim.get_device(f, v)
+            adj[FIELD_INDEX[f]] = m * v
+        nxt = [t.empty(n, dtype=t.float64, device="cuda") for _ in CONSERVED_FIELDS]
+        alphamax_bar = 0.0
+        for start in sorted(self.checkpoints, reverse=True):
+            end = min(start + self.every, self.steps)
+            # recompute the segment's starting states from its checkpoint
+            states = [self.checkpoints[start]]
+            self.sim.load_state(*states[0])
+            for _ in range(start, end - 1):
+                self.sim.step()
+                states.append(self._store())
+            for s in reversed(range(start, end)):
+                self.sim.load_state(*states[s - start])
+                alphamax_bar += self.sim.step_vjp(adj, nxt)
+                adj, nxt = nxt, adj
+        ids = self.checkpoints[0][1].cpu().numpy()
+        gtemp = adj[FIELD_INDEX["temp"]].cpu().numpy()
+        grad_u0 = np.empty(n)
+        grad_u0[ids] = gtemp / self.cv
+        return grad_u0, alphamax_bar
+
+    def close(self):
+        if self.sim is not None:
+            self.sim.close()
+            self.sim = None
+
+
+def kinetic_energy_function():
+    """torch.autograd.Function computing the final kinetic energy of an AdjointRun from (u0, alphamax)."""
+    import torch
+
+    class KineticEnergy(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, u0, alphamax, run):
+            value = run.forward(u0.detach().cpu().numpy(), float(alphamax))
+            ctx.run = run
+            return torch.tensor(value, dtype=torch.float64)
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            gu, ga = ctx.run.backward()
+            g = float(grad_out)
+            return torch.from_numpy(gu * g), torch.tensor(ga * g, dtype=torch.float64), None
+
+    return KineticEnergy

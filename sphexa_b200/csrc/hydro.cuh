@@ -47,6 +47,24 @@ struct alignas(8 * sizeof(T)) GradRec
     T c11, c12, c13, c22, c23, c33, divv, alpha;
 };
 
+/*! Intermediate values the adjoint of the chain needs and the outputs do not determine; written only when the
+ *  pointers are set (a step recomputed for its adjoint). whomega, wrho0: the two kernel-derivative sums of VeDefGradh
+ *  after normalisation; gx, gy, gz, vsig, vsigJ: the divv gradient, the signal velocity of the AV switches and the
+ *  neighbour that set it (-1: none); energy, avisc: the energy and viscous-energy sums of MomentumEnergy. */
+template<class T>
+struct ChainTape
+{
+    T* whomega{nullptr};
+    T* wrho0{nullptr};
+    T* gx{nullptr};
+    T* gy{nullptr};
+    T* gz{nullptr};
+    T* vsig{nullptr};
+    int* vsigJ{nullptr};
+    T* energy{nullptr};
+    T* avisc{nullptr};
+};
+
 //! device arrays of one simulation used by the chain; derived fields are stored in T
 template<class T>
 struct ChainArrays
@@ -80,6 +98,7 @@ struct ChainArrays
     GradRec<T>* grec;
     // reduction outputs: [0] max divv (ordered bits), [1] min Courant dt (ordered bits)
     unsigned long long* reduce;
+    ChainTape<T> tape;
 };
 
 template<class T>

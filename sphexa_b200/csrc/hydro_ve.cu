@@ -10,6 +10,7 @@
 // periodic wrap by overflow; one unit = L / 2^32), all pair arithmetic is FP32, the kernel W is a degree-12
 // polynomial instead of a table, and every neighbour sum is block-compensated: plain FP32 partial sums over blocks of
 // 8 neighbours, each added to a Kahan-compensated FP32 accumulator.
+#include "chain_detail.cuh"
 #include "hydro.cuh"
 #include "neighbors.cuh"
 #include "primitives.cuh"
@@ -20,263 +21,7 @@ namespace sphb
 namespace
 {
 
-constexpr int kChainThreads = 128;
-
-/*! Neighbour-sum accumulator. FP64: every term is added as it comes, in list order (the reference's order).
- *  FP32: terms are summed plainly within one list chunk of 8 neighbours and each chunk sum is added to a
- *  Kahan-compensated accumulator; explicit round-to-nearest intrinsics keep the compiler from fusing or reordering
- *  the compensation. */
-template<class T>
-struct BlockSum;
-
-template<>
-struct BlockSum<double>
-{
-    double s;
-    __device__ explicit BlockSum(double v = 0.0)
-        : s(v)
-    {
-    }
-    __device__ void add(double v) { s += v; }
-    __device__ void flush() {}
-    __device__ double get() const { return s; }
-};
-
-template<>
-struct BlockSum<float>
-{
-    float s, comp, part;
-    __device__ explicit BlockSum(float v = 0.f)
-        : s(v)
-        , comp(0.f)
-        , part(0.f)
-    {
-    }
-    __device__ void add(float v) { part += v; }
-    __device__ void flush()
-    {
-        float y = __fsub_rn(part, comp);
-        float t = __fadd_rn(s, y);
-        comp    = __fsub_rn(__fsub_rn(t, s), y);
-        s       = t;
-        part    = 0.f;
-    }
-    __device__ float get() const { return s; }
-};
-
-//! a / b: IEEE division in FP64 (the reference's rounding), the fast 2-ulp reciprocal-multiply in FP32
-__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
-
-//! linear interpolation in a 20000-entry table on [0, 2] (sph/include/sph/table_lookup.hpp:14-26)
-template<class T>
-__device__ __forceinline__ T tableLookup(const T* __restrict__ table, T v)
-{
-    constexpr int numIntervals = kTableSize - 1;
-    constexpr T dx             = T(2.0) / numIntervals;
-    constexpr T invDx          = T(1) / dx;
-    int idx                    = int(v * invDx);
-    if (idx >= numIntervals) { return T(0); }
-    T t0 = __ldg(table + idx);
-    T t1 = __ldg(table + idx + 1);
-    T derivative = (t1 - t0) * invDx;
-    return t0 + derivative * (v - T(idx) * dx);
-}
-
-//! Horner evaluation of the FP32 kernel polynomial in t = v^2/2 - 1
-__device__ __forceinline__ float polyEval(const float (&c)[kPolyTerms], float v)
-{
-    float t   = fmaf(0.5f * v, v, -1.0f);
-    float acc = c[kPolyTerms - 1];
-#pragma unroll
-    for (int p = kPolyTerms - 2; p >= 0; --p)
-    {
-        acc = fmaf(acc, t, c[p]);
-    }
-    return acc;
-}
-
-//! the smoothing kernel W(v), zero from v = 2 on: FP64 by table lookup (as the reference), FP32 by polynomial
-template<class T>
-__device__ __forceinline__ T kernelW(const T* __restrict__ table, const HydroConsts<T>& k, T v)
-{
-    if constexpr (sizeof(T) == 4)
-    {
-        if (k.usePoly) { return v < T(2) ? polyEval(k.wpoly, v) : T(0); }
-    }
-    return tableLookup(table, v);
-}
-
-//! dW/dv, zero from v = 2 on
-template<class T>
-__device__ __forceinline__ T kernelDW(const T* __restrict__ table, const HydroConsts<T>& k, T v)
-{
-    if constexpr (sizeof(T) == 4)
-    {
-        if (k.usePoly) { return v < T(2) ? v * polyEval(k.dwpoly, v) : T(0); }
-    }
-    return tableLookup(table, v);
-}
-
-//! periodic shift of a pair separation by one box length if it exceeds r (cstone/sfc/box.hpp applyPBC, legacy form)
-__device__ __forceinline__ void shiftPbc(double& rx, double& ry, double& rz, double r, const DevBox& box)
-{
-    if (box.periodic[0])
-    {
-        if (rx > r) { rx -= box.len[0]; }
-        else if (rx < -r) { rx += box.len[0]; }
-    }
-    if (box.periodic[1])
-    {
-        if (ry > r) { ry -= box.len[1]; }
-        else if (ry < -r) { ry += box.len[1]; }
-    }
-    if (box.periodic[2])
-    {
-        if (rz > r) { rz -= box.len[2]; }
-        else if (rz < -r) { rz += box.len[2]; }
-    }
-}
-
-//! 32-byte read-only load as two 16-byte vector loads (one sector)
-__device__ __forceinline__ double4 ldg4(const double4* p)
-{
-    const double2* q = reinterpret_cast<const double2*>(p);
-    double2 lo = __ldg(q), hi = __ldg(q + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
-}
-
-// ---------------------------------------------------------------------------------------------------------------
-// positions and pair separations per precision
-// ---------------------------------------------------------------------------------------------------------------
-
-template<class T>
-struct Pos;
-
-template<>
-struct Pos<double>
-{
-    double x, y, z, m;
-};
-
-template<>
-struct Pos<float>
-{
-    int x, y, z;
-    float m;
-};
-
-__device__ __forceinline__ Pos<double> posOf(const ChainArrays<double>& a, size_t j)
-{
-    double4 v = ldg4(a.pos + j);
-    return {v.x, v.y, v.z, v.w};
-}
-
-__device__ __forceinline__ Pos<float> posOf(const ChainArrays<float>& a, size_t j)
-{
-    int4 v = __ldg(a.posq + j);
-    return {v.x, v.y, v.z, __int_as_float(v.w)};
-}
-
-template<class T>
-struct Sep
-{
-    T rx, ry, rz;
-};
-
-//! x_i - x_j with the reference's periodic shift (threshold r = 2 h_i), FP64
-__device__ __forceinline__ Sep<double> separation(const Pos<double>& pi, const Pos<double>& pj, double r,
-                                                  const DevBox& box, const HydroConsts<double>&)
-{
-    double rx = pi.x - pj.x, ry = pi.y - pj.y, rz = pi.z - pj.z;
-    shiftPbc(rx, ry, rz, r, box);
-    return {rx, ry, rz};
-}
-
-//! x_i - x_j from fixed-point coordinates: an exact integer difference, wrapped to the nearest image on periodic
-//! axes, rounded once to FP32
-__device__ __forceinline__ Sep<float> separation(const Pos<float>& pi, const Pos<float>& pj, double,
-                                                 const DevBox&, const HydroConsts<float>& k)
-{
-    int dx = int(unsigned(pi.x) - unsigned(pj.x));
-    int dy = int(unsigned(pi.y) - unsigned(pj.y));
-    int dz = int(unsigned(pi.z) - unsigned(pj.z));
-    return {float(dx) * k.qscale[0], float(dy) * k.qscale[1], float(dz) * k.qscale[2]};
-}
-
-template<class T>
-__device__ __forceinline__ HydroRec<T> loadHydro(const HydroRec<T>* p)
-{
-    HydroRec<T> r;
-    if constexpr (sizeof(T) == 8)
-    {
-        const double4* q = reinterpret_cast<const double4*>(p);
-        double4 a = ldg4(q), b = ldg4(q + 1);
-        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
-    }
-    else
-    {
-        const float4* q = reinterpret_cast<const float4*>(p);
-        float4 a = __ldg(q), b = __ldg(q + 1);
-        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
-    }
-    return r;
-}
-
-template<class T>
-__device__ __forceinline__ GradRec<T> loadGrad(const GradRec<T>* p)
-{
-    GradRec<T> r;
-    if constexpr (sizeof(T) == 8)
-    {
-        const double4* q = reinterpret_cast<const double4*>(p);
-        double4 a = ldg4(q), b = ldg4(q + 1);
-        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
-    }
-    else
-    {
-        const float4* q = reinterpret_cast<const float4*>(p);
-        float4 a = __ldg(q), b = __ldg(q + 1);
-        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
-    }
-    return r;
-}
-
-struct Target
-{
-    size_t i;
-    size_t group;
-    unsigned lane;
-    unsigned count;
-    unsigned ngPad;
-};
-
-__device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned ngmax, Target& t)
-{
-    t.i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-    if (t.i >= n) { return false; }
-    t.group = t.i >> 5;
-    t.lane  = unsigned(t.i & 31);
-    t.count = min(nc[t.i] - 1u, ngmax);
-    t.ngPad = paddedNgmax(ngmax);
-    return true;
-}
-
-//! the 8 neighbour indices of list chunk q0 / 8 of the target (two 16-byte loads of one sector)
-__device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t, unsigned ngPad, unsigned q0,
-                                          uint32_t (&js)[kNbChunk])
-{
-    const uint4* p = reinterpret_cast<const uint4*>(nidx + nidxAt(t.group, ngPad, q0, t.lane));
-    uint4 a = __ldg(p), b = __ldg(p + 1);
-    js[0] = a.x;
-    js[1] = a.y;
-    js[2] = a.z;
-    js[3] = a.w;
-    js[4] = b.x;
-    js[5] = b.y;
-    js[6] = b.z;
-    js[7] = b.w;
-}
+using namespace chain;
 
 // ---------------------------------------------------------------------------------------------------------------
 // XMass: rho0_i = (m_i + sum_j W_ij m_j) K / h_i^3, xm_i = m_i / rho0_i (sph/include/sph/hydro_ve/xmass_kern.hpp:50-79)
@@ -361,6 +106,11 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays
     T kxi      = kxS.get() * (k.K * h3Inv);
     T whomegai = whomegaS.get() * (k.K * h3Inv * hInv);
     T wrho0i   = wrho0S.get() * (k.K * h3Inv * hInv);
+    if (a.tape.whomega)
+    {
+        a.tape.whomega[t.i] = whomegai;
+        a.tape.wrho0[t.i]   = wrho0i;
+    }
     whomegai   = whomegai * mi / xmassi + (kxi - k.K * xmassi * h3Inv) * wrho0i;
     T rhoi     = kxi * mi / xmassi;
     T dhdrho   = -hi / (rhoi * T(3));
@@ -564,6 +314,7 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
     T divvI        = gr.divv;
 
     BlockSum<T> gx, gy, gz;
+    int vsigJ = -1;
     for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
     {
         uint32_t js[kNbChunk];
@@ -582,6 +333,7 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
             T rv           = r.rx * (hr.vx - hj.vx) + r.ry * (hr.vy - hj.vy) + r.rz * (hr.vz - hj.vz);
             T vsig         = T(0);
             if (rv < T(0)) { vsig = ci + hj.c - fdiv(T(3) * rv, dist); }
+            if (!(vijsignalI > vsig)) { vsigJ = int(j); }
             vijsignalI = vijsignalI > vsig ? vijsignalI : vsig;
             T Wi       = KhiInv3 * kernelW(a.wh, k, dist * hiInv);
             T tA1      = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
@@ -598,6 +350,14 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
     }
     T gdx      = gx.get(), gdy = gy.get(), gdz = gz.get();
     T graddivv = sqrt(gdx * gdx + gdy * gdy + gdz * gdz);
+    if (a.tape.gx)
+    {
+        a.tape.gx[t.i]    = gdx;
+        a.tape.gy[t.i]    = gdy;
+        a.tape.gz[t.i]    = gdz;
+        a.tape.vsig[t.i]  = vijsignalI;
+        a.tape.vsigJ[t.i] = vsigJ;
+    }
     T alphaI   = T(a.alpha[t.i]);
     T alphaloc = T(0);
     if (divvI < T(0))
@@ -730,6 +490,11 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArray
             momZ.flush();
             energyS.flush();
             aViscE.flush();
+        }
+        if (a.tape.energy)
+        {
+            a.tape.energy[t.i] = energyS.get();
+            a.tape.avisc[t.i]  = aViscE.get();
         }
         T aViscEnergy = aViscE.get() > T(0) ? aViscE.get() : T(0);
         a.du[t.i] = double(k.K * (prhoi * energyS.get() + T(0.5) * aViscEnergy));

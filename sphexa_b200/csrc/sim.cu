@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "hydro.cuh"
 #include "integrate.cuh"
 #include "neighbors.cuh"
@@ -87,6 +88,16 @@ struct sphb_sim
     uint64_t iteration{1};
     bool uploaded{false};
     bool forcesDone{false};
+
+    // fixed time step (> 0) instead of computeTimestep; required by the step adjoint
+    double fixedDt{0};
+    // adjoint support: when taping, the forward also records what its adjoint needs
+    bool taping{false};
+    DeviceBuffer<double> hPre, alphaPre;
+    DeviceBuffer<char> tapeT;
+    DeviceBuffer<int> tapeJ;
+    DeviceBuffer<char> adjT;
+    DeviceBuffer<double> adjWork, adjScalar;
 
     cudaEvent_t ev[kNumStages + 1]{};
     float stageMs[kNumStages]{};
@@ -298,6 +309,19 @@ ChainArrays<T> chainArrays(sphb_sim& s)
     a.hrec   = reinterpret_cast<HydroRec<T>*>(s.hrec.data());
     a.grec   = reinterpret_cast<GradRec<T>*>(s.grec.data());
     a.reduce = s.reduce.data();
+    if (s.taping)
+    {
+        T* t          = reinterpret_cast<T*>(s.tapeT.data());
+        a.tape.whomega = t;
+        a.tape.wrho0   = t + s.n;
+        a.tape.gx      = t + 2 * s.n;
+        a.tape.gy      = t + 3 * s.n;
+        a.tape.gz      = t + 4 * s.n;
+        a.tape.vsig    = t + 5 * s.n;
+        a.tape.energy  = t + 6 * s.n;
+        a.tape.avisc   = t + 7 * s.n;
+        a.tape.vsigJ   = s.tapeJ.data();
+    }
     return a;
 }
 
@@ -347,6 +371,11 @@ int runChain(sphb_sim& s)
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIad], st));
     SPHB_TRY(launchIadDivvCurlv(a, k, s.box, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sAV], st));
+    if (s.taping)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.alphaPre.data(), s.f[fAlpha].data(), s.n * sizeof(double),
+                                      cudaMemcpyDeviceToDevice, st));
+    }
     SPHB_TRY(launchAVswitches(a, k, s.box, s.minDt, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sMomentum], st));
     SPHB_TRY(launchMomentumEnergy(a, k, s.box, st));
@@ -359,6 +388,11 @@ int computeForces(sphb_sim& s)
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sSync], st));
     SPHB_TRY(syncDomain(s));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sNeighbors], st));
+    if (s.taping)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.hPre.data(), s.f[fH].data(), s.n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                      st));
+    }
 
     unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
     SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
@@ -435,7 +469,7 @@ int runPositions(sphb_sim& s, double cv)
 int integrateStep(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
-    double dtNew    = std::min({s.minDtCourant, s.minDtRho, 1.1 * s.minDt});
+    double dtNew    = s.fixedDt > 0 ? s.fixedDt : std::min({s.minDtCourant, s.minDtRho, 1.1 * s.minDt});
     s.ttot += dtNew;
     s.minDt_m1 = s.minDt;
     s.minDt    = dtNew;
@@ -456,6 +490,70 @@ int integrateStep(sphb_sim& s)
     s.iteration++;
     s.forcesDone = false;
     return flag ? kErrNotConverged : kOk;
+}
+
+int allocateAdjoint(sphb_sim& s)
+{
+    size_t n = s.n;
+    SPHB_TRY(s.hPre.reserve(n));
+    SPHB_TRY(s.alphaPre.reserve(n));
+    SPHB_TRY(s.tapeT.reserve(8 * n * s.elemBytes()));
+    SPHB_TRY(s.tapeJ.reserve(n));
+    SPHB_TRY(s.adjT.reserve(size_t(kNumAdjFields) * n * s.elemBytes()));
+    SPHB_TRY(s.adjWork.reserve(14 * n));
+    SPHB_TRY(s.adjScalar.reserve(1));
+    return kOk;
+}
+
+template<class T>
+int runStepVjp(sphb_sim& s, const double* const* post, double* const* pre, double* alphamaxBar)
+{
+    ChainArrays<T> a = chainArrays<T>(s);
+    HydroConsts<T> k = hydroConsts<T>(s);
+    if (!a.tape.whomega || !a.tape.energy || !a.tape.vsigJ) { return SPHB_ERR_STATE; }
+    AdjointStepArgs args;
+    args.n           = s.n;
+    args.dt          = s.fixedDt;
+    args.dtm1        = s.fixedDt;
+    args.cv          = idealGasCv(s.p.mui, s.p.gamma);
+    args.gamma       = s.p.gamma;
+    args.ng0         = s.p.ng0;
+    args.order       = s.order.data();
+    args.hPre        = s.hPre.data();
+    args.alphaPre    = s.alphaPre.data();
+    args.temp        = s.f[fTemp].data();
+    args.xm1         = s.f[fXm1].data();
+    args.ym1         = s.f[fYm1].data();
+    args.zm1         = s.f[fZm1].data();
+    args.duM1        = s.f[fDuM1].data();
+    args.du          = s.du.data();
+    args.dtAV        = s.minDt;
+    args.alphamaxBar = s.adjScalar.data();
+
+    StateAdj postA, preA, work;
+    for (int f = 0; f < kNumConserved; ++f)
+    {
+        postA.f[f] = const_cast<double*>(post[f]);
+        preA.f[f]  = pre[f];
+        work.f[f]  = s.adjWork.data() + size_t(f) * s.n;
+    }
+    AdjArrays<T> g;
+    T* base = reinterpret_cast<T*>(s.adjT.data());
+    T** slots[kNumAdjFields] = {&g.x,      &g.y,      &g.z,      &g.vx,     &g.vy,     &g.vz,      &g.h,
+                                &g.c,      &g.prho,   &g.alpha,  &g.cij[0], &g.cij[1], &g.cij[2],  &g.cij[3],
+                                &g.cij[4], &g.cij[5], &g.divv,   &g.xm,     &g.vol,    &g.kx,      &g.gradh,
+                                &g.ax,     &g.ay,     &g.az,     &g.du};
+    for (int q = 0; q < kNumAdjFields; ++q)
+    {
+        *slots[q] = base + size_t(q) * s.n;
+    }
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.adjScalar.data(), 0, sizeof(double), s.stream));
+    SPHB_TRY(stepVjp<T>(a, k, s.box, args, postA, preA, g, work, s.stream));
+    double amB = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&amB, s.adjScalar.data(), sizeof(double), cudaMemcpyDeviceToHost, s.stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    if (alphamaxBar) { *alphamaxBar += amB; }
+    return kOk;
 }
 
 } // namespace
@@ -791,4 +889,53 @@ extern "C" int sphb_sim_store_state(sphb_sim* s, double* const* fields, uint64_t
     SPHB_CUDA_TRY(cudaMemcpyAsync(id, s->id.data(), s->n * sizeof(uint64_t), kind, s->stream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SPHB_OK;
+}
+
+extern "C" int sphb_sim_set_fixed_dt(sphb_sim* s, double dt)
+{
+    if (!s || !(dt >= 0.0)) { return SPHB_ERR_ARG; }
+    s->fixedDt = dt;
+    if (dt > 0)
+    {
+        s->minDt    = dt;
+        s->minDt_m1 = dt;
+    }
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_set_params(sphb_sim* s, const sphb_params* p)
+{
+    if (!s || !p) { return SPHB_ERR_ARG; }
+    if (p->ng0 != s->p.ng0 || p->ngmax != s->p.ngmax || p->precision != s->p.precision ||
+        p->sinc_index != s->p.sinc_index || p->bucket_focus != s->p.bucket_focus || !(p->gamma > 1.0))
+    {
+        return SPHB_ERR_ARG;
+    }
+    double minDt = s->p.minDt, minDtM1 = s->p.minDt_m1;
+    s->p          = *p;
+    s->p.minDt    = minDt;
+    s->p.minDt_m1 = minDtM1;
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_step_vjp(sphb_sim* s, const double* const* adj_post, double* const* adj_pre,
+                                 double* alphamax_bar)
+{
+    if (!s || !adj_post || !adj_pre) { return SPHB_ERR_ARG; }
+    for (int f = 0; f < kNumConserved; ++f)
+    {
+        if (!adj_post[f] || !adj_pre[f] || adj_post[f] == adj_pre[f]) { return SPHB_ERR_ARG; }
+    }
+    if (!s->uploaded || !(s->fixedDt > 0)) { return SPHB_ERR_STATE; }
+    if (!s->hPre.data()) { SPHB_TRY(allocateAdjoint(*s)); }
+    // the chain arrays of the recomputed step and of its adjoint both carry the tape pointers
+    s->taping = true;
+    int rc    = computeForces(*s);
+    if (rc == SPHB_OK)
+    {
+        rc = s->mixed ? runStepVjp<float>(*s, adj_post, adj_pre, alphamax_bar)
+                      : runStepVjp<double>(*s, adj_post, adj_pre, alphamax_bar);
+    }
+    s->taping = false;
+    return rc;
 }

@@ -44,7 +44,8 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sim_step", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
             "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches",
             "sphb_sim_stream", "sphb_sim_load_state", "sphb_sim_store_state", "sphb_probe_fma_peak",
-            "sphb_sort_by_key_static", "sphb_sort_by_key_static_max")
+            "sphb_sort_by_key_static", "sphb_sort_by_key_static_max", "sphb_sim_set_fixed_dt",
+            "sphb_sim_set_params", "sphb_sim_step_vjp")
 
 _lib = None
 
@@ -86,6 +87,9 @@ def load() -> C.CDLL:
         "sphb_probe_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
         "sphb_sort_by_key_static": (C.c_int, [P, P, S, C.c_int, P]),
         "sphb_sort_by_key_static_max": (S, []),
+        "sphb_sim_set_fixed_dt": (C.c_int, [P, C.c_double]),
+        "sphb_sim_set_params": (C.c_int, [P, C.POINTER(Params)]),
+        "sphb_sim_step_vjp": (C.c_int, [P, P, P, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -112,6 +112,33 @@ class Simulation:
     def kernel_launches(self) -> int:
         return int(self.lib.sphb_sim_kernel_launches(self.h))
 
+    def set_fixed_dt(self, dt: float):
+        L.check(self.lib.sphb_sim_set_fixed_dt(self.h, float(dt)), "set_fixed_dt")
+
+    def set_params(self, **over):
+        """Change physics parameters between steps (gamma, mui, Kcour, Krho, alphamin, alphamax, decay_constant)."""
+        self.params.update(over)
+        prec = L.SPHB_MIXED if self.precision == "mixed" else L.SPHB_FP64
+        prm = L.make_params(self.params, prec)
+        L.check(self.lib.sphb_sim_set_params(self.h, C.byref(prm)), "set_params")
+
+    def store_state(self, fields, ids, on_device: bool = True):
+        """Copy the 14 conserved fields (CONSERVED_FIELDS order) and ids into the given buffers."""
+        tbl = (C.c_void_p * len(fields))(*[L.ptr(f).value for f in fields])
+        L.check(self.lib.sphb_sim_store_state(self.h, tbl, L.ptr(ids), int(on_device)), "store_state")
+
+    def load_state(self, fields, ids, on_device: bool = True):
+        tbl = (C.c_void_p * len(fields))(*[L.ptr(f).value for f in fields])
+        L.check(self.lib.sphb_sim_load_state(self.h, tbl, L.ptr(ids), int(on_device)), "load_state")
+
+    def step_vjp(self, adj_post, adj_pre) -> float:
+        """Adjoint of one step from the current state (see sphb_sim_step_vjp); returns d/d alphamax."""
+        post = (C.c_void_p * len(adj_post))(*[L.ptr(f).value for f in adj_post])
+        pre = (C.c_void_p * len(adj_pre))(*[L.ptr(f).value for f in adj_pre])
+        am = C.c_double(0.0)
+        L.check(self.lib.sphb_sim_step_vjp(self.h, post, pre, C.byref(am)), "step_vjp")
+        return am.value
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.sphb_sim_destroy(self.h)
