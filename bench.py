@@ -48,6 +48,7 @@ def parse():
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--no-fp64-leg", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (48^3, 20 steps)")
     return ap.parse_args()
 
 
@@ -415,6 +416,8 @@ def run_ours(args, ws, rank, local):
                 "fields": field_errors(main_leg["snap"], fp64["snap"])}}
         fp64["sim_obj"].close()
     main_leg["sim_obj"].close()
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = adjoint_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ic, n)
     if dist is not None:
@@ -422,6 +425,74 @@ def run_ours(args, ws, rank, local):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def adjoint_leg(side=48, steps=20, dt=1e-5, every=5, directions=64, eps=1e-6) -> dict:
+    """Gradient of the final kinetic energy after K fixed-dt steps with respect to the initial internal energy of
+    every particle and alphamax, through the hand-written step adjoints with checkpoints every `every` steps.
+    Times are device-synchronised wall clock around the whole forward (K steps) and the whole backward
+    (checkpoint restores, segment recomputation and K step adjoints). The FP64 gradient is checked against central
+    differences of the FP64 forward on `directions` random directions (relative perturbations u0 (1 + eps xi),
+    alphamax (1 + eps zeta)); the FP32 (mixed) gradient is compared with the FP64 one."""
+    import torch
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.adjoint import AdjointRun, ideal_gas_cv
+    ic = icm.sedov(side)
+    n = ic["x"].size
+    cv = ideal_gas_cv(ic["params"]["mui"], ic["params"]["gamma"])
+    u0 = ic["temp"] * cv
+    am0 = float(ic["params"]["alphamax"])
+    out = {"workload": f"sedov-{side}^3 ({n:,} particles), {steps} steps at fixed dt={dt:g}, objective sum m|v|^2/2 "
+                       f"after the last step, gradient w.r.t. u0 (per particle) and alphamax, checkpoints every "
+                       f"{every} steps with recomputation, neighbour lists frozen per step"}
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, (time.perf_counter() - t0) * 1e3
+
+    grads = {}
+    for prec in ("fp64", "mixed"):
+        run = AdjointRun(ic, prec, dt=dt, steps=steps, checkpoint_every=every)
+        run.forward(u0, am0)
+        run.backward()
+        loss, t_fwd = timed(lambda: run.forward(u0, am0, checkpoints=False))
+        _, t_fwd_ck = timed(lambda: run.forward(u0, am0))
+        nc_base = run.sim.get("nc")
+        (gu, ga), t_bwd = timed(run.backward)
+        grads[prec] = (gu, ga)
+        entry = {"loss": loss, "forward_ms": t_fwd, "forward_with_checkpoints_ms": t_fwd_ck, "backward_ms": t_bwd,
+                 "adjoint_over_forward": t_bwd / t_fwd, "dL_dalphamax": ga,
+                 "dL_du0_norm": float(np.linalg.norm(gu))}
+        if prec == "fp64":
+            rng = np.random.default_rng(2024)
+            errs, changed = [], 0
+            for _ in range(directions):
+                xi = rng.uniform(-1.0, 1.0, n)
+                zeta = rng.uniform(-1.0, 1.0)
+                du, da = xi * u0, zeta * am0
+                lp = run.forward(u0 + eps * du, am0 + eps * da, checkpoints=False)
+                changed += int(not np.array_equal(run.sim.get("nc"), nc_base))
+                lm = run.forward(u0 - eps * du, am0 - eps * da, checkpoints=False)
+                changed += int(not np.array_equal(run.sim.get("nc"), nc_base))
+                fd = (lp - lm) / (2 * eps)
+                ad = float(np.dot(gu, du) + ga * da)
+                errs.append(abs(fd - ad) / max(abs(fd), 1e-300))
+            errs = np.array(errs)
+            entry["finite_differences"] = {"directions": directions, "eps": eps, "max_rel_err": float(errs.max()),
+                                           "median_rel_err": float(np.median(errs)),
+                                           "within_1e-4": int((errs <= 1e-4).sum()),
+                                           "runs_with_changed_neighbour_counts": changed}
+        run.close()
+        out[prec] = entry
+    g64, a64 = grads["fp64"]
+    g32, a32 = grads["mixed"]
+    out["fp32_vs_fp64"] = {"dL_du0_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
+                           "dL_du0_max_rel_to_max": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64))),
+                           "dL_dalphamax_rel": abs(a32 - a64) / max(abs(a64), 1e-300)}
+    return out
 
 
 def host_threads() -> int:

@@ -38,6 +38,7 @@ class AdjointRun:
         self.n = int(ic["x"].size)
         self.cv = ideal_gas_cv(ic["params"]["mui"], ic["params"]["gamma"])
         self.sim = None
+        self.initial = None
         self.checkpoints = {}
         self.forward_steps = 0
 
@@ -74,9 +75,20 @@ class AdjointRun:
 
     # forward and backward -------------------------------------------------------------------------------------
     def forward(self, u0: np.ndarray, alphamax: float, checkpoints: bool = True) -> float:
-        if self.sim is not None:
-            self.sim.close()
-        self.sim = self._make_sim(u0, alphamax)
+        """Run the K steps from u0 (initial-condition order) and alphamax; returns the final kinetic energy.
+        The first call builds the simulation; later calls restore its initial state with the new u0 and alphamax
+        (the physics does not depend on the domain bookkeeping a fresh simulation would rebuild)."""
+        if self.sim is None:
+            self.sim = self._make_sim(u0, alphamax)
+            self.initial = self._store()
+        else:
+            fields, ids = self.initial
+            fields = [f.clone() for f in fields]
+            order = ids.cpu().numpy()
+            temp = np.asarray(u0, dtype=np.float64)[order] / self.cv
+            fields[FIELD_INDEX["temp"]] = self.torch.from_numpy(temp).cuda()
+            self.sim.load_state(fields, ids)
+            self.sim.set_params(alphamax=float(alphamax))
         self.checkpoints = {}
         for s in range(self.steps):
             if checkpoints and s % self.every == 0:
@@ -122,6 +134,7 @@ class AdjointRun:
         if self.sim is not None:
             self.sim.close()
             self.sim = None
+            self.initial = None
 
 
 def kinetic_energy_function():
