@@ -219,7 +219,58 @@ int sphb_sim_set_params(sphb_sim* sim, const sphb_params* params);
 int sphb_sim_step_vjp(sphb_sim* sim, const double* const* adj_post, double* const* adj_pre, double* alphamax_bar);
 
 /* ---------------------------------------------------------------------------------------------------------------- */
-/* 4. Measurement helper                                                                                            */
+/* 4. Batched ensemble                                                                                              */
+/* ---------------------------------------------------------------------------------------------------------------- */
+
+/*! Many independent simulations stepped together: every stage of the VE step runs as one launch over all instances,
+ *  the step has no host synchronisation, and sphb_ensemble_step replays it as one captured CUDA graph. Each instance
+ *  evolves exactly as an sphb_sim of the same particles and parameters would. No counterpart in the reference (it
+ *  runs one simulation per process). */
+typedef struct sphb_ensemble sphb_ensemble;
+
+/*! num instances (1..254) with sizes[k] particles each, in one periodic box shared by all. params[k] per instance:
+ *  gamma, mui, minDt and minDt_m1 may differ; ng0, ngmax, precision, sinc_index, bucket_focus, Kcour, Krho and the
+ *  AV constants must be equal (SPHB_ERR_ARG otherwise). Open boundaries are not supported (SPHB_ERR_ARG). */
+int sphb_ensemble_create(sphb_ensemble** ens, int num, const size_t* sizes, const sphb_box* box,
+                         const sphb_params* params);
+
+int sphb_ensemble_destroy(sphb_ensemble* ens);
+
+/*! The 14 conserved fields and ids of instance k (as sphb_sim_upload). */
+int sphb_ensemble_upload(sphb_ensemble* ens, int k, const double* const* fields, const uint64_t* id, int on_device);
+
+/*! Sort every instance into SFC order and build its trees (host-driven; after all uploads). */
+int sphb_ensemble_initial_sync(sphb_ensemble* ens);
+
+/*! Rebuild the per-instance focus trees from the current particle order (outside the captured step). */
+int sphb_ensemble_rebuild_trees(sphb_ensemble* ens);
+
+/*! Block sizes (multiples of 32, at most 256) of the five J-loop launches: XMass, VeDefGradh+EOS, IAD+divv/curlv,
+ *  AV switches, MomentumEnergy. */
+int sphb_ensemble_set_threads(sphb_ensemble* ens, const int* threads5);
+
+/*! Time every J-loop at 64, 128 and 256 threads per block on the current state, keep the fastest, and write the
+ *  choice to threads5_out (5 ints, may be null). The particle state is unchanged. */
+int sphb_ensemble_autotune(sphb_ensemble* ens, int* threads5_out);
+
+/*! Advance every instance by steps steps; use_graph != 0 replays one captured step (captured on first use). */
+int sphb_ensemble_step(sphb_ensemble* ens, int steps, int use_graph);
+
+/*! Number of particles of instance k. */
+size_t sphb_ensemble_size(const sphb_ensemble* ens, int k);
+
+/*! Field of instance k by name (as sphb_sim_get_field), n_k doubles in host memory, in the instance's SFC order. */
+int sphb_ensemble_get_field(sphb_ensemble* ens, int k, const char* name, double* out);
+
+/*! Scalars of instance k: minDt, minDt_m1, ttot, etot, ecin, eint, linmom, angmom, totalNeighbors (9 doubles; the
+ *  conserved quantities of the last force computation). */
+int sphb_ensemble_scalars(sphb_ensemble* ens, int k, double* out);
+
+/*! The CUDA stream of the ensemble. */
+void* sphb_ensemble_stream(sphb_ensemble* ens);
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* 5. Measurement helper                                                                                            */
 /* ---------------------------------------------------------------------------------------------------------------- */
 
 /*! Measure the CUDA-core FMA throughput of the current device: which = 0 for FP32, 1 for FP64. Runs a short

@@ -241,10 +241,12 @@ struct Target
     unsigned ngPad;
 };
 
-__device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned ngmax, Target& t)
+__device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned ngmax, Target& t,
+                                         const uint8_t* inst = nullptr)
 {
     t.i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
     if (t.i >= n) { return false; }
+    if (inst && inst[t.i] == kGhost) { return false; }
     t.group = t.i >> 5;
     t.lane  = unsigned(t.i & 31);
     t.count = min(nc[t.i] - 1u, ngmax);
@@ -266,6 +268,48 @@ __device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t,
     js[5] = b.y;
     js[6] = b.z;
     js[7] = b.w;
+}
+
+/*! Maximum (kMax) or minimum of one double per thread, published as ordered bits with one atomic per block on
+ *  *single (one simulation), or one atomic per warp on the warp's instance slot batch.reduce[2 q + slot] (an ensemble:
+ *  a warp never spans two instances). Every thread of the block must call it. */
+template<bool kMax>
+__device__ __forceinline__ void reduceOrdered(double v, size_t n, unsigned long long* single, const BatchView& batch,
+                                              int slot)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        double o = __shfl_xor_sync(0xffffffffu, v, off);
+        v        = kMax ? fmax(v, o) : fmin(v, o);
+    }
+    if (batch.inst)
+    {
+        size_t first = blockIdx.x * size_t(blockDim.x) + (threadIdx.x & ~31u);
+        if ((threadIdx.x & 31) == 0 && first < n)
+        {
+            uint8_t q = batch.inst[first];
+            if (q != kGhost)
+            {
+                if (kMax) { atomicMax(batch.reduce + 2 * q + slot, orderedBits(v)); }
+                else { atomicMin(batch.reduce + 2 * q + slot, orderedBits(v)); }
+            }
+        }
+        return;
+    }
+    __shared__ double warpVal[kChainMaxThreads / 32];
+    if ((threadIdx.x & 31) == 0) { warpVal[threadIdx.x >> 5] = v; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        double m = warpVal[0];
+        for (int w = 1; w < int(blockDim.x >> 5); ++w)
+        {
+            m = kMax ? fmax(m, warpVal[w]) : fmin(m, warpVal[w]);
+        }
+        if (kMax) { atomicMax(single, orderedBits(m)); }
+        else { atomicMin(single, orderedBits(m)); }
+    }
 }
 
 } // namespace chain

@@ -17,6 +17,21 @@ constexpr unsigned kMaxLevel  = 21;
 constexpr uint64_t kRootRange = uint64_t(1) << 63;
 //! the key that flags a particle for removal; it sorts after every valid key (definitions.h:70-75)
 constexpr uint64_t kRemoveKey = uint64_t(1) << 63;
+
+//! instance index of a padding slot in a batched ensemble
+constexpr uint8_t kGhost = 255;
+
+/*! Per-slot instance map and per-instance values of a batched ensemble step (all null for one simulation). Instances
+ *  occupy 32-aligned runs of slots, padded with ghost slots, so a warp group never spans two instances. */
+struct BatchView
+{
+    const uint8_t* inst{nullptr};         // per slot: instance index, kGhost for padding
+    const double* gamma{nullptr};         // per instance
+    const double* cv{nullptr};            // per instance
+    const double* dt{nullptr};            // per instance: the step being taken (AV switches: the previous one)
+    const double* dtm1{nullptr};          // per instance: the step before
+    unsigned long long* reduce{nullptr};  // per instance: [2k] max divv, [2k+1] min Courant dt (ordered bits)
+};
 constexpr int kTableSize      = 20000;
 constexpr int kWarp           = 32;
 

@@ -9,6 +9,9 @@ namespace sphb
 //! number of coefficients of the FP32 polynomial kernel (degree 12 in t)
 constexpr int kPolyTerms = 13;
 
+//! largest block size a J-loop launch may use (ChainArrays::threads; the ensemble autotuner picks 64, 128 or 256)
+constexpr int kChainMaxThreads = 256;
+
 //! physics constants of one simulation, in the J-loop type T
 template<class T>
 struct HydroConsts
@@ -99,6 +102,8 @@ struct ChainArrays
     // reduction outputs: [0] max divv (ordered bits), [1] min Courant dt (ordered bits)
     unsigned long long* reduce;
     ChainTape<T> tape;
+    BatchView batch;
+    int threads{128}; // block size of the J-loop launches
 };
 
 template<class T>

@@ -27,10 +27,10 @@ using namespace chain;
 // XMass: rho0_i = (m_i + sum_j W_ij m_j) K / h_i^3, xm_i = m_i / rho0_i (sph/include/sph/hydro_ve/xmass_kern.hpp:50-79)
 // ---------------------------------------------------------------------------------------------------------------
 template<class T>
-__global__ void __launch_bounds__(kChainThreads) xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads) xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
+    if (!targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst)) { return; }
     Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
@@ -64,10 +64,10 @@ __global__ void __launch_bounds__(kChainThreads) xmassKernel(ChainArrays<T> a, H
 // sph/include/sph/eos.hpp:19-50); writes kx, gradh, prho, c and the hydro record of the particle.
 // ---------------------------------------------------------------------------------------------------------------
 template<class T>
-__global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
+    if (!targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst)) { return; }
     Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
@@ -117,11 +117,18 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhEosKernel(ChainArrays
     T gradhi   = T(1) - dhdrho * whomegai;
 
     // EOS in FP64 (per particle): rho = kx m / xm, p = rho u (gamma - 1), c = sqrt(gamma u (gamma - 1))
+    double gamma = k.gamma, cv = k.cv;
+    if (a.batch.inst)
+    {
+        uint8_t q = a.batch.inst[t.i];
+        gamma     = a.batch.gamma[q];
+        cv        = a.batch.cv[q];
+    }
     double rho  = double(kxi) * double(mi) / double(xmassi);
-    double u    = k.cv * a.temp[t.i];
-    double tmp  = u * (k.gamma - 1.0);
+    double u    = cv * a.temp[t.i];
+    double tmp  = u * (gamma - 1.0);
     double p    = rho * tmp;
-    double c    = sqrt(k.gamma * tmp);
+    double c    = sqrt(gamma * tmp);
     double prho = p / (double(kxi) * double(mi) * double(mi) * double(gradhi));
 
     a.kx[t.i]    = kxi;
@@ -143,10 +150,10 @@ __device__ __forceinline__ int expOf(T v)
 }
 
 template<class T>
-__global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid     = targetOf(a.n, a.nc, k.ngmax, t);
+    bool valid     = targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst);
     double divvOut = -INFINITY;
     if (valid)
     {
@@ -271,36 +278,18 @@ __global__ void __launch_bounds__(kChainThreads) iadDivvCurlvKernel(ChainArrays<
         a.grec[t.i]   = GradRec<T>{c11i, c12i, c13i, c22i, c23i, c33i, divv, T(a.alpha[t.i])};
         divvOut       = double(divv);
     }
-    // block max of divv -> one atomic per block
-    double v = divvOut;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
-    }
-    __shared__ double warpMax[kChainThreads / 32];
-    if ((threadIdx.x & 31) == 0) { warpMax[threadIdx.x >> 5] = v; }
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        double m = warpMax[0];
-        for (int w = 1; w < kChainThreads / 32; ++w)
-        {
-            m = fmax(m, warpMax[w]);
-        }
-        atomicMax(a.reduce + 0, orderedBits(m));
-    }
+    reduceOrdered<true>(divvOut, a.n, a.reduce + 0, a.batch, 0);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
 // AV switches (sph/include/sph/hydro_ve/av_switches_kern.hpp:43-137)
 // ---------------------------------------------------------------------------------------------------------------
 template<class T>
-__global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box,
+__global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box,
                                                                   double dt)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t)) { return; }
+    if (!targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst)) { return; }
     Pos<T> pi      = posOf(a, t.i);
     double hiD     = a.h[t.i];
     HydroRec<T> hr = a.hrec[t.i];
@@ -370,7 +359,8 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
     {
         T decay    = hi / (k.decay * vijsignalI);
         T alphadot = alphaloc >= k.alphamin ? (alphaloc - alphaI) / decay : (k.alphamin - alphaI) / decay;
-        alphaI += alphadot * T(dt);
+        double dtq = a.batch.inst ? a.batch.dt[a.batch.inst[t.i]] : dt;
+        alphaI += alphadot * T(dtq);
     }
     a.alpha[t.i]      = double(alphaI);
     a.grec[t.i].alpha = alphaI; // the alpha slot of the record is not read by this kernel
@@ -382,10 +372,10 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesKernel(ChainArrays<T>
 // (tsKCourant, kernels.hpp:10-17) reduced to the minimum.
 // ---------------------------------------------------------------------------------------------------------------
 template<class T>
-__global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid   = targetOf(a.n, a.nc, k.ngmax, t);
+    bool valid   = targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst);
     double dtMin = INFINITY;
     if (valid)
     {
@@ -505,30 +495,13 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyKernel(ChainArray
         double v = maxvsignalI > T(0) ? double(maxvsignalI) : double(ci);
         dtMin    = hiD > 0.0 ? k.Kcour * hiD / v : INFINITY;
     }
-    double m = dtMin;
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        m = fmin(m, __shfl_xor_sync(0xffffffffu, m, off));
-    }
-    __shared__ double warpMin[kChainThreads / 32];
-    if ((threadIdx.x & 31) == 0) { warpMin[threadIdx.x >> 5] = m; }
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        double b = warpMin[0];
-        for (int w = 1; w < kChainThreads / 32; ++w)
-        {
-            b = fmin(b, warpMin[w]);
-        }
-        atomicMin(a.reduce + 1, orderedBits(b));
-    }
+    reduceOrdered<false>(dtMin, a.n, a.reduce + 1, a.batch, 1);
 }
 
 template<class T>
 unsigned chainBlocks(const ChainArrays<T>& a)
 {
-    return ceilDiv(a.n, kChainThreads);
+    return ceilDiv(a.n, size_t(a.threads));
 }
 
 } // namespace
@@ -537,7 +510,7 @@ template<class T>
 int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    xmassKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    xmassKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -547,7 +520,7 @@ template<class T>
 int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    veDefGradhEosKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    veDefGradhEosKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -557,7 +530,7 @@ template<class T>
 int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    iadDivvCurlvKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    iadDivvCurlvKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -567,7 +540,7 @@ template<class T>
 int launchAVswitches(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, double dt, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    avSwitchesKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box, dt);
+    avSwitchesKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box, dt);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -577,7 +550,7 @@ template<class T>
 int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    momentumEnergyKernel<T><<<chainBlocks(a), kChainThreads, 0, s>>>(a, k, box);
+    momentumEnergyKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

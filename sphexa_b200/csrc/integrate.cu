@@ -49,6 +49,14 @@ __global__ void positionsKernel(size_t n, IntegrateArrays<T> a, DevBox box, doub
 {
     size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
     if (i >= n) { return; }
+    if (a.batch.inst)
+    {
+        uint8_t q = a.batch.inst[i];
+        if (q == kGhost) { return; }
+        dt   = a.batch.dt[q];
+        dtm1 = a.batch.dtm1[q];
+        cv   = a.batch.cv[q];
+    }
     double X[3]  = {a.x[i], a.y[i], a.z[i]};
     double A[3]  = {double(a.ax[i]), double(a.ay[i]), double(a.az[i])};
     double dX[3] = {a.xm1[i], a.ym1[i], a.zm1[i]};
@@ -79,10 +87,12 @@ __global__ void positionsKernel(size_t n, IntegrateArrays<T> a, DevBox box, doub
 
 /*! end-of-step smoothing length: h * 0.5 (1 + 1023 ng0/nc)^(1/10); nc <= 1 flags the particle for removal
  *  (sph/include/sph/update_h.hpp:12-33) */
-__global__ void updateHKernel(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag)
+__global__ void updateHKernel(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag,
+                              const uint8_t* inst)
 {
     size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
     if (i >= n) { return; }
+    if (inst && inst[i] == kGhost) { return; }
     unsigned c = nc[i];
     if (c <= 1)
     {
@@ -210,10 +220,10 @@ int launchPositions(size_t n, const IntegrateArrays<T>& a, const DevBox& box, do
 }
 
 int launchUpdateH(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag,
-                  cudaStream_t s)
+                  cudaStream_t s, const uint8_t* inst)
 {
     if (n == 0) { return kOk; }
-    updateHKernel<<<ceilDiv(n, 256), 256, 0, s>>>(n, ng0, nc, h, keys, flag);
+    updateHKernel<<<ceilDiv(n, 256), 256, 0, s>>>(n, ng0, nc, h, keys, flag, inst);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

@@ -16,6 +16,7 @@ struct IntegrateArrays
     double* duM1;
     const double* du;
     const T *ax, *ay, *az;
+    BatchView batch; // an ensemble: per-instance dt, dtm1, cv; padding slots skipped
 };
 
 //! the fixed-point frame of the FP32 J-loops: q = (x - lo) * invUnit, x - lo = q * unit
@@ -37,7 +38,7 @@ int launchPositions(size_t n, const IntegrateArrays<T>& a, const DevBox& box, do
                     cudaStream_t s);
 
 int launchUpdateH(size_t n, unsigned ng0, const unsigned* nc, double* h, uint64_t* keys, unsigned* flag,
-                  cudaStream_t s);
+                  cudaStream_t s, const uint8_t* inst = nullptr);
 
 //! eKin (sum m v^2), eInt, linear momentum (3), angular momentum (3), sum nc -> out9 (device)
 int conservedSums(size_t n, const double* x, const double* y, const double* z, const double* vx, const double* vy,

@@ -117,7 +117,9 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                                                                   const double* __restrict__ z, double* h, size_t n,
                                                                   TreeView tree, DevBox box, NeighborParams prm,
                                                                   uint32_t* __restrict__ nidx,
-                                                                  unsigned* __restrict__ ncOut, unsigned* status)
+                                                                  unsigned* __restrict__ ncOut, unsigned* status,
+                                                                  const TreeView* __restrict__ views,
+                                                                  const uint8_t* __restrict__ inst)
 {
     __shared__ NbShared sh;
     const int warp         = threadIdx.x / kWarp;
@@ -126,8 +128,11 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
     const size_t group     = size_t(blockIdx.x) * kNbWarps + warp;
     if (group >= numGroups) { return; }
 
-    const size_t i   = group * kWarp + lane;
-    const bool valid = i < n;
+    const size_t i = group * kWarp + lane;
+    // an ensemble: the group's instance (its first slot is never padding) selects the tree; padding slots idle
+    TreeView tv = tree;
+    if (views) { tv = views[inst[group * kWarp]]; }
+    const bool valid = i < n && !(inst && inst[i] == kGhost);
     const double xi  = valid ? x[i] : 0.0;
     const double yi  = valid ? y[i] : 0.0;
     const double zi  = valid ? z[i] : 0.0;
@@ -286,8 +291,8 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                     int c = b / kBlockSize + (t - blkPre[rr]);
                     ps    = max(c * kBlockSize, b);
                     plen  = min(c * kBlockSize + kBlockSize, e) - ps;
-                    float4 lo = __ldg(tree.blockLo + c);
-                    float4 hb = __ldg(tree.blockHi + c);
+                    float4 lo = __ldg(tv.blockLo + c);
+                    float4 hb = __ldg(tv.blockHi + c);
                     float bl[3] = {lo.x, lo.y, lo.z};
                     float bh[3] = {hb.x, hb.y, hb.z};
                     keep = plen > 0;
@@ -362,15 +367,15 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         {
             int node = stack[sp - 1];
             --sp;
-            int child0 = tree.childOffsets[node];
+            int child0 = tv.childOffsets[node];
             if (child0 == 0)
             {
                 if (numLeaves == kLeafCap) { flush(); }
                 if (lane == 0)
                 {
-                    int leaf             = tree.nodeToLeaf[node];
-                    leafFirst[numLeaves] = tree.layout[leaf];
-                    leafEnd[numLeaves]   = tree.layout[leaf + 1];
+                    int leaf             = tv.nodeToLeaf[node];
+                    leafFirst[numLeaves] = tv.layout[leaf];
+                    leafEnd[numLeaves]   = tv.layout[leaf + 1];
                 }
                 ++numLeaves;
                 __syncwarp();
@@ -384,9 +389,9 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
                 {
-                    double d = tree.centers[3 * c + k] - gc[k];
+                    double d = tv.centers[3 * c + k] - gc[k];
                     if (box.periodic[k]) { d -= box.len[k] * rint(d * box.ilen[k]); }
-                    ov = ov && fabs(d) <= gs[k] + tree.sizes[3 * c + k] * (1.0 + 1e-12);
+                    ov = ov && fabs(d) <= gs[k] + tv.sizes[3 * c + k] * (1.0 + 1e-12);
                 }
             }
             unsigned m = __ballot_sync(0xffffffffu, ov) & 0xffu;
@@ -475,12 +480,14 @@ int computeBlockBoxes(const double* x, const double* y, const double* z, size_t 
 
 int findNeighbors(const double* x, const double* y, const double* z, double* h, size_t n, const TreeView& tree,
                   const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc, unsigned* status,
-                  cudaStream_t stream)
+                  cudaStream_t stream, const TreeView* views, const uint8_t* inst)
 {
     if (n == 0) { return kOk; }
+    if ((views == nullptr) != (inst == nullptr)) { return kErrArg; }
     size_t numGroups = (n + kWarp - 1) / kWarp;
     unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
-    findNeighborsKernel<<<blocks, kNbThreads, 0, stream>>>(x, y, z, h, n, tree, box, prm, nidx, nc, status);
+    findNeighborsKernel<<<blocks, kNbThreads, 0, stream>>>(x, y, z, h, n, tree, box, prm, nidx, nc, status, views,
+                                                           inst);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

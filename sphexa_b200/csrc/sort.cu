@@ -249,6 +249,17 @@ size_t sortScratchBytes(size_t n)
            256;
 }
 
+namespace
+{
+int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, unsigned passMask,
+              cudaStream_t stream);
+
+__global__ void orErrorKernel(const uint32_t* err, uint32_t* out)
+{
+    if (*err) { atomicOr(out, 1u); }
+}
+} // namespace
+
 int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,
               cudaStream_t stream)
 {
@@ -282,6 +293,47 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
         }
     }
 
+    unsigned mask = 0;
+    for (int p = 0; p < kPasses; ++p)
+    {
+        mask |= doPass[p] ? (1u << p) : 0u;
+    }
+    SPHB_TRY(runPasses(keys, values, n, s, mask, stream));
+    uint32_t err = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    return err ? kErrCapacity : kOk;
+}
+
+int sortByKeyAsync(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,
+                   unsigned passMask, uint32_t* errorOut, cudaStream_t stream)
+{
+    if (n == 0) { return kOk; }
+    if (n >= (size_t(1) << 30)) { return kErrArg; }
+    if (!scratch || scratchBytes < sortScratchBytes(n)) { return kErrCapacity; }
+    SortScratch s = carve(scratch, n);
+    if (initValues)
+    {
+        iotaKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(values, n);
+        SPHB_CUDA_TRY(cudaGetLastError());
+    }
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.hist, 0, kPasses * kRadix * sizeof(uint32_t), stream));
+    unsigned histBlocks = unsigned(std::min<size_t>(ceilDiv(n, 256 * 16), size_t(smCount()) * 4));
+    histogramKernel<<<histBlocks, 256, 0, stream>>>(keys, n, s.hist);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    SPHB_TRY(runPasses(keys, values, n, s, passMask, stream));
+    if (errorOut) { orErrorKernel<<<1, 1, 0, stream>>>(s.counters + 1, errorOut); }
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+namespace
+{
+
+//! scan the histograms and run the passes of passMask (bit p: digit p), leaving the result in keys/values
+int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, unsigned passMask,
+              cudaStream_t stream)
+{
     histScanKernel<<<kPasses, kRadix, 0, stream>>>(s.hist);
     SPHB_CUDA_TRY(cudaGetLastError());
     SPHB_CUDA_TRY(cudaMemsetAsync(s.counters + 1, 0, sizeof(uint32_t), stream));
@@ -293,7 +345,7 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
     uint32_t* vOut    = s.valsAlt;
     for (int p = 0; p < kPasses; ++p)
     {
-        if (!doPass[p]) { continue; }
+        if (!(passMask & (1u << p))) { continue; }
         SPHB_CUDA_TRY(cudaMemsetAsync(s.status, 0, tiles * kRadix * sizeof(uint32_t), stream));
         SPHB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(uint32_t), stream));
         onesweepKernel<<<unsigned(tiles), kSortThreads, 0, stream>>>(kIn, vIn, kOut, vOut, n, p * kRadixBits,
@@ -307,11 +359,10 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
         SPHB_CUDA_TRY(cudaMemcpyAsync(keys, kIn, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream));
         SPHB_CUDA_TRY(cudaMemcpyAsync(values, vIn, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
     }
-    uint32_t err = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
-    return err ? kErrCapacity : kOk;
+    return kOk;
 }
+
+} // namespace
 
 // ---------------------------------------------------------------------------------------------------------------
 // Allocation-free variant: the scratch lives in a fixed device array of this library (see sphb_sort_by_key_static)
