@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--no-fp64-leg", action="store_true", help="skip the plain FP64 comparison leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (48^3, 20 steps)")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-instance ensemble leg")
     return ap.parse_args()
 
 
@@ -418,6 +419,8 @@ def run_ours(args, ws, rank, local):
     main_leg["sim_obj"].close()
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = adjoint_leg()
+    if rank == 0 and not args.no_ensemble:
+        line["ensemble"] = ensemble_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ic, n)
     if dist is not None:
@@ -493,6 +496,64 @@ def adjoint_leg(side=48, steps=20, dt=1e-5, every=5, directions=64, eps=1e-6) ->
                            "dL_du0_max_rel_to_max": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64))),
                            "dL_dalphamax_rel": abs(a32 - a64) / max(abs(a64), 1e-300)}
     return out
+
+
+def ensemble_config(num=64, seed=4, lo=20, hi=64):
+    """Members of the batched-ensemble workload: side uniform in [lo, hi], blast energy uniform in [0.5, 2], gamma in
+    {1.4, 5/3}, each member its own lattice seed (splitmix64 streams, so the set is the same everywhere)."""
+    from sphexa_b200.ic import uniform01
+    u = uniform01(seed, np.arange(3 * num, dtype=np.uint64), 7)
+    sides = [lo + min(int(u[3 * k] * (hi - lo + 1)), hi - lo) for k in range(num)]
+    energies = [0.5 + 1.5 * float(u[3 * k + 1]) for k in range(num)]
+    gammas = [1.4 if u[3 * k + 2] < 0.5 else 5.0 / 3.0 for k in range(num)]
+    return sides, energies, gammas
+
+
+def ensemble_leg(num=64, steps=20) -> dict:
+    """num uneven Sedov instances advanced `steps` steps in mixed precision: one batched ensemble (autotuned launch
+    shapes, one captured graph replayed per step) against the same instances run one after another as single
+    simulations. Device-synchronised wall clock around the stepping of each (set-up excluded for both); the final
+    states of the first and last member are compared bit for bit."""
+    import torch
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.ensemble import Ensemble
+    from sphexa_b200.simulation import Simulation
+    sides, energies, gammas = ensemble_config(num)
+    ics = [icm.sedov(s, seed=100 + k, energy=e, gamma=g) for k, (s, e, g) in enumerate(zip(sides, energies, gammas))]
+    total = sum(ic["x"].size for ic in ics)
+
+    ens = Ensemble(ics, "mixed")
+    choice = ens.autotune()
+    ens.step(0, graph=True)  # capture
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc = ens.step(steps, graph=True)
+    torch.cuda.synchronize()
+    t_ens = time.perf_counter() - t0
+    launches = None
+    finals = {k: ens.get(k, "x") for k in (0, num - 1)}
+    ens.close()
+
+    t_seq = 0.0
+    same = True
+    for k, ic in enumerate(ics):
+        sim = Simulation(ic, "mixed")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            sim.step()
+        torch.cuda.synchronize()
+        t_seq += time.perf_counter() - t0
+        if k in finals:
+            same = same and bool(np.array_equal(finals[k], sim.get("x")))
+        sim.close()
+    return {"workload": f"{num} Sedov instances, sides {min(sides)}..{max(sides)} (seeded), {total:,} particles in "
+                        f"total, blast energy U[0.5,2], gamma in {{1.4, 5/3}}, {steps} steps, mixed precision",
+            "instances": num, "particles": total, "steps": steps,
+            "ensemble": {"seconds": t_ens, "particle_steps_per_s": total * steps / t_ens, "status": rc,
+                         "autotuned_threads": choice},
+            "sequential": {"seconds": t_seq, "particle_steps_per_s": total * steps / t_seq},
+            "speedup": t_seq / t_ens, "first_and_last_member_bit_identical": same}
 
 
 def host_threads() -> int:
