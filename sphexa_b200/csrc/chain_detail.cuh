@@ -12,6 +12,10 @@ namespace chain
 
 constexpr int kChainThreads = 128;
 
+//! compile-time variants of the J-loop kernels: write the adjoint's tape, or run over a batched ensemble
+constexpr int kModeTape  = 1;
+constexpr int kModeBatch = 2;
+
 /*! Neighbour-sum accumulator. FP64: every term is added as it comes, in list order (the reference's order).
  *  FP32: terms are summed plainly within one list chunk of 8 neighbours and each chunk sum is added to a
  *  Kahan-compensated accumulator; explicit round-to-nearest intrinsics keep the compiler from fusing or reordering
@@ -273,7 +277,7 @@ __device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t,
 /*! Maximum (kMax) or minimum of one double per thread, published as ordered bits with one atomic per block on
  *  *single (one simulation), or one atomic per warp on the warp's instance slot batch.reduce[2 q + slot] (an ensemble:
  *  a warp never spans two instances). Every thread of the block must call it. */
-template<bool kMax>
+template<bool kMax, bool kBatched>
 __device__ __forceinline__ void reduceOrdered(double v, size_t n, unsigned long long* single, const BatchView& batch,
                                               int slot)
 {
@@ -283,7 +287,7 @@ __device__ __forceinline__ void reduceOrdered(double v, size_t n, unsigned long 
         double o = __shfl_xor_sync(0xffffffffu, v, off);
         v        = kMax ? fmax(v, o) : fmin(v, o);
     }
-    if (batch.inst)
+    if constexpr (kBatched)
     {
         size_t first = blockIdx.x * size_t(blockDim.x) + (threadIdx.x & ~31u);
         if ((threadIdx.x & 31) == 0 && first < n)

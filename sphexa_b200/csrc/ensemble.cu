@@ -589,7 +589,7 @@ int stepBatched(sphb_ensemble& e)
     countLaunch();
     TreeView dummy{};
     NeighborParams np{e.p.ng0, e.p.ngmax, 10};
-    SPHB_TRY(findNeighbors(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.f[3].data(), n, dummy, e.box, np,
+    SPHB_TRY(findNeighbors(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy, e.box, np,
                            e.nidx.data(), e.nc.data(), e.status.data(), st, e.views.data(), e.inst.data()));
     if (e.mixed) { SPHB_TRY(runChainBatched<float>(e)); }
     else { SPHB_TRY(runChainBatched<double>(e)); }
@@ -859,7 +859,7 @@ extern "C" int sphb_ensemble_autotune(sphb_ensemble* e, int* threads_out)
     SPHB_CUDA_TRY(cudaMemcpyAsync(e->hBackup.data(), e->f[3].data(), n * sizeof(double), cudaMemcpyDeviceToDevice, st));
     TreeView dummy{};
     NeighborParams np{e->p.ng0, e->p.ngmax, 10};
-    SPHB_TRY(findNeighbors(e->f[0].data(), e->f[1].data(), e->f[2].data(), e->f[3].data(), n, dummy, e->box, np,
+    SPHB_TRY(findNeighbors(e->f[0].data(), e->f[1].data(), e->f[2].data(), e->pos.data(), e->f[3].data(), n, dummy, e->box, np,
                            e->nidx.data(), e->nc.data(), e->status.data(), st, e->views.data(), e->inst.data()));
     SPHB_CUDA_TRY(cudaMemcpyAsync(e->alphaBackup.data(), e->f[13].data(), n * sizeof(double),
                                   cudaMemcpyDeviceToDevice, st));

@@ -26,11 +26,11 @@ using namespace chain;
 // ---------------------------------------------------------------------------------------------------------------
 // XMass: rho0_i = (m_i + sum_j W_ij m_j) K / h_i^3, xm_i = m_i / rho0_i (sph/include/sph/hydro_ve/xmass_kern.hpp:50-79)
 // ---------------------------------------------------------------------------------------------------------------
-template<class T>
+template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst)) { return; }
+    if (!targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr)) { return; }
     Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
@@ -63,11 +63,11 @@ __global__ void __launch_bounds__(kChainMaxThreads) xmassKernel(ChainArrays<T> a
 // VeDefGradh (sph/include/sph/hydro_ve/ve_def_gradh_kern.hpp:43-90) + ideal-gas EOS (hydro_ve/eos.hpp:52-94,
 // sph/include/sph/eos.hpp:19-50); writes kx, gradh, prho, c and the hydro record of the particle.
 // ---------------------------------------------------------------------------------------------------------------
-template<class T>
+template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst)) { return; }
+    if (!targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr)) { return; }
     Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArr
     T kxi      = kxS.get() * (k.K * h3Inv);
     T whomegai = whomegaS.get() * (k.K * h3Inv * hInv);
     T wrho0i   = wrho0S.get() * (k.K * h3Inv * hInv);
-    if (a.tape.whomega)
+    if constexpr (kMode & kModeTape)
     {
         a.tape.whomega[t.i] = whomegai;
         a.tape.wrho0[t.i]   = wrho0i;
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArr
 
     // EOS in FP64 (per particle): rho = kx m / xm, p = rho u (gamma - 1), c = sqrt(gamma u (gamma - 1))
     double gamma = k.gamma, cv = k.cv;
-    if (a.batch.inst)
+    if constexpr (kMode & kModeBatch)
     {
         uint8_t q = a.batch.inst[t.i];
         gamma     = a.batch.gamma[q];
@@ -149,11 +149,11 @@ __device__ __forceinline__ int expOf(T v)
     return v == T(0) ? 0 : ilogb(v);
 }
 
-template<class T>
+template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid     = targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst);
+    bool valid     = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
     double divvOut = -INFINITY;
     if (valid)
     {
@@ -278,18 +278,149 @@ __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArra
         a.grec[t.i]   = GradRec<T>{c11i, c12i, c13i, c22i, c23i, c33i, divv, T(a.alpha[t.i])};
         divvOut       = double(divv);
     }
-    reduceOrdered<true>(divvOut, a.n, a.reduce + 0, a.batch, 0);
+    reduceOrdered<true, (kMode & kModeBatch) != 0>(divvOut, a.n, a.reduce + 0, a.batch, 0);
+}
+
+/*! FP32 IAD + divv/curlv in one pass over the list. The divv/curlv loop of the reference sums, per pair,
+ *  f_a tA_b with f = (v_j - v_i) xm_j and tA = -(C_i r) W, i.e. dV_ab = -sum_c C_bc M_ac with
+ *  M_ac = sum_j f_a r_c W: M is accumulated in the same pass as tau, and C_i, known only after the pass, is applied
+ *  to the nine sums at the end. Same quantities, one gather of each neighbour instead of two. */
+template<int kMode>
+__global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvFusedKernel(ChainArrays<float> a,
+                                                                              HydroConsts<float> k, DevBox box)
+{
+    using T = float;
+    Target t;
+    bool valid     = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
+    double divvOut = -INFINITY;
+    if (valid)
+    {
+        Pos<T> pi      = posOf(a, t.i);
+        double hiD     = a.h[t.i];
+        T hi           = T(hiD);
+        T hiInv        = T(1) / hi;
+        HydroRec<T> hr = a.hrec[t.i];
+
+        BlockSum<T> s11, s12, s13, s22, s23, s33;
+        BlockSum<T> mxx, mxy, mxz, myx, myy, myz, mzx, mzy, mzz;
+        for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
+        {
+            uint32_t js[kNbChunk];
+            loadChunk(a.nidx, t, t.ngPad, q0, js);
+            unsigned qn = min(kNbChunk, t.count - q0);
+#pragma unroll
+            for (unsigned q = 0; q < kNbChunk; ++q)
+            {
+                if (q >= qn) { break; }
+                uint32_t j     = js[q];
+                Pos<T> pj      = posOf(a, j);
+                HydroRec<T> hj = loadHydro(a.hrec + j);
+                Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+                T dist         = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
+                T w            = kernelW(a.wh, k, dist * hiInv);
+                T voljW        = hj.vol * w;
+                s11.add(r.rx * r.rx * voljW);
+                s12.add(r.rx * r.ry * voljW);
+                s13.add(r.rx * r.rz * voljW);
+                s22.add(r.ry * r.ry * voljW);
+                s23.add(r.ry * r.rz * voljW);
+                s33.add(r.rz * r.rz * voljW);
+                T xw = hj.xm * w;
+                T fx = (hj.vx - hr.vx) * xw;
+                T fy = (hj.vy - hr.vy) * xw;
+                T fz = (hj.vz - hr.vz) * xw;
+                mxx.add(fx * r.rx);
+                mxy.add(fx * r.ry);
+                mxz.add(fx * r.rz);
+                myx.add(fy * r.rx);
+                myy.add(fy * r.ry);
+                myz.add(fy * r.rz);
+                mzx.add(fz * r.rx);
+                mzy.add(fz * r.ry);
+                mzz.add(fz * r.rz);
+            }
+            s11.flush();
+            s12.flush();
+            s13.flush();
+            s22.flush();
+            s23.flush();
+            s33.flush();
+            mxx.flush();
+            mxy.flush();
+            mxz.flush();
+            myx.flush();
+            myy.flush();
+            myz.flush();
+            mzx.flush();
+            mzy.flush();
+            mzz.flush();
+        }
+        T tau11 = s11.get(), tau12 = s12.get(), tau13 = s13.get();
+        T tau22 = s22.get(), tau23 = s23.get(), tau33 = s33.get();
+        int expSum = expOf(tau11) + expOf(tau12) + expOf(tau13) + expOf(tau22) + expOf(tau23) + expOf(tau33);
+        T norm     = ldexp(T(1), -expSum / 6);
+        tau11 *= norm;
+        tau12 *= norm;
+        tau13 *= norm;
+        tau22 *= norm;
+        tau23 *= norm;
+        tau33 *= norm;
+        T det = tau11 * tau22 * tau33 + T(2) * tau12 * tau23 * tau13 - tau11 * tau23 * tau23 - tau22 * tau13 * tau13 -
+                tau33 * tau12 * tau12;
+        T factor = norm * (hi * hi * hi) / (det * k.K);
+        if (isnan(factor) && t.count == 0) { factor = T(0); }
+        T c11i = (tau22 * tau33 - tau23 * tau23) * factor;
+        T c12i = (tau13 * tau23 - tau33 * tau12) * factor;
+        T c13i = (tau12 * tau23 - tau22 * tau13) * factor;
+        T c22i = (tau11 * tau33 - tau13 * tau13) * factor;
+        T c23i = (tau13 * tau12 - tau11 * tau23) * factor;
+        T c33i = (tau11 * tau22 - tau12 * tau12) * factor;
+
+        // dV_ab = -sum_c C_bc M_ac
+        T M[3][3] = {{mxx.get(), mxy.get(), mxz.get()}, {myx.get(), myy.get(), myz.get()},
+                     {mzx.get(), mzy.get(), mzz.get()}};
+        T C[3][3] = {{c11i, c12i, c13i}, {c12i, c22i, c23i}, {c13i, c23i, c33i}};
+        T dV[3][3];
+#pragma unroll
+        for (int p = 0; p < 3; ++p)
+        {
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+            {
+                dV[p][q] = -(C[q][0] * M[p][0] + C[q][1] * M[p][1] + C[q][2] * M[p][2]);
+            }
+        }
+        T hiInv3 = hiInv * hiInv * hiInv;
+        T normKx = k.K * hiInv3 / a.kx[t.i];
+        T divv   = normKx * (dV[0][0] + dV[1][1] + dV[2][2]);
+        T cx     = dV[2][1] - dV[1][2];
+        T cy     = dV[0][2] - dV[2][0];
+        T cz     = dV[1][0] - dV[0][1];
+        T curlv  = normKx * sqrt(cx * cx + cy * cy + cz * cz);
+
+        a.cij[0][t.i] = c11i;
+        a.cij[1][t.i] = c12i;
+        a.cij[2][t.i] = c13i;
+        a.cij[3][t.i] = c22i;
+        a.cij[4][t.i] = c23i;
+        a.cij[5][t.i] = c33i;
+        a.divv[t.i]   = divv;
+        a.curlv[t.i]  = curlv;
+        a.grec[t.i]   = GradRec<T>{c11i, c12i, c13i, c22i, c23i, c33i, divv, T(a.alpha[t.i])};
+        divvOut       = double(divv);
+    }
+    reduceOrdered<true, (kMode & kModeBatch) != 0>(divvOut, a.n, a.reduce + 0, a.batch, 0);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
 // AV switches (sph/include/sph/hydro_ve/av_switches_kern.hpp:43-137)
 // ---------------------------------------------------------------------------------------------------------------
-template<class T>
+template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box,
                                                                   double dt)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst)) { return; }
+    if (!targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr)) { return; }
     Pos<T> pi      = posOf(a, t.i);
     double hiD     = a.h[t.i];
     HydroRec<T> hr = a.hrec[t.i];
@@ -322,24 +453,45 @@ __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays
             T rv           = r.rx * (hr.vx - hj.vx) + r.ry * (hr.vy - hj.vy) + r.rz * (hr.vz - hj.vz);
             T vsig         = T(0);
             if (rv < T(0)) { vsig = ci + hj.c - fdiv(T(3) * rv, dist); }
-            if (!(vijsignalI > vsig)) { vsigJ = int(j); }
+            if constexpr (kMode & kModeTape)
+            {
+                if (!(vijsignalI > vsig)) { vsigJ = int(j); }
+            }
             vijsignalI = vijsignalI > vsig ? vijsignalI : vsig;
             T Wi       = KhiInv3 * kernelW(a.wh, k, dist * hiInv);
-            T tA1      = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
-            T tA2      = -(gr.c12 * r.rx + gr.c22 * r.ry + gr.c23 * r.rz) * Wi;
-            T tA3      = -(gr.c13 * r.rx + gr.c23 * r.ry + gr.c33 * r.rz) * Wi;
             T fac      = hj.vol * (divvI - divvJ);
-            gx.add(fac * tA1);
-            gy.add(fac * tA2);
-            gz.add(fac * tA3);
+            if constexpr (sizeof(T) == 4)
+            {
+                // FP32: sum fac W r and apply -C_i once after the loop (the same vector, 9 FMAs less per pair)
+                T sw = fac * Wi;
+                gx.add(sw * r.rx);
+                gy.add(sw * r.ry);
+                gz.add(sw * r.rz);
+            }
+            else
+            {
+                T tA1 = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
+                T tA2 = -(gr.c12 * r.rx + gr.c22 * r.ry + gr.c23 * r.rz) * Wi;
+                T tA3 = -(gr.c13 * r.rx + gr.c23 * r.ry + gr.c33 * r.rz) * Wi;
+                gx.add(fac * tA1);
+                gy.add(fac * tA2);
+                gz.add(fac * tA3);
+            }
         }
         gx.flush();
         gy.flush();
         gz.flush();
     }
-    T gdx      = gx.get(), gdy = gy.get(), gdz = gz.get();
+    T gdx = gx.get(), gdy = gy.get(), gdz = gz.get();
+    if constexpr (sizeof(T) == 4)
+    {
+        T sx = gdx, sy = gdy, sz = gdz;
+        gdx  = -(gr.c11 * sx + gr.c12 * sy + gr.c13 * sz);
+        gdy  = -(gr.c12 * sx + gr.c22 * sy + gr.c23 * sz);
+        gdz  = -(gr.c13 * sx + gr.c23 * sy + gr.c33 * sz);
+    }
     T graddivv = sqrt(gdx * gdx + gdy * gdy + gdz * gdz);
-    if (a.tape.gx)
+    if constexpr (kMode & kModeTape)
     {
         a.tape.gx[t.i]    = gdx;
         a.tape.gy[t.i]    = gdy;
@@ -359,7 +511,8 @@ __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays
     {
         T decay    = hi / (k.decay * vijsignalI);
         T alphadot = alphaloc >= k.alphamin ? (alphaloc - alphaI) / decay : (k.alphamin - alphaI) / decay;
-        double dtq = a.batch.inst ? a.batch.dt[a.batch.inst[t.i]] : dt;
+        double dtq = dt;
+        if constexpr (kMode & kModeBatch) { dtq = a.batch.dt[a.batch.inst[t.i]]; }
         alphaI += alphadot * T(dtq);
     }
     a.alpha[t.i]      = double(alphaI);
@@ -371,11 +524,11 @@ __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays
 // artificial_viscosity sph/include/sph/kernels.hpp:71-85) with the Courant time step per particle
 // (tsKCourant, kernels.hpp:10-17) reduced to the minimum.
 // ---------------------------------------------------------------------------------------------------------------
-template<class T>
+template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid   = targetOf(a.n, a.nc, k.ngmax, t, a.batch.inst);
+    bool valid   = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
     double dtMin = INFINITY;
     if (valid)
     {
@@ -481,7 +634,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainAr
             energyS.flush();
             aViscE.flush();
         }
-        if (a.tape.energy)
+        if constexpr (kMode & kModeTape)
         {
             a.tape.energy[t.i] = energyS.get();
             a.tape.avisc[t.i]  = aViscE.get();
@@ -495,7 +648,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainAr
         double v = maxvsignalI > T(0) ? double(maxvsignalI) : double(ci);
         dtMin    = hiD > 0.0 ? k.Kcour * hiD / v : INFINITY;
     }
-    reduceOrdered<false>(dtMin, a.n, a.reduce + 1, a.batch, 1);
+    reduceOrdered<false, (kMode & kModeBatch) != 0>(dtMin, a.n, a.reduce + 1, a.batch, 1);
 }
 
 template<class T>
@@ -506,11 +659,28 @@ unsigned chainBlocks(const ChainArrays<T>& a)
 
 } // namespace
 
+//! kernel variant: kModeTape when the adjoint's tape pointers are set, kModeBatch for an ensemble
+template<class T>
+int chainMode(const ChainArrays<T>& a)
+{
+    int mode = (a.tape.energy ? kModeTape : 0) | (a.batch.inst ? kModeBatch : 0);
+    return mode == (kModeTape | kModeBatch) ? -1 : mode;
+}
+
+#define SPHB_DISPATCH(KERNEL, ...)                                                                                      \
+    switch (chainMode(a))                                                                                               \
+    {                                                                                                                   \
+    case 0: KERNEL<T, 0><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                                    \
+    case kModeTape: KERNEL<T, kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
+    case kModeBatch: KERNEL<T, kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                  \
+    default: return kErrArg;                                                                                            \
+    }
+
 template<class T>
 int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    xmassKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+    SPHB_DISPATCH(xmassKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -520,7 +690,7 @@ template<class T>
 int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    veDefGradhEosKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+    SPHB_DISPATCH(veDefGradhEosKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -530,7 +700,17 @@ template<class T>
 int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    iadDivvCurlvKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+    if constexpr (sizeof(T) == 4)
+    {
+        switch (chainMode(a))
+        {
+        case 0: iadDivvCurlvFusedKernel<0><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
+        case kModeTape: iadDivvCurlvFusedKernel<kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
+        case kModeBatch: iadDivvCurlvFusedKernel<kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
+        default: return kErrArg;
+        }
+    }
+    else { SPHB_DISPATCH(iadDivvCurlvKernel, a, k, box) }
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -540,7 +720,7 @@ template<class T>
 int launchAVswitches(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, double dt, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    avSwitchesKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box, dt);
+    SPHB_DISPATCH(avSwitchesKernel, a, k, box, dt)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -550,7 +730,7 @@ template<class T>
 int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    momentumEnergyKernel<T><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+    SPHB_DISPATCH(momentumEnergyKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

@@ -98,6 +98,14 @@ __device__ inline int findSlot(const int* pre, int n, int t)
     return lo;
 }
 
+//! 32-byte read-only load of a packed position (two 16-byte loads of one sector)
+__device__ inline double4 ldPos(const double4* p)
+{
+    const double2* q = reinterpret_cast<const double2*>(p);
+    double2 lo = __ldg(q), hi = __ldg(q + 1);
+    return make_double4(lo.x, lo.y, hi.x, hi.y);
+}
+
 //! d folded to the nearest periodic image: d - L * rint(d / L), rounded like the reference's uncontracted CPU code
 __device__ inline double minImage(double d, double len, double ilen, int periodic)
 {
@@ -112,9 +120,11 @@ __device__ inline double updateH(unsigned ng0, unsigned nc, double h)
     return __dmul_rn(__dmul_rn(h, 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
 }
 
+template<bool kBatched>
 __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const double* __restrict__ x,
                                                                   const double* __restrict__ y,
-                                                                  const double* __restrict__ z, double* h, size_t n,
+                                                                  const double* __restrict__ z,
+                                                                  const double4* __restrict__ pos, double* h, size_t n,
                                                                   TreeView tree, DevBox box, NeighborParams prm,
                                                                   uint32_t* __restrict__ nidx,
                                                                   unsigned* __restrict__ ncOut, unsigned* status,
@@ -131,8 +141,8 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
     const size_t i = group * kWarp + lane;
     // an ensemble: the group's instance (its first slot is never padding) selects the tree; padding slots idle
     TreeView tv = tree;
-    if (views) { tv = views[inst[group * kWarp]]; }
-    const bool valid = i < n && !(inst && inst[i] == kGhost);
+    if constexpr (kBatched) { tv = views[inst[group * kWarp]]; }
+    const bool valid = i < n && !(kBatched && inst[i] == kGhost);
     const double xi  = valid ? x[i] : 0.0;
     const double yi  = valid ? y[i] : 0.0;
     const double zi  = valid ? z[i] : 0.0;
@@ -205,8 +215,9 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         // test the staged 32 candidates against this lane's particle and append the neighbours in index order
         auto testStaged = [&]() {
             if (!active) { return; }
-            // bit k: candidate k may lie inside the sphere (FP32 distance below the upper edge of the band)
-            unsigned maybe = 0u;
+            // bit k of sure: candidate k lies inside the sphere by its FP32 distance (below the band); of maybe: it
+            // may (below the upper edge of the band)
+            unsigned maybe = 0u, sure = 0u;
             const float2 mx = make_float2(-rix, -rix), my = make_float2(-riy, -riy), mz = make_float2(-riz, -riz);
 #pragma unroll
             for (int k = 0; k < kWarp; k += 2)
@@ -219,35 +230,35 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 float2 dz = __fadd2_rn(Z, mz);
                 float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
                 maybe |= (unsigned(d2.x < r2hi) << k) | (unsigned(d2.y < r2hi) << (k + 1));
+                sure |= (unsigned(d2.x < r2lo) << k) | (unsigned(d2.y < r2lo) << (k + 1));
             }
-            while (maybe)
+            // candidates too close to the search radius for FP32: the exact test of the reference (rare)
+            unsigned band = maybe & ~sure;
+            while (band)
             {
-                int k = __ffs(maybe) - 1;
-                maybe &= maybe - 1u;
+                int k = __ffs(band) - 1;
+                band &= band - 1u;
+                int j = sh.cj[warp][k];
+                double4 pj = ldPos(pos + j);
+                double ex  = minImage(pj.x - xi, box.len[0], box.ilen[0], box.periodic[0]);
+                double ey  = minImage(pj.y - yi, box.len[1], box.ilen[1], box.periodic[1]);
+                double ez  = minImage(pj.z - zi, box.len[2], box.ilen[2], box.periodic[2]);
+                double d2  = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+                if (d2 < radiusSq) { sure |= 1u << k; }
+            }
+            // append the neighbours in candidate (= index) order
+            while (sure)
+            {
+                int k = __ffs(sure) - 1;
+                sure &= sure - 1u;
                 int j = sh.cj[warp][k];
                 if (size_t(j) == i) { continue; }
-                float dx = __fsub_rn(sh.cx[warp][k], rix);
-                float dy = __fsub_rn(sh.cy[warp][k], riy);
-                float dz = __fsub_rn(sh.cz[warp][k], riz);
-                bool in  = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx))) < r2lo;
-                if (!in)
+                if (count < prm.ngmax)
                 {
-                    // too close to the search radius for FP32: the exact test of the reference
-                    double ex = minImage(x[j] - xi, box.len[0], box.ilen[0], box.periodic[0]);
-                    double ey = minImage(y[j] - yi, box.len[1], box.ilen[1], box.periodic[1]);
-                    double ez = minImage(z[j] - zi, box.len[2], box.ilen[2], box.periodic[2]);
-                    double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-                    in        = d2 < radiusSq;
+                    chunk[count % kNbChunk] = uint32_t(j);
+                    if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
                 }
-                if (in)
-                {
-                    if (count < prm.ngmax)
-                    {
-                        chunk[count % kNbChunk] = uint32_t(j);
-                        if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
-                    }
-                    ++count;
-                }
+                ++count;
             }
         };
 
@@ -478,16 +489,24 @@ int computeBlockBoxes(const double* x, const double* y, const double* z, size_t 
     return kOk;
 }
 
-int findNeighbors(const double* x, const double* y, const double* z, double* h, size_t n, const TreeView& tree,
-                  const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc, unsigned* status,
-                  cudaStream_t stream, const TreeView* views, const uint8_t* inst)
+int findNeighbors(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
+                  const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
+                  unsigned* status, cudaStream_t stream, const TreeView* views, const uint8_t* inst)
 {
     if (n == 0) { return kOk; }
     if ((views == nullptr) != (inst == nullptr)) { return kErrArg; }
     size_t numGroups = (n + kWarp - 1) / kWarp;
     unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
-    findNeighborsKernel<<<blocks, kNbThreads, 0, stream>>>(x, y, z, h, n, tree, box, prm, nidx, nc, status, views,
-                                                           inst);
+    if (views)
+    {
+        findNeighborsKernel<true><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm, nidx, nc, status,
+                                                                     views, inst);
+    }
+    else
+    {
+        findNeighborsKernel<false><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm, nidx, nc, status,
+                                                                      nullptr, nullptr);
+    }
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

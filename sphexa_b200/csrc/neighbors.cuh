@@ -48,12 +48,13 @@ struct NeighborParams
     int maxIterations; // smoothing-length updates (10 in the reference, sph/include/sph/find_neighbors.hpp:19)
 };
 
-/*! Search all particles: updates h where the count left [ng0/4, ngmax+1], writes nc (count incl. self) and lists.
+/*! Search all particles (x, y, z and the same coordinates packed as pos = (x, y, z, m)): updates h where the count left [ng0/4, ngmax+1], writes nc (count incl. self) and lists.
  *  status[0] is set to a non-zero value if a per-warp buffer overflowed (the search then returns SPHB_ERR_CAPACITY).
  *  An ensemble passes views (one tree per instance, on the device) and inst (instance per slot, kGhost for
  *  padding): each group searches its instance's tree, padding slots are skipped. */
-int findNeighbors(const double* x, const double* y, const double* z, double* h, size_t n, const TreeView& tree,
-                  const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc, unsigned* status,
-                  cudaStream_t stream, const TreeView* views = nullptr, const uint8_t* inst = nullptr);
+int findNeighbors(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
+                  const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
+                  unsigned* status, cudaStream_t stream, const TreeView* views = nullptr,
+                  const uint8_t* inst = nullptr);
 
 } // namespace sphb

@@ -408,8 +408,8 @@ int computeForces(sphb_sim& s)
     tv.blockHi      = s.blockHi.data();
     tv.numNodes     = s.ftree.tree.numNodes;
     NeighborParams np{s.p.ng0, s.p.ngmax, 10};
-    SPHB_TRY(findNeighbors(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fH].data(), s.n, tv, s.box, np,
-                           s.nidx.data(), s.nc.data(), s.status.data(), st));
+    SPHB_TRY(findNeighbors(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
+                           s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
 
     if (s.mixed) { SPHB_TRY(runChain<float>(s)); }
