@@ -264,6 +264,20 @@ EVAL_FIELDS = ("nc", "m", "kx", "xm", "c", "prho", "gradh", "du", "ax", "ay", "a
 SNAP_FIELDS = ("id", "x", "y", "z", "h", "m", "temp", "vx", "vy", "vz", "kx", "xm", "ax", "ay", "az")
 
 
+def replica_throughput(ms_local: float, n_local: int, steps: int, dist=None, device="cpu"):
+    """Whole-job figures of independent replicas: the slowest rank's time (the job ends when it does) and the
+    particle-steps of all ranks over it. One MAX and one SUM all-reduce; no other traffic between ranks."""
+    import torch
+    if dist is None:
+        return ms_local, n_local * steps / (ms_local * 1e-3)
+    t = torch.tensor([ms_local], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(n_local)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    ms = float(t.item())
+    return ms, float(c.item()) * steps / (ms * 1e-3)
+
+
 def run_ours(args, ws, rank, local):
     import torch
 
@@ -320,12 +334,12 @@ def run_ours(args, ws, rank, local):
         barrier_sync()
         clk = clocks.stop() if with_clocks else None
         launches = sim.kernel_launches() - launches0
-        ms = e0.elapsed_time(e1)
-        ms = max_over_ranks(ms)
+        ms_local = e0.elapsed_time(e1)
+        ms = max_over_ranks(ms_local)
         nc = sim.get("nc").astype(np.int64)
         pairs = int(np.minimum(nc - 1, int(ic["params"]["ngmax"])).sum())
         snap = {f: sim.get(f) for f in SNAP_FIELDS}
-        res = {"ms_total": ms, "stage_ms": {k: v / steps for k, v in stage_sum.items()}, "launches": launches,
+        res = {"ms_total": ms, "ms_local": ms_local, "stage_ms": {k: v / steps for k, v in stage_sum.items()}, "launches": launches,
                "pairs": pairs, "clocks": clk, "snap": snap, "energy": energy, "ttot": sim.scalars()["ttot"]}
         if with_e2e:
             # per step: host->device copy of the whole particle state from pinned memory, the step, and the
@@ -380,8 +394,8 @@ def run_ours(args, ws, rank, local):
         roofline["traffic"] = roofline["traffic"] * n
 
     steps = args.steps
-    ms_step = main_leg["ms_total"] / steps
-    value = n * ws * steps / (main_leg["ms_total"] * 1e-3)
+    ms_job, value = replica_throughput(main_leg["ms_local"], n, steps, dist, "cuda")
+    ms_step = ms_job / steps
     energy = main_leg["energy"]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": steps, "warmup": args.warmup,
