@@ -61,6 +61,8 @@ typedef struct
     double minDt_m1;        /* previous time step                                          */
     int precision;          /* SPHB_FP64 or SPHB_MIXED                                     */
     uint32_t bucket_focus;  /* max particles per leaf of the neighbour-search tree (64)    */
+    int av_clean;           /* 1: AV cleaning in MomentumEnergy (HydroVeProp<avClean = true>,
+                               momentum_energy_kern.hpp:43-63,165-169); 0 (default): off   */
 } sphb_params;
 
 /*! Fill p with the reference defaults listed above (precision = SPHB_FP64). */
@@ -215,7 +217,8 @@ int sphb_sim_set_params(sphb_sim* sim, const sphb_params* params);
  *  the step (indexed like the state the step starts from); *alphamax_bar (host) is incremented by the derivative
  *  with respect to alphamax. The adjoint of m is passed through unchanged. Precision follows the simulation: FP64
  *  adjoint for SPHB_FP64, FP32 J-loop adjoints for SPHB_MIXED. Afterwards the simulation holds the recomputed
- *  post-force state, not the state after the step. No counterpart in the reference. */
+ *  post-force state, not the state after the step. Not available with AV cleaning (SPHB_ERR_STATE).
+ *  No counterpart in the reference. */
 int sphb_sim_step_vjp(sphb_sim* sim, const double* const* adj_post, double* const* adj_pre, double* alphamax_bar);
 
 /* ---------------------------------------------------------------------------------------------------------------- */

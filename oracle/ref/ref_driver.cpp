@@ -51,6 +51,7 @@ struct RefSim
     cstone::Box<double> box{0, 1};
     double timeSync{0}, timeNeighbors{0}, timeChain{0}, timeIntegrate{0};
     bool synced{false};
+    bool avClean{false};
 };
 
 namespace
@@ -163,6 +164,19 @@ extern "C"
 
     void ref_sim_destroy(void* p) { delete static_cast<RefSim*>(p); }
 
+    //! @brief HydroVeProp<avClean = true> (ve_hydro.hpp:48-90,175-185): the symmetric velocity gradients are kept
+    //! (iad_divv_curlv.hpp:62-69 computes them when the fields exist) and MomentumEnergy applies the AV cleaning
+    void ref_sim_set_av_clean(void* p, int on)
+    {
+        auto& s   = *static_cast<RefSim*>(p);
+        s.avClean = on != 0;
+        if (s.avClean)
+        {
+            s.d.setDependent("dV11", "dV12", "dV13", "dV22", "dV23", "dV33");
+            s.d.resize(s.d.x.size());
+        }
+    }
+
     //! @brief the sync that the main program performs once before the first step (sphexa.cpp:141)
     int ref_sim_initial_sync(void* p)
     {
@@ -208,7 +222,8 @@ extern "C"
             computeIadDivvCurlv(grp, d, s.box);
             d.minDtRho = rhoTimestep(first, last, d);
             computeAVswitches(grp, d, s.box);
-            computeMomentumEnergy<false>(grp, nullptr, d, s.box);
+            if (s.avClean) { computeMomentumEnergy<true>(grp, nullptr, d, s.box); }
+            else { computeMomentumEnergy<false>(grp, nullptr, d, s.box); }
             s.timeChain += since(t0);
 
             sphexa::computeConservedQuantities(first, last, d, MPI_COMM_WORLD);

@@ -36,6 +36,7 @@ def load(mixed: bool = False):
         getattr(lib, name).argtypes = [P]
         getattr(lib, name).restype = C.c_int
     lib.ref_sim_destroy.argtypes = [P]
+    lib.ref_sim_set_av_clean.argtypes = [P, C.c_int]
     lib.ref_sim_get.argtypes = [P, C.c_char_p, P]
     lib.ref_sim_set.argtypes = [P, C.c_char_p, P]
     lib.ref_sim_keys.argtypes = [P, P]
@@ -73,6 +74,7 @@ class RefSim:
     """One simulation of the reference CPU hydro step (1 rank, OpenMP)."""
 
     def __init__(self, ic: dict, mixed: bool = False):
+        """ic["params"].get("avClean") selects HydroVeProp<avClean = true>."""
         from sphexa_b200.ic import CONSERVED_FIELDS
         self.lib = load(mixed)
         p = ic["params"]
@@ -86,6 +88,8 @@ class RefSim:
         self.n0 = self._id.size
         self.h = self.lib.ref_sim_create(self.n0, arr, ptr(self._id), ptr(self._box), int(bool(ic["periodic"])),
                                          ptr(prm))
+        if p.get("avClean"):
+            self.lib.ref_sim_set_av_clean(self.h, 1)
         rc = self.lib.ref_sim_initial_sync(self.h)
         if rc:
             raise RuntimeError("reference initial sync failed")

@@ -13,8 +13,9 @@ namespace chain
 constexpr int kChainThreads = 128;
 
 //! compile-time variants of the J-loop kernels: write the adjoint's tape, or run over a batched ensemble
-constexpr int kModeTape  = 1;
-constexpr int kModeBatch = 2;
+constexpr int kModeTape    = 1;
+constexpr int kModeBatch   = 2;
+constexpr int kModeAvClean = 4;
 
 /*! Neighbour-sum accumulator. FP64: every term is added as it comes, in list order (the reference's order).
  *  FP32: terms are summed plainly within one list chunk of 8 neighbours and each chunk sum is added to a
@@ -256,6 +257,46 @@ __device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned 
     t.count = min(nc[t.i] - 1u, ngmax);
     t.ngPad = paddedNgmax(ngmax);
     return true;
+}
+
+template<class T>
+__device__ __forceinline__ void loadDV(const DVRec<T>* p, T (&g)[6])
+{
+    if constexpr (sizeof(T) == 8)
+    {
+        const double2* q = reinterpret_cast<const double2*>(p);
+        double2 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+        g[0] = a.x, g[1] = a.y, g[2] = b.x, g[3] = b.y, g[4] = c.x, g[5] = c.y;
+    }
+    else
+    {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        float4 a = __ldg(q);
+        float2 b = __ldg(reinterpret_cast<const float2*>(q + 1));
+        g[0] = a.x, g[1] = a.y, g[2] = a.z, g[3] = a.w, g[4] = b.x, g[5] = b.y;
+    }
+}
+
+/*! Additive AV-cleaning correction of rv = r . v_ij (momentum_energy_kern.hpp:43-63): the quadratic forms of both
+ *  particles' symmetrised velocity gradients along r, damped by how far min(v_i, v_j) falls below eta_crit. */
+template<class T>
+__device__ __forceinline__ T avRvCorrection(T rx, T ry, T rz, T etaAb, T etaCrit, const T (&gi)[6], const T (&gj)[6])
+{
+    T dmy1 = rx * (gi[0] * rx + gi[1] * ry + gi[2] * rz) + ry * (gi[3] * ry + gi[4] * rz) + rz * (gi[5] * rz);
+    T dmy2 = rx * (gj[0] * rx + gj[1] * ry + gj[2] * rz) + ry * (gj[3] * ry + gj[4] * rz) + rz * (gj[5] * rz);
+    T dmy3 = T(1);
+    if (etaAb < etaCrit)
+    {
+        T etaDiff = T(5) * (etaAb - etaCrit);
+        dmy3      = exp(-etaDiff * etaDiff);
+    }
+    T aAb   = (dmy2 != T(0)) ? dmy1 / dmy2 : T(0);
+    T aAbp1 = T(1) + aAb;
+    T q     = T(4) * aAb / (aAbp1 * aAbp1);
+    q       = q < T(1) ? q : T(1);
+    q       = q > T(0) ? q : T(0);
+    T phiAb = T(0.5) * dmy3 * q;
+    return -phiAb * (dmy1 + dmy2);
 }
 
 //! the 8 neighbour indices of list chunk q0 / 8 of the target (two 16-byte loads of one sector)

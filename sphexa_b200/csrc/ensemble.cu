@@ -90,6 +90,7 @@ struct sphb_ensemble
     DeviceBuffer<char> derived[kNumDerived];
     DeviceBuffer<double> du;
     DeviceBuffer<char> hrec, grec;
+    DeviceBuffer<char> dvrec, dv; // AV cleaning only
     DeviceBuffer<double> whD, whdD;
     DeviceBuffer<float> whF, whdF;
     double K{0};
@@ -267,6 +268,11 @@ int allocate(sphb_ensemble& e)
     SPHB_TRY(e.du.reserve(n));
     SPHB_TRY(e.hrec.reserve(n * 8 * e.elemBytes()));
     SPHB_TRY(e.grec.reserve(n * 8 * e.elemBytes()));
+    if (e.p.av_clean)
+    {
+        SPHB_TRY(e.dvrec.reserve(n * 8 * e.elemBytes()));
+        SPHB_TRY(e.dv.reserve(n * 6 * e.elemBytes()));
+    }
     SPHB_TRY(e.alphaBackup.reserve(n));
     SPHB_TRY(e.hBackup.reserve(n));
     int m = e.num;
@@ -489,6 +495,14 @@ ChainArrays<T> chainOf(sphb_ensemble& e)
     a.batch.dt     = e.dt.data();
     a.batch.dtm1   = e.dtm1.data();
     a.batch.reduce = e.reduce.data();
+    if (e.p.av_clean)
+    {
+        a.dvrec = reinterpret_cast<DVRec<T>*>(e.dvrec.data());
+        for (int q = 0; q < 6; ++q)
+        {
+            a.dv[q] = reinterpret_cast<T*>(e.dv.data()) + size_t(q) * e.slots;
+        }
+    }
     return a;
 }
 
@@ -711,7 +725,7 @@ extern "C" int sphb_ensemble_create(sphb_ensemble** out, int num, const size_t* 
         if (sizes[k] == 0 || q.ng0 != p0.ng0 || q.ngmax != p0.ngmax || q.precision != p0.precision ||
             q.sinc_index != p0.sinc_index || q.bucket_focus != p0.bucket_focus || q.alphamin != p0.alphamin ||
             q.alphamax != p0.alphamax || q.decay_constant != p0.decay_constant || q.Kcour != p0.Kcour ||
-            q.Krho != p0.Krho || !(q.gamma > 1.0))
+            q.Krho != p0.Krho || q.av_clean != p0.av_clean || !(q.gamma > 1.0))
         {
             return SPHB_ERR_ARG;
         }

@@ -50,6 +50,16 @@ struct alignas(8 * sizeof(T)) GradRec
     T c11, c12, c13, c22, c23, c33, divv, alpha;
 };
 
+/*! AV cleaning only: the symmetrised velocity gradient of a particle (dV11, dV12 = dVxy + dVyx, dV13, dV22, dV23,
+ *  dV33, each times K / (h^3 kx); divv_curlv_kern.hpp:114-122), written by IAD, read per neighbour by
+ *  MomentumEnergy. */
+template<class T>
+struct alignas(8 * sizeof(T)) DVRec
+{
+    T dv[6];
+    T pad0, pad1;
+};
+
 /*! Intermediate values the adjoint of the chain needs and the outputs do not determine; written only when the
  *  pointers are set (a step recomputed for its adjoint). whomega, wrho0: the two kernel-derivative sums of VeDefGradh
  *  after normalisation; gx, gy, gz, vsig, vsigJ: the divv gradient, the signal velocity of the AV switches and the
@@ -103,6 +113,8 @@ struct ChainArrays
     unsigned long long* reduce;
     ChainTape<T> tape;
     BatchView batch;
+    DVRec<T>* dvrec{nullptr}; // set: AV cleaning (HydroVeProp<avClean = true>)
+    T* dv[6]{};              // the same six fields as arrays (dV11 .. dV33)
     int threads{128}; // block size of the J-loop launches
 };
 

@@ -266,6 +266,19 @@ __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArra
         T cy     = dVxz.get() - dVzx.get();
         T cz     = dVyx.get() - dVxy.get();
         T curlv  = normKx * sqrt(cx * cx + cy * cy + cz * cz);
+        if constexpr (kMode & kModeAvClean)
+        {
+            DVRec<T> g{{normKx * dVxx.get(), normKx * (dVxy.get() + dVyx.get()), normKx * (dVxz.get() + dVzx.get()),
+                        normKx * dVyy.get(), normKx * (dVyz.get() + dVzy.get()), normKx * dVzz.get()},
+                       T(0),
+                       T(0)};
+            a.dvrec[t.i] = g;
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+            {
+                a.dv[q][t.i] = g.dv[q];
+            }
+        }
 
         a.cij[0][t.i] = c11i;
         a.cij[1][t.i] = c12i;
@@ -397,6 +410,19 @@ __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvFusedKernel(Chai
         T cy     = dV[0][2] - dV[2][0];
         T cz     = dV[1][0] - dV[0][1];
         T curlv  = normKx * sqrt(cx * cx + cy * cy + cz * cz);
+        if constexpr (kMode & kModeAvClean)
+        {
+            DVRec<T> g{{normKx * dV[0][0], normKx * (dV[0][1] + dV[1][0]), normKx * (dV[0][2] + dV[2][0]),
+                        normKx * dV[1][1], normKx * (dV[1][2] + dV[2][1]), normKx * dV[2][2]},
+                       T(0),
+                       T(0)};
+            a.dvrec[t.i] = g;
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+            {
+                a.dv[q][t.i] = g.dv[q];
+            }
+        }
 
         a.cij[0][t.i] = c11i;
         a.cij[1][t.i] = c12i;
@@ -548,6 +574,13 @@ __global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainAr
         T hiInv3      = hiInv * hiInv * hiInv;
         T maxvsignalI = T(0);
         BlockSum<T> momX, momY, momZ, energyS, aViscE;
+        [[maybe_unused]] T gradVi[6];
+        [[maybe_unused]] T etaCrit = T(0);
+        if constexpr (kMode & kModeAvClean)
+        {
+            loadDV(a.dvrec + t.i, gradVi);
+            etaCrit = T(cbrt(32.0 * M_PI / 3.0 / double(t.count + 1)));
+        }
 
         for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
         {
@@ -586,6 +619,12 @@ __global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainAr
                 T rhoj   = fdiv(mj, hj.vol);
 
                 T rv   = r.rx * vxij + r.ry * vyij + r.rz * vzij;
+                if constexpr (kMode & kModeAvClean)
+                {
+                    T gradVj[6];
+                    loadDV(a.dvrec + j, gradVj);
+                    rv += avRvCorrection(r.rx, r.ry, r.rz, v1 < v2 ? v1 : v2, etaCrit, gradVi, gradVj);
+                }
                 T wij  = fdiv(rv, dist);
                 T visc = T(0);
                 if (wij < T(0))
@@ -667,6 +706,28 @@ int chainMode(const ChainArrays<T>& a)
     return mode == (kModeTape | kModeBatch) ? -1 : mode;
 }
 
+//! the mode of the two kernels that AV cleaning changes (IAD writes the gradients, MomentumEnergy reads them)
+template<class T>
+int chainModeAv(const ChainArrays<T>& a)
+{
+    int mode = chainMode(a);
+    if (mode < 0 || !a.dvrec) { return mode; }
+    return (mode & kModeTape) ? -1 : (mode | kModeAvClean); // the adjoint has no AV-cleaning variant
+}
+
+#define SPHB_DISPATCH_AV(KERNEL, ...)                                                                                   \
+    switch (chainModeAv(a))                                                                                             \
+    {                                                                                                                   \
+    case 0: KERNEL<T, 0><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                                    \
+    case kModeTape: KERNEL<T, kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
+    case kModeBatch: KERNEL<T, kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                  \
+    case kModeAvClean: KERNEL<T, kModeAvClean><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;              \
+    case kModeAvClean | kModeBatch:                                                                                     \
+        KERNEL<T, kModeAvClean | kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__);                         \
+        break;                                                                                                          \
+    default: return kErrArg;                                                                                            \
+    }
+
 #define SPHB_DISPATCH(KERNEL, ...)                                                                                      \
     switch (chainMode(a))                                                                                               \
     {                                                                                                                   \
@@ -702,15 +763,21 @@ int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const D
     if (a.n == 0) { return kOk; }
     if constexpr (sizeof(T) == 4)
     {
-        switch (chainMode(a))
+        switch (chainModeAv(a))
         {
         case 0: iadDivvCurlvFusedKernel<0><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
         case kModeTape: iadDivvCurlvFusedKernel<kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
         case kModeBatch: iadDivvCurlvFusedKernel<kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
+        case kModeAvClean:
+            iadDivvCurlvFusedKernel<kModeAvClean><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+            break;
+        case kModeAvClean | kModeBatch:
+            iadDivvCurlvFusedKernel<kModeAvClean | kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+            break;
         default: return kErrArg;
         }
     }
-    else { SPHB_DISPATCH(iadDivvCurlvKernel, a, k, box) }
+    else { SPHB_DISPATCH_AV(iadDivvCurlvKernel, a, k, box) }
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -730,7 +797,7 @@ template<class T>
 int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0) { return kOk; }
-    SPHB_DISPATCH(momentumEnergyKernel, a, k, box)
+    SPHB_DISPATCH_AV(momentumEnergyKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

@@ -65,6 +65,7 @@ struct sphb_sim
     DeviceBuffer<char> derived[kNumDerived];
     DeviceBuffer<double> du;
     DeviceBuffer<char> hrec, grec;
+    DeviceBuffer<char> dvrec, dv; // AV cleaning only: symmetrised velocity gradients (record + 6 arrays)
     DeviceBuffer<double> whD, whdD;
     DeviceBuffer<float> whF, whdF;
     DeviceBuffer<unsigned long long> reduce;
@@ -141,6 +142,11 @@ int allocateSim(sphb_sim& s)
     SPHB_TRY(s.du.reserve(n));
     SPHB_TRY(s.hrec.reserve(n * 8 * s.elemBytes()));
     SPHB_TRY(s.grec.reserve(n * 8 * s.elemBytes()));
+    if (s.p.av_clean)
+    {
+        SPHB_TRY(s.dvrec.reserve(n * 8 * s.elemBytes()));
+        SPHB_TRY(s.dv.reserve(n * 6 * s.elemBytes()));
+    }
     SPHB_TRY(s.reduce.reserve(4));
     SPHB_TRY(s.status.reserve(4));
     SPHB_TRY(s.partial.reserve(9 * 1024));
@@ -309,6 +315,14 @@ ChainArrays<T> chainArrays(sphb_sim& s)
     a.hrec   = reinterpret_cast<HydroRec<T>*>(s.hrec.data());
     a.grec   = reinterpret_cast<GradRec<T>*>(s.grec.data());
     a.reduce = s.reduce.data();
+    if (s.p.av_clean)
+    {
+        a.dvrec = reinterpret_cast<DVRec<T>*>(s.dvrec.data());
+        for (int q = 0; q < 6; ++q)
+        {
+            a.dv[q] = reinterpret_cast<T*>(s.dv.data()) + size_t(q) * s.n;
+        }
+    }
     if (s.taping)
     {
         T* t          = reinterpret_cast<T*>(s.tapeT.data());
@@ -579,6 +593,7 @@ extern "C" void sphb_default_params(sphb_params* p)
     p->minDt_m1       = 1e-12;
     p->precision      = SPHB_FP64;
     p->bucket_focus   = 64;
+    p->av_clean       = 0;
 }
 
 extern "C" const char* sphb_version(void) { return "sphb200 0.1 (sm_100a)"; }
@@ -710,6 +725,16 @@ bool findField(sphb_sim* s, const char* name, void** ptr, int* kind)
         *ptr  = s->du.data();
         *kind = 0;
         return true;
+    }
+    static const char* const dvNames[6] = {"dV11", "dV12", "dV13", "dV22", "dV23", "dV33"};
+    for (int q = 0; q < 6 && s->p.av_clean; ++q)
+    {
+        if (std::strcmp(name, dvNames[q]) == 0)
+        {
+            *ptr  = s->dv.data() + size_t(q) * s->n * s->elemBytes();
+            *kind = 1;
+            return true;
+        }
     }
     if (std::strcmp(name, "nc") == 0)
     {
@@ -907,7 +932,8 @@ extern "C" int sphb_sim_set_params(sphb_sim* s, const sphb_params* p)
 {
     if (!s || !p) { return SPHB_ERR_ARG; }
     if (p->ng0 != s->p.ng0 || p->ngmax != s->p.ngmax || p->precision != s->p.precision ||
-        p->sinc_index != s->p.sinc_index || p->bucket_focus != s->p.bucket_focus || !(p->gamma > 1.0))
+        p->sinc_index != s->p.sinc_index || p->bucket_focus != s->p.bucket_focus || p->av_clean != s->p.av_clean ||
+        !(p->gamma > 1.0))
     {
         return SPHB_ERR_ARG;
     }
@@ -926,7 +952,7 @@ extern "C" int sphb_sim_step_vjp(sphb_sim* s, const double* const* adj_post, dou
     {
         if (!adj_post[f] || !adj_pre[f] || adj_post[f] == adj_pre[f]) { return SPHB_ERR_ARG; }
     }
-    if (!s->uploaded || !(s->fixedDt > 0)) { return SPHB_ERR_STATE; }
+    if (!s->uploaded || !(s->fixedDt > 0) || s->p.av_clean) { return SPHB_ERR_STATE; }
     if (!s->hPre.data()) { SPHB_TRY(allocateAdjoint(*s)); }
     // the chain arrays of the recomputed step and of its adjoint both carry the tape pointers
     s->taping = true;

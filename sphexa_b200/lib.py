@@ -34,7 +34,8 @@ class Params(C.Structure):
     _fields_ = [("ng0", C.c_uint32), ("ngmax", C.c_uint32), ("gamma", C.c_double), ("mui", C.c_double),
                 ("Kcour", C.c_double), ("Krho", C.c_double), ("alphamin", C.c_double), ("alphamax", C.c_double),
                 ("decay_constant", C.c_double), ("sinc_index", C.c_double), ("minDt", C.c_double),
-                ("minDt_m1", C.c_double), ("precision", C.c_int), ("bucket_focus", C.c_uint32)]
+                ("minDt_m1", C.c_double), ("precision", C.c_int), ("bucket_focus", C.c_uint32),
+                ("av_clean", C.c_int)]
 
 
 #: every extern "C" symbol of include/sphb200.h
@@ -153,4 +154,5 @@ def make_params(p: dict, precision: int = SPHB_FP64, bucket: int = 64) -> Params
     prm.minDt_m1 = float(p["minDt_m1"])
     prm.precision = int(precision)
     prm.bucket_focus = int(bucket)
+    prm.av_clean = int(bool(p.get("avClean", False)))
     return prm

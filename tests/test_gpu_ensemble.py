@@ -16,11 +16,14 @@ def _ics():
             icm.sedov(14, seed=5, energy=1.6, gamma=5.0 / 3.0)]
 
 
-@pytest.mark.parametrize("precision,graph", [("mixed", True), ("fp64", False)])
-def test_ensemble_matches_single_simulations(cuda_device, precision, graph):
+@pytest.mark.parametrize("precision,graph,av_clean", [("mixed", True, False), ("fp64", False, False),
+                                                     ("mixed", True, True)])
+def test_ensemble_matches_single_simulations(cuda_device, precision, graph, av_clean):
     from sphexa_b200.ensemble import Ensemble
     from sphexa_b200.simulation import Simulation
     ics = _ics()
+    for ic in ics:
+        ic["params"] = dict(ic["params"], avClean=av_clean)
     steps = 4
     ens = Ensemble(ics, precision)
     assert ens.step(steps, graph=graph) == 0

@@ -220,3 +220,48 @@ def test_noh_mixed_vs_fp64(lib):
     rho_b = b.get("kx") * b.get("m") / b.get("xm")
     assert _max_rel(rho_b, rho_a) < 1e-5
     assert _max_rel(b.get("temp"), a.get("temp")) < 1e-5
+
+
+def test_sedov_av_clean_vs_reference(lib, ref):
+    """AV cleaning (HydroVeProp<avClean = true>): the symmetrised velocity gradients of IAD and the corrected
+    MomentumEnergy against the reference's own step, FP64, over three steps."""
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(20)
+    ic["params"] = dict(ic["params"], avClean=True)
+    r = ref.RefSim(ic)
+    g = Simulation(ic, "fp64")
+    for step in range(3):
+        r.compute_forces()
+        g.compute_forces()
+        assert np.array_equal(g.get("nc"), r.get("nc")), step
+        for f in ("dV11", "dV12", "dV13", "dV22", "dV23", "dV33", "ax", "ay", "az", "du"):
+            a, b = g.get(f), r.get(f)
+            scale = np.max(np.abs(b))
+            assert _max_rel(a, b, floor=1e-6 * scale) < 1e-8, (step, f)
+        r.integrate()
+        g.integrate()
+    for f in ("x", "vx", "temp"):
+        scale = 1e-3 if f != "vx" else np.max(np.abs(r.get(f)))
+        assert _max_rel(g.get(f), r.get(f), floor=scale) < 1e-9, f
+    # the correction changes the forces where the viscosity acts
+    plain = Simulation(icm.sedov(20), "fp64")
+    for _ in range(3):
+        plain.step()
+    assert not np.array_equal(plain.get("vx"), g.get("vx"))
+
+
+def test_av_clean_mixed_vs_fp64(lib):
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(24)
+    ic["params"] = dict(ic["params"], avClean=True)
+    a = Simulation(ic, "fp64")
+    b = Simulation(ic, "mixed")
+    a.compute_forces()
+    b.compute_forces()
+    for f in ("dV11", "dV22", "dV33"):
+        scale = np.max(np.abs(a.get(f)))
+        assert _max_rel(b.get(f), a.get(f), floor=1e-3 * scale) < 1e-4, f
+    scale = np.max(np.abs(a.get("du")))
+    assert _max_rel(b.get("du"), a.get("du"), floor=1e-3 * scale) < 1e-4
