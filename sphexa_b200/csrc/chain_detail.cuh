@@ -260,6 +260,26 @@ __device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned 
 }
 
 template<class T>
+__device__ __forceinline__ AVRec<T> loadAV(const AVRec<T>* p)
+{
+    AVRec<T> r;
+    if constexpr (sizeof(T) == 8)
+    {
+        const double4* q = reinterpret_cast<const double4*>(p);
+        double4 a = ldg4(q), b = ldg4(q + 1);
+        r = {a.x, a.y, a.z, a.w, b.x, b.y, T(0), T(0)};
+    }
+    else
+    {
+        const float4* q = reinterpret_cast<const float4*>(p);
+        float4 a = __ldg(q);
+        float2 b = __ldg(reinterpret_cast<const float2*>(q + 1));
+        r = {a.x, a.y, a.z, a.w, b.x, b.y, 0.f, 0.f};
+    }
+    return r;
+}
+
+template<class T>
 __device__ __forceinline__ void loadDV(const DVRec<T>* p, T (&g)[6])
 {
     if constexpr (sizeof(T) == 8)

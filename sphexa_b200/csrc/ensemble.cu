@@ -89,7 +89,7 @@ struct sphb_ensemble
     DeviceBuffer<unsigned> nc;
     DeviceBuffer<char> derived[kNumDerived];
     DeviceBuffer<double> du;
-    DeviceBuffer<char> hrec, grec;
+    DeviceBuffer<char> hrec, grec, avrec;
     DeviceBuffer<char> dvrec, dv; // AV cleaning only
     DeviceBuffer<double> whD, whdD;
     DeviceBuffer<float> whF, whdF;
@@ -268,6 +268,7 @@ int allocate(sphb_ensemble& e)
     SPHB_TRY(e.du.reserve(n));
     SPHB_TRY(e.hrec.reserve(n * 8 * e.elemBytes()));
     SPHB_TRY(e.grec.reserve(n * 8 * e.elemBytes()));
+    SPHB_TRY(e.avrec.reserve(n * 8 * e.elemBytes()));
     if (e.p.av_clean)
     {
         SPHB_TRY(e.dvrec.reserve(n * 8 * e.elemBytes()));
@@ -495,6 +496,7 @@ ChainArrays<T> chainOf(sphb_ensemble& e)
     a.batch.dt     = e.dt.data();
     a.batch.dtm1   = e.dtm1.data();
     a.batch.reduce = e.reduce.data();
+    a.avrec        = reinterpret_cast<AVRec<T>*>(e.avrec.data());
     if (e.p.av_clean)
     {
         a.dvrec = reinterpret_cast<DVRec<T>*>(e.dvrec.data());

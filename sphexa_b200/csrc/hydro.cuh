@@ -50,6 +50,15 @@ struct alignas(8 * sizeof(T)) GradRec
     T c11, c12, c13, c22, c23, c33, divv, alpha;
 };
 
+/*! Neighbour-side record of the AV switches, written by IAD: velocity, sound speed, xm/kx and divv (one 32-byte
+ *  gather per neighbour instead of three records). */
+template<class T>
+struct alignas(8 * sizeof(T)) AVRec
+{
+    T vx, vy, vz, c, vol, divv;
+    T pad0, pad1;
+};
+
 /*! AV cleaning only: the symmetrised velocity gradient of a particle (dV11, dV12 = dVxy + dVyx, dV13, dV22, dV23,
  *  dV33, each times K / (h^3 kx); divv_curlv_kern.hpp:114-122), written by IAD, read per neighbour by
  *  MomentumEnergy. */
@@ -113,6 +122,7 @@ struct ChainArrays
     unsigned long long* reduce;
     ChainTape<T> tape;
     BatchView batch;
+    AVRec<T>* avrec{nullptr};
     DVRec<T>* dvrec{nullptr}; // set: AV cleaning (HydroVeProp<avClean = true>)
     T* dv[6]{};              // the same six fields as arrays (dV11 .. dV33)
     int threads{128}; // block size of the J-loop launches

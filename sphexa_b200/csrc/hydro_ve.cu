@@ -289,6 +289,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArra
         a.divv[t.i]   = divv;
         a.curlv[t.i]  = curlv;
         a.grec[t.i]   = GradRec<T>{c11i, c12i, c13i, c22i, c23i, c33i, divv, T(a.alpha[t.i])};
+        a.avrec[t.i]  = AVRec<T>{hrI.vx, hrI.vy, hrI.vz, hrI.c, hrI.vol, divv, T(0), T(0)};
         divvOut       = double(divv);
     }
     reduceOrdered<true, (kMode & kModeBatch) != 0>(divvOut, a.n, a.reduce + 0, a.batch, 0);
@@ -433,6 +434,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvFusedKernel(Chai
         a.divv[t.i]   = divv;
         a.curlv[t.i]  = curlv;
         a.grec[t.i]   = GradRec<T>{c11i, c12i, c13i, c22i, c23i, c33i, divv, T(a.alpha[t.i])};
+        a.avrec[t.i]  = AVRec<T>{hr.vx, hr.vy, hr.vz, hr.c, hr.vol, divv, T(0), T(0)};
         divvOut       = double(divv);
     }
     reduceOrdered<true, (kMode & kModeBatch) != 0>(divvOut, a.n, a.reduce + 0, a.batch, 0);
@@ -472,8 +474,8 @@ __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays
             if (q >= qn) { break; }
             uint32_t j = js[q];
             Pos<T> pj      = posOf(a, j);
-            HydroRec<T> hj = loadHydro(a.hrec + j);
-            T divvJ        = __ldg(reinterpret_cast<const T*>(a.grec + j) + 6); // the divv slot of the record
+            AVRec<T> hj    = loadAV(a.avrec + j);
+            T divvJ        = hj.divv;
             Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
             T dist         = sqrt(r.rx * r.rx + r.ry * r.ry + r.rz * r.rz);
             T rv           = r.rx * (hr.vx - hj.vx) + r.ry * (hr.vy - hj.vy) + r.rz * (hr.vz - hj.vz);

@@ -64,7 +64,7 @@ struct sphb_sim
     DeviceBuffer<unsigned> nc;
     DeviceBuffer<char> derived[kNumDerived];
     DeviceBuffer<double> du;
-    DeviceBuffer<char> hrec, grec;
+    DeviceBuffer<char> hrec, grec, avrec;
     DeviceBuffer<char> dvrec, dv; // AV cleaning only: symmetrised velocity gradients (record + 6 arrays)
     DeviceBuffer<double> whD, whdD;
     DeviceBuffer<float> whF, whdF;
@@ -142,6 +142,7 @@ int allocateSim(sphb_sim& s)
     SPHB_TRY(s.du.reserve(n));
     SPHB_TRY(s.hrec.reserve(n * 8 * s.elemBytes()));
     SPHB_TRY(s.grec.reserve(n * 8 * s.elemBytes()));
+    SPHB_TRY(s.avrec.reserve(n * 8 * s.elemBytes()));
     if (s.p.av_clean)
     {
         SPHB_TRY(s.dvrec.reserve(n * 8 * s.elemBytes()));
@@ -315,6 +316,7 @@ ChainArrays<T> chainArrays(sphb_sim& s)
     a.hrec   = reinterpret_cast<HydroRec<T>*>(s.hrec.data());
     a.grec   = reinterpret_cast<GradRec<T>*>(s.grec.data());
     a.reduce = s.reduce.data();
+    a.avrec  = reinterpret_cast<AVRec<T>*>(s.avrec.data());
     if (s.p.av_clean)
     {
         a.dvrec = reinterpret_cast<DVRec<T>*>(s.dvrec.data());
