@@ -324,7 +324,8 @@ __device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t,
                                           uint32_t (&js)[kNbChunk])
 {
     const uint4* p = reinterpret_cast<const uint4*>(nidx + nidxAt(t.group, ngPad, q0, t.lane));
-    uint4 a = __ldg(p), b = __ldg(p + 1);
+    // the lists are read once per kernel: streaming loads keep them from evicting the neighbour records in L2
+    uint4 a = __ldcs(p), b = __ldcs(p + 1);
     js[0] = a.x;
     js[1] = a.y;
     js[2] = a.z;

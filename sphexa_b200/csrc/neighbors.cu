@@ -208,8 +208,8 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         auto storeChunk = [&](unsigned c) {
             uint4* dst       = reinterpret_cast<uint4*>(nidx + nidxAt(group, ngPad, c * kNbChunk, lane));
             const uint4* src = reinterpret_cast<const uint4*>(chunk);
-            dst[0]           = src[0];
-            dst[1]           = src[1];
+            __stcs(dst, src[0]); // streaming: the lists are next read once per J-loop
+            __stcs(dst + 1, src[1]);
         };
 
         // test the staged 32 candidates against this lane's particle and append the neighbours in index order
