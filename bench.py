@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (48^3, 20 steps)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-instance ensemble leg")
+    ap.add_argument("--no-noh", action="store_true", help="skip the Noh 160^3 leg")
     return ap.parse_args()
 
 
@@ -439,6 +440,8 @@ def run_ours(args, ws, rank, local):
         line["adjoint"] = adjoint_leg()
     if rank == 0 and not args.no_ensemble:
         line["ensemble"] = ensemble_leg()
+    if rank == 0 and not args.no_noh:
+        line["noh"] = noh_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ic, n)
     if dist is not None:
@@ -513,6 +516,38 @@ def adjoint_leg(side=48, steps=20, dt=1e-5, every=5, directions=64, eps=1e-6) ->
     out["fp32_vs_fp64"] = {"dL_du0_rel_l2": float(np.linalg.norm(g32 - g64) / np.linalg.norm(g64)),
                            "dL_du0_max_rel_to_max": float(np.max(np.abs(g32 - g64)) / np.max(np.abs(g64))),
                            "dL_dalphamax_rel": abs(a32 - a64) / max(abs(a64), 1e-300)}
+    return out
+
+
+def noh_leg(side=160, steps=20, warmup=3) -> dict:
+    """Noh implosion: the side^3 lattice cut to r <= 0.5 (open box), mixed precision. Device time of `steps` steps
+    after `warmup` (CUDA events on the simulation's stream), the largest density reached, total-energy drift."""
+    import torch
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.noh(side)
+    n = ic["x"].size
+    sim = Simulation(ic, "mixed")
+    stream = torch.cuda.ExternalStream(sim.lib.sphb_sim_stream(sim.h))
+    for _ in range(warmup):
+        sim.step()
+    e0 = sim.scalars()["etot"]
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(steps):
+        sim.step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b)
+    rho = sim.get("kx") * sim.get("m") / sim.get("xm")
+    s = sim.scalars()
+    out = {"workload": f"noh-{side}^3 lattice cut to r <= 0.5 ({n:,} particles), open box, mixed precision",
+           "particles": n, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
+           "particle_steps_per_s": n * steps / (ms * 1e-3), "max_density": float(rho.max()),
+           "time": s["ttot"], "energy_drift": abs(s["etot"] - e0) / abs(e0)}
+    sim.close()
     return out
 
 

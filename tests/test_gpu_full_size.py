@@ -1,0 +1,63 @@
+"""GPU checks at the benchmark size (Sedov 128^3 = 2,097,152 particles, mixed and FP64) through properties that do
+not need the oracle to run at that size: SFC keys sorted and ids a permutation after every sync; every list entry a
+distinct particle within 2h_i, in ascending index order; the count equal to the reference CPU search on a sample of
+particles (recomputed here by brute force on the CPU for those particles); linear momentum conserved to round-off
+by the antisymmetric pair forces; total energy drift bounded."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sedov128(cuda_device):
+    from sphexa_b200 import ic as icm
+    return icm.sedov(128)
+
+
+def _check_lists(sim, sample, rng):
+    n = sim.n
+    x, y, z, h = (sim.get(f) for f in ("x", "y", "z", "h"))
+    nc = sim.get("nc").astype(np.int64)
+    nb = sim.neighbors()
+    ngmax = nb.shape[1]
+    for i in rng.choice(n, sample, replace=False):
+        cnt = min(nc[i] - 1, ngmax)
+        lst = nb[i, :cnt].astype(np.int64)
+        assert np.all(np.diff(lst) > 0), i           # ascending, no duplicates
+        assert not np.any(lst == i), i
+        d = np.stack([x[lst] - x[i], y[lst] - y[i], z[lst] - z[i]])
+        d -= np.rint(d)                               # periodic unit box
+        r2 = np.sum(d * d, axis=0)
+        assert np.all(r2 < 4.0 * h[i] * h[i]), i
+        # brute-force count of every particle within 2h_i (the list is complete unless capped at ngmax)
+        D = np.stack([x - x[i], y - y[i], z - z[i]])
+        D -= np.rint(D)
+        full = int(np.sum(np.sum(D * D, axis=0) < 4.0 * h[i] * h[i])) - 1
+        assert full == nc[i] - 1, (i, full, nc[i])
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64"])
+def test_sedov128_invariants(sedov128, precision):
+    from sphexa_b200.simulation import Simulation
+    rng = np.random.default_rng(5)
+    sim = Simulation(sedov128, precision)
+    e0 = None
+    for step in range(6):
+        sim.compute_forces()
+        keys = sim.keys()
+        assert np.all(np.diff(keys.astype(np.uint64)) >= 0)
+        ids = sim.get("id").astype(np.int64)
+        assert np.array_equal(np.sort(ids), np.arange(sim.n))
+        s = sim.scalars()
+        if e0 is None:
+            e0 = s["etot"]
+        # Sedov starts at rest and the pair forces are antisymmetric: |P| stays at round-off of sum m |v|
+        m, vx, vy, vz = (sim.get(f) for f in ("m", "vx", "vy", "vz"))
+        scale = np.sum(m * np.sqrt(vx * vx + vy * vy + vz * vz)) + 1e-300
+        assert s["linmom"] <= 1e-5 * scale, (step, s["linmom"], scale)
+        if step in (0, 5):
+            _check_lists(sim, 64, rng)
+        sim.integrate()
+    assert abs(sim.scalars()["etot"] - e0) <= 1e-3 * abs(e0)
+    sim.close()
