@@ -196,7 +196,21 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         {
             reach = fmaxf(reach, __shfl_xor_sync(0xffffffffu, reach, off));
         }
-        const float band = active ? bandOf(reach, twoH) : 0.f;
+        // Differences of two coordinates that were each folded to the nearest image of the group centre are the
+        // minimum image of the pair only while 2h + (offset from the centre) < L/2 on every periodic axis. Groups
+        // whose reach exceeds that (search radii comparable to the box) test every candidate exactly instead.
+        bool wrapTest = false;
+        float maxSpan = 0.f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+        {
+            if (box.periodic[k])
+            {
+                wrapTest = wrapTest || reach >= 0.5f * lenf[k];
+                maxSpan  = fmaxf(maxSpan, 0.5f * lenf[k]);
+            }
+        }
+        const float band = active ? bandOf(wrapTest ? fmaxf(reach, maxSpan) : reach, twoH) : 0.f;
         const float r2lo = r2f * (1.f - band);
         const float r2hi = r2f * (1.f + band);
 
@@ -213,24 +227,33 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         };
 
         // test the staged 32 candidates against this lane's particle and append the neighbours in index order
-        auto testStaged = [&]() {
+        auto testStaged = [&](int numReal) {
             if (!active) { return; }
             // bit k of sure: candidate k lies inside the sphere by its FP32 distance (below the band); of maybe: it
             // may (below the upper edge of the band)
             unsigned maybe = 0u, sure = 0u;
-            const float2 mx = make_float2(-rix, -rix), my = make_float2(-riy, -riy), mz = make_float2(-riz, -riz);
-#pragma unroll
-            for (int k = 0; k < kWarp; k += 2)
+            if (!wrapTest)
             {
-                float2 X  = *reinterpret_cast<const float2*>(&sh.cx[warp][k]);
-                float2 Y  = *reinterpret_cast<const float2*>(&sh.cy[warp][k]);
-                float2 Z  = *reinterpret_cast<const float2*>(&sh.cz[warp][k]);
-                float2 dx = __fadd2_rn(X, mx);
-                float2 dy = __fadd2_rn(Y, my);
-                float2 dz = __fadd2_rn(Z, mz);
-                float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                maybe |= (unsigned(d2.x < r2hi) << k) | (unsigned(d2.y < r2hi) << (k + 1));
-                sure |= (unsigned(d2.x < r2lo) << k) | (unsigned(d2.y < r2lo) << (k + 1));
+                const float2 mx = make_float2(-rix, -rix), my = make_float2(-riy, -riy), mz = make_float2(-riz, -riz);
+#pragma unroll
+                for (int k = 0; k < kWarp; k += 2)
+                {
+                    float2 X  = *reinterpret_cast<const float2*>(&sh.cx[warp][k]);
+                    float2 Y  = *reinterpret_cast<const float2*>(&sh.cy[warp][k]);
+                    float2 Z  = *reinterpret_cast<const float2*>(&sh.cz[warp][k]);
+                    float2 dx = __fadd2_rn(X, mx);
+                    float2 dy = __fadd2_rn(Y, my);
+                    float2 dz = __fadd2_rn(Z, mz);
+                    float2 d2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                    maybe |= (unsigned(d2.x < r2hi) << k) | (unsigned(d2.y < r2hi) << (k + 1));
+                    sure |= (unsigned(d2.x < r2lo) << k) | (unsigned(d2.y < r2lo) << (k + 1));
+                }
+            }
+            else
+            {
+                // every real candidate of the chunk goes through the exact FP64 test below, which folds the pair
+                // difference itself (padding sits at the end of the last chunk)
+                maybe = numReal >= kWarp ? 0xffffffffu : ((1u << numReal) - 1u);
             }
             // candidates too close to the search radius for FP32: the exact test of the reference (rare)
             unsigned band = maybe & ~sure;
@@ -362,7 +385,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                         sh.cj[warp][lane] = -1;
                     }
                     __syncwarp();
-                    testStaged();
+                    testStaged(totalCand - cbase);
                     __syncwarp();
                 }
             }
