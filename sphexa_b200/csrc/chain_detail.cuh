@@ -133,12 +133,20 @@ __device__ __forceinline__ void shiftPbc(double& rx, double& ry, double& rz, dou
     }
 }
 
+//! one 32-byte (256-bit) read-only vector load of 8 floats; p must be 32-byte aligned
+__device__ __forceinline__ void ldg256(const void* p, float (&v)[8])
+{
+    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+        : "l"(p));
+}
+
 //! 32-byte read-only load as two 16-byte vector loads (one sector)
 __device__ __forceinline__ double4 ldg4(const double4* p)
 {
-    const double2* q = reinterpret_cast<const double2*>(p);
-    double2 lo = __ldg(q), hi = __ldg(q + 1);
-    return make_double4(lo.x, lo.y, hi.x, hi.y);
+    double4 v;
+    asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];" : "=d"(v.x), "=d"(v.y), "=d"(v.z), "=d"(v.w) : "l"(p));
+    return v;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -211,9 +219,9 @@ __device__ __forceinline__ HydroRec<T> loadHydro(const HydroRec<T>* p)
     }
     else
     {
-        const float4* q = reinterpret_cast<const float4*>(p);
-        float4 a = __ldg(q), b = __ldg(q + 1);
-        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
+        float v[8];
+        ldg256(p, v);
+        r = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
     }
     return r;
 }
@@ -230,9 +238,9 @@ __device__ __forceinline__ GradRec<T> loadGrad(const GradRec<T>* p)
     }
     else
     {
-        const float4* q = reinterpret_cast<const float4*>(p);
-        float4 a = __ldg(q), b = __ldg(q + 1);
-        r = {T(a.x), T(a.y), T(a.z), T(a.w), T(b.x), T(b.y), T(b.z), T(b.w)};
+        float v[8];
+        ldg256(p, v);
+        r = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
     }
     return r;
 }
@@ -271,10 +279,9 @@ __device__ __forceinline__ AVRec<T> loadAV(const AVRec<T>* p)
     }
     else
     {
-        const float4* q = reinterpret_cast<const float4*>(p);
-        float4 a = __ldg(q);
-        float2 b = __ldg(reinterpret_cast<const float2*>(q + 1));
-        r = {a.x, a.y, a.z, a.w, b.x, b.y, 0.f, 0.f};
+        float v[8];
+        ldg256(p, v);
+        r = {v[0], v[1], v[2], v[3], v[4], v[5], 0.f, 0.f};
     }
     return r;
 }
