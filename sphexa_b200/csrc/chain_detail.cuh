@@ -330,17 +330,12 @@ __device__ __forceinline__ T avRvCorrection(T rx, T ry, T rz, T etaAb, T etaCrit
 __device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t, unsigned ngPad, unsigned q0,
                                           uint32_t (&js)[kNbChunk])
 {
-    const uint4* p = reinterpret_cast<const uint4*>(nidx + nidxAt(t.group, ngPad, q0, t.lane));
-    // the lists are read once per kernel: streaming loads keep them from evicting the neighbour records in L2
-    uint4 a = __ldcs(p), b = __ldcs(p + 1);
-    js[0] = a.x;
-    js[1] = a.y;
-    js[2] = a.z;
-    js[3] = a.w;
-    js[4] = b.x;
-    js[5] = b.y;
-    js[6] = b.z;
-    js[7] = b.w;
+    const uint32_t* p = nidx + nidxAt(t.group, ngPad, q0, t.lane);
+    // one 256-bit load of the chunk's sector; the lists are read once per kernel, so the streaming (evict-first)
+    // hint keeps them from evicting the neighbour records in L2
+    asm("ld.global.cs.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(js[0]), "=r"(js[1]), "=r"(js[2]), "=r"(js[3]), "=r"(js[4]), "=r"(js[5]), "=r"(js[6]), "=r"(js[7])
+        : "l"(p));
 }
 
 /*! Maximum (kMax) or minimum of one double per thread, published as ordered bits with one atomic per block on

@@ -220,10 +220,13 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         // this lane's chunk buffer and its store to the chunked list layout (nidxAt)
         uint32_t* chunk = sh.nbuf[warp][lane];
         auto storeChunk = [&](unsigned c) {
-            uint4* dst       = reinterpret_cast<uint4*>(nidx + nidxAt(group, ngPad, c * kNbChunk, lane));
+            uint32_t* dst    = nidx + nidxAt(group, ngPad, c * kNbChunk, lane);
             const uint4* src = reinterpret_cast<const uint4*>(chunk);
-            __stcs(dst, src[0]); // streaming: the lists are next read once per J-loop
-            __stcs(dst + 1, src[1]);
+            uint4 a = src[0], b = src[1];
+            // one 256-bit streaming store of the whole sector (the lists are next read once per J-loop)
+            asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(a.x), "r"(a.y),
+                         "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+                         : "memory");
         };
 
         // test the staged 32 candidates against this lane's particle and append the neighbours in index order
