@@ -35,6 +35,7 @@ struct NbShared
     int blkPre[kNbWarps][kLeafCap + 1]; // exclusive prefix of the number of blocks per buffered leaf
     int pStart[kNbWarps][kWarp];       // surviving pieces (block and leaf intersections) of one round
     int pPre[kNbWarps][kWarp + 1];     // exclusive prefix of their lengths
+    uint8_t pieceOf[kNbWarps][kWarp * kBlockSize]; // candidate of the round -> its piece
     // staged candidates: position relative to the group centre (FP32, pairs loaded as float2) and index
     alignas(16) float cx[kNbWarps][kWarp];
     alignas(16) float cy[kNbWarps][kWarp];
@@ -342,7 +343,6 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                     }
                 }
                 unsigned m = __ballot_sync(0xffffffffu, keep);
-                int numPieces = __popc(m);
                 int totalCand;
                 int ex = warpExclusive(keep ? plen : 0, lane, &totalCand);
                 if (keep)
@@ -350,6 +350,10 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                     int pos     = __popc(m & ((1u << lane) - 1u));
                     pStart[pos] = ps;
                     pPre[pos]   = ex;
+                    for (int q = 0; q < plen; ++q)
+                    {
+                        sh.pieceOf[warp][ex + q] = uint8_t(pos);
+                    }
                 }
                 __syncwarp();
                 for (int cbase = 0; cbase < totalCand; cbase += kWarp)
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                     int tc = cbase + lane;
                     if (tc < totalCand)
                     {
-                        int rr = findSlot(pPre, numPieces, tc);
+                        int rr = sh.pieceOf[warp][tc];
                         int j  = pStart[rr] + (tc - pPre[rr]);
                         if (j < 0 || size_t(j) >= n)
                         {
