@@ -221,6 +221,19 @@ int sphb_sim_set_params(sphb_sim* sim, const sphb_params* params);
  *  No counterpart in the reference. */
 int sphb_sim_step_vjp(sphb_sim* sim, const double* const* adj_post, double* const* adj_pre, double* alphamax_bar);
 
+/*! Reserve device memory for `slots` recorded steps (about 1 KB per particle each). Recording replaces the force
+ *  recomputation of sphb_sim_step_vjp when the caller replays a segment of steps anyway (checkpointing). */
+int sphb_sim_tape_reserve(sphb_sim* sim, int slots);
+
+/*! One step (as sphb_sim_step, fixed time step required) that also records in `slot` everything the step's adjoint
+ *  reads: the post-sync state, lists, derived fields and the adjoint tape. */
+int sphb_sim_step_record(sphb_sim* sim, int slot);
+
+/*! sphb_sim_step_vjp for the step recorded in `slot`, without recomputing its forces. Leaves the simulation holding
+ *  that step's recorded post-force state. */
+int sphb_sim_step_vjp_recorded(sphb_sim* sim, int slot, const double* const* adj_post, double* const* adj_pre,
+                               double* alphamax_bar);
+
 /* ---------------------------------------------------------------------------------------------------------------- */
 /* 4. Batched ensemble                                                                                              */
 /* ---------------------------------------------------------------------------------------------------------------- */

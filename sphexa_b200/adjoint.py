@@ -1,10 +1,12 @@
 """Gradients through K steps of the VE hydro propagator with the hand-written adjoint kernels (sphb_sim_step_vjp).
 
 The forward runs K steps at a fixed time step and keeps a checkpoint of the full particle state every
-`checkpoint_every` steps. The backward pass walks the checkpoints in reverse: it restores one, recomputes the forward
-steps of that segment to recover each step's starting state, then applies the step adjoints in reverse order. Each
-step adjoint recomputes the step's forces with the same sort, neighbour lists and branch choices as the forward
-(they are deterministic functions of the restored state), so neighbour lists are frozen per step by construction.
+`checkpoint_every` steps. The backward pass walks the checkpoints in reverse: it restores one and replays that
+segment's steps once, recording each step's forces (the post-sync state, neighbour lists, derived fields and the
+adjoint tape) in a device slot; then it applies the step adjoints in reverse order from those records. Each replayed
+step makes the same sort, neighbour lists and branch choices as the forward (they are deterministic functions of the
+restored state), so neighbour lists are frozen per step by construction. With recorded=False each step adjoint
+recomputes its step's forces instead of reading a record (one more force computation per step, less memory).
 
 Objective: the total kinetic energy sum_i m_i |v_i|^2 / 2 after K steps. Parameters: the initial internal energy per
 particle u0 = cv * temp0 (in the order of the initial conditions) and the artificial-viscosity alphamax
@@ -27,7 +29,9 @@ def ideal_gas_cv(mui: float, gamma: float) -> float:
 
 class AdjointRun:
     def __init__(self, ic: dict, precision: str = "fp64", dt: float = 1e-5, steps: int = 20,
-                 checkpoint_every: int = 5):
+                 checkpoint_every: int = 5, recorded: bool = True):
+        """recorded: replay each checkpoint segment once and record every step's forces for its adjoint
+        (sphb_sim_step_record); otherwise every step adjoint recomputes its forces (sphb_sim_step_vjp)."""
         import torch
         self.torch = torch
         self.ic = ic
@@ -35,6 +39,7 @@ class AdjointRun:
         self.dt = float(dt)
         self.steps = int(steps)
         self.every = int(checkpoint_every)
+        self.recorded = bool(recorded)
         self.n = int(ic["x"].size)
         self.cv = ideal_gas_cv(ic["params"]["mui"], ic["params"]["gamma"])
         self.sim = None
@@ -112,18 +117,28 @@ class AdjointRun:
             adj[FIELD_INDEX[f]] = m * v
         nxt = [t.empty(n, dtype=t.float64, device="cuda") for _ in CONSERVED_FIELDS]
         alphamax_bar = 0.0
+        if self.recorded:
+            self.sim.tape_reserve(self.every)
         for start in sorted(self.checkpoints, reverse=True):
             end = min(start + self.every, self.steps)
-            # recompute the segment's starting states from its checkpoint
-            states = [self.checkpoints[start]]
-            self.sim.load_state(*states[0])
-            for _ in range(start, end - 1):
-                self.sim.step()
-                states.append(self._store())
-            for s in reversed(range(start, end)):
-                self.sim.load_state(*states[s - start])
-                alphamax_bar += self.sim.step_vjp(adj, nxt)
-                adj, nxt = nxt, adj
+            self.sim.load_state(*self.checkpoints[start])
+            if self.recorded:
+                # replay the segment once, recording every step's forces, then apply the adjoints from the records
+                for s in range(start, end):
+                    self.sim.step_record(s - start)
+                for s in reversed(range(start, end)):
+                    alphamax_bar += self.sim.step_vjp_recorded(s - start, adj, nxt)
+                    adj, nxt = nxt, adj
+            else:
+                # replay the segment for its starting states; each step adjoint recomputes its forces
+                states = [self.checkpoints[start]]
+                for _ in range(start, end - 1):
+                    self.sim.step()
+                    states.append(self._store())
+                for s in reversed(range(start, end)):
+                    self.sim.load_state(*states[s - start])
+                    alphamax_bar += self.sim.step_vjp(adj, nxt)
+                    adj, nxt = nxt, adj
         ids = self.checkpoints[0][1].cpu().numpy()
         gtemp = adj[FIELD_INDEX["temp"]].cpu().numpy()
         grad_u0 = np.empty(n)

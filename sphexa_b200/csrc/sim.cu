@@ -99,6 +99,10 @@ struct sphb_sim
     DeviceBuffer<int> tapeJ;
     DeviceBuffer<char> adjT;
     DeviceBuffer<double> adjWork, adjScalar;
+    // recorded steps: copies of everything the step adjoint reads, one slot per step of a checkpoint segment
+    DeviceBuffer<char> tapeSlots;
+    size_t tapeSlotBytes{0};
+    int numTapeSlots{0};
 
     cudaEvent_t ev[kNumStages + 1]{};
     float stageMs[kNumStages]{};
@@ -518,6 +522,52 @@ int allocateAdjoint(sphb_sim& s)
     SPHB_TRY(s.adjT.reserve(size_t(kNumAdjFields) * n * s.elemBytes()));
     SPHB_TRY(s.adjWork.reserve(14 * n));
     SPHB_TRY(s.adjScalar.reserve(1));
+    return kOk;
+}
+
+//! the device buffers a step adjoint reads after the taped force computation (pointer, bytes)
+std::vector<std::pair<void*, size_t>> tapedBuffers(sphb_sim& s)
+{
+    size_t n = s.n, e = s.elemBytes();
+    std::vector<std::pair<void*, size_t>> b;
+    for (int k = 0; k < kNumConserved; ++k)
+    {
+        b.push_back({s.f[k].data(), n * sizeof(double)});
+    }
+    b.push_back({s.order.data(), n * sizeof(uint32_t)});
+    b.push_back({s.pos.data(), n * sizeof(double4)});
+    if (s.mixed) { b.push_back({s.posq.data(), n * sizeof(int4)}); }
+    b.push_back({s.nidx.data(), s.numGroups() * size_t(paddedNgmax(s.p.ngmax)) * kWarp * sizeof(uint32_t)});
+    b.push_back({s.nc.data(), n * sizeof(unsigned)});
+    for (int d = 0; d < kNumDerived; ++d)
+    {
+        b.push_back({s.derived[d].data(), n * e});
+    }
+    b.push_back({s.du.data(), n * sizeof(double)});
+    b.push_back({s.hrec.data(), n * 8 * e});
+    b.push_back({s.grec.data(), n * 8 * e});
+    b.push_back({s.avrec.data(), n * 8 * e});
+    b.push_back({s.tapeT.data(), 8 * n * e});
+    b.push_back({s.tapeJ.data(), n * sizeof(int)});
+    b.push_back({s.hPre.data(), n * sizeof(double)});
+    b.push_back({s.alphaPre.data(), n * sizeof(double)});
+    return b;
+}
+
+size_t alignTape(size_t x) { return (x + 255) / 256 * 256; }
+
+//! copy the taped buffers into slot (save) or back from it
+int copyTape(sphb_sim& s, int slot, bool save)
+{
+    char* base = s.tapeSlots.data() + size_t(slot) * s.tapeSlotBytes;
+    size_t off = 0;
+    for (auto [ptr, bytes] : tapedBuffers(s))
+    {
+        void* dst = save ? static_cast<void*>(base + off) : ptr;
+        void* src = save ? ptr : static_cast<void*>(base + off);
+        SPHB_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s.stream));
+        off += alignTape(bytes);
+    }
     return kOk;
 }
 
@@ -964,6 +1014,51 @@ extern "C" int sphb_sim_step_vjp(sphb_sim* s, const double* const* adj_post, dou
         rc = s->mixed ? runStepVjp<float>(*s, adj_post, adj_pre, alphamax_bar)
                       : runStepVjp<double>(*s, adj_post, adj_pre, alphamax_bar);
     }
+    s->taping = false;
+    return rc;
+}
+
+extern "C" int sphb_sim_tape_reserve(sphb_sim* s, int slots)
+{
+    if (!s || slots < 1) { return SPHB_ERR_ARG; }
+    if (!s->uploaded || s->p.av_clean) { return SPHB_ERR_STATE; }
+    if (!s->hPre.data()) { SPHB_TRY(allocateAdjoint(*s)); }
+    size_t bytes = 0;
+    for (auto pb : tapedBuffers(*s))
+    {
+        bytes += alignTape(pb.second);
+    }
+    SPHB_TRY(s->tapeSlots.reserve(bytes * size_t(slots)));
+    s->tapeSlotBytes = bytes;
+    s->numTapeSlots  = slots;
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_step_record(sphb_sim* s, int slot)
+{
+    if (!s || slot < 0) { return SPHB_ERR_ARG; }
+    if (!s->uploaded || !(s->fixedDt > 0) || slot >= s->numTapeSlots) { return SPHB_ERR_STATE; }
+    s->taping = true;
+    int rc    = computeForces(*s);
+    s->taping = false;
+    if (rc != SPHB_OK) { return rc; }
+    SPHB_TRY(copyTape(*s, slot, true));
+    return integrateStep(*s);
+}
+
+extern "C" int sphb_sim_step_vjp_recorded(sphb_sim* s, int slot, const double* const* adj_post,
+                                          double* const* adj_pre, double* alphamax_bar)
+{
+    if (!s || !adj_post || !adj_pre || slot < 0) { return SPHB_ERR_ARG; }
+    for (int f = 0; f < kNumConserved; ++f)
+    {
+        if (!adj_post[f] || !adj_pre[f] || adj_post[f] == adj_pre[f]) { return SPHB_ERR_ARG; }
+    }
+    if (!s->uploaded || !(s->fixedDt > 0) || slot >= s->numTapeSlots) { return SPHB_ERR_STATE; }
+    SPHB_TRY(copyTape(*s, slot, false));
+    s->taping = true;
+    int rc = s->mixed ? runStepVjp<float>(*s, adj_post, adj_pre, alphamax_bar)
+                      : runStepVjp<double>(*s, adj_post, adj_pre, alphamax_bar);
     s->taping = false;
     return rc;
 }

@@ -139,6 +139,22 @@ class Simulation:
         L.check(self.lib.sphb_sim_step_vjp(self.h, post, pre, C.byref(am)), "step_vjp")
         return am.value
 
+    def tape_reserve(self, slots: int):
+        L.check(self.lib.sphb_sim_tape_reserve(self.h, int(slots)), "tape_reserve")
+
+    def step_record(self, slot: int) -> int:
+        rc = self.lib.sphb_sim_step_record(self.h, int(slot))
+        if rc not in (L.SPHB_OK, 4):
+            L.check(rc, "step_record")
+        return rc
+
+    def step_vjp_recorded(self, slot: int, adj_post, adj_pre) -> float:
+        post = (C.c_void_p * len(adj_post))(*[L.ptr(f).value for f in adj_post])
+        pre = (C.c_void_p * len(adj_pre))(*[L.ptr(f).value for f in adj_pre])
+        am = C.c_double(0.0)
+        L.check(self.lib.sphb_sim_step_vjp_recorded(self.h, int(slot), post, pre, C.byref(am)), "step_vjp_recorded")
+        return am.value
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.sphb_sim_destroy(self.h)

@@ -134,3 +134,19 @@ def test_autograd_function_and_fp32_adjoint(setup):
     rel = np.linalg.norm(g32 - g64) / np.linalg.norm(g64)
     assert rel < 1e-3, rel
     assert abs(a32 - a64) <= 1e-2 * abs(a64) + 1e-30, (a32, a64)
+
+
+def test_recorded_and_recomputed_adjoints_agree(setup):
+    """The backward pass from recorded steps equals the one that recomputes every step's forces (up to the order of
+    the atomic scatters)."""
+    ic, u0, AdjointRun, _ = setup
+    am0 = ic["params"]["alphamax"]
+    grads = []
+    for recorded in (True, False):
+        run = AdjointRun(ic, "fp64", dt=1e-5, steps=7, checkpoint_every=3, recorded=recorded)
+        run.forward(u0, am0)
+        grads.append(run.backward())
+        run.close()
+    (g1, a1), (g2, a2) = grads
+    assert np.linalg.norm(g1 - g2) <= 1e-10 * np.linalg.norm(g2)
+    assert abs(a1 - a2) <= 1e-10 * abs(a2)
