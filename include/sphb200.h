@@ -104,6 +104,14 @@ int sphb_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, int init_values
  *  No counterpart in the reference. */
 int sphb_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* stream);
 
+/*! Same result as sphb_sort_by_key with init_values = 1, for keys that are nearly in order (the particles of the
+ *  previous step, which moved a fraction of a smoothing length). If no adjacent pair is out of order nothing moves
+ *  and *identity is set to 1. Otherwise the 2048-key tiles that hold inversions are sorted in shared memory (two
+ *  overlapping tilings), and the full radix sort runs only if inversions remain. Host-blocking (two small reads).
+ *  No counterpart in the reference (it sorts from scratch every step, assignment.hpp:112). */
+int sphb_sort_by_key_nearly_sorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, size_t scratch_bytes,
+                                   int* identity, void* stream);
+
 /*! Largest n accepted by sphb_sort_by_key_static. */
 size_t sphb_sort_by_key_static_max(void);
 

@@ -235,25 +235,31 @@ int syncDomain(sphb_sim& s)
     SPHB_TRY(updateBox(s));
     s.boxFirstCall = false;
     SPHB_TRY(launchSfcKeys(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.keys.data(), s.n, s.box, st));
-    SPHB_TRY(sortByKey(s.keys.data(), s.order.data(), s.n, true, s.sortScratch.data(), s.sortScratch.capacity(), st));
+    // particles move a fraction of h per step, so the previous order is nearly sorted (often exactly)
+    bool identity = false;
+    SPHB_TRY(sortNearlySorted(s.keys.data(), s.order.data(), s.n, s.sortScratch.data(), s.sortScratch.capacity(),
+                              &identity, st));
     SPHB_TRY(updateGlobalTree(s.gtree, s.keys.data(), s.n, s.ts, st));
 
-    // reorder every conserved field and the ids into SFC order
-    const void* src[kNumConserved + 1];
-    void* dst[kNumConserved + 1];
-    for (int k = 0; k < kNumConserved; ++k)
+    if (!identity)
     {
-        src[k] = s.f[k].data();
-        dst[k] = s.fAlt[k].data();
+        // reorder every conserved field and the ids into SFC order
+        const void* src[kNumConserved + 1];
+        void* dst[kNumConserved + 1];
+        for (int k = 0; k < kNumConserved; ++k)
+        {
+            src[k] = s.f[k].data();
+            dst[k] = s.fAlt[k].data();
+        }
+        src[kNumConserved] = s.id.data();
+        dst[kNumConserved] = s.idAlt.data();
+        SPHB_TRY(gather8(s.order.data(), s.n, kNumConserved + 1, src, dst, st));
+        for (int k = 0; k < kNumConserved; ++k)
+        {
+            s.f[k].swap(s.fAlt[k]);
+        }
+        s.id.swap(s.idAlt);
     }
-    src[kNumConserved] = s.id.data();
-    dst[kNumConserved] = s.idAlt.data();
-    SPHB_TRY(gather8(s.order.data(), s.n, kNumConserved + 1, src, dst, st));
-    for (int k = 0; k < kNumConserved; ++k)
-    {
-        s.f[k].swap(s.fAlt[k]);
-    }
-    s.id.swap(s.idAlt);
 
     bool converged = false;
     if (s.ftree.firstCall)

@@ -111,6 +111,94 @@ __global__ void iotaKernel(uint32_t* v, size_t n)
     if (i < n) { v[i] = uint32_t(i); }
 }
 
+//! *count += number of adjacent pairs with keys[i] > keys[i + 1] (one atomic per block)
+__global__ void __launch_bounds__(256) inversionsKernel(const uint64_t* __restrict__ keys, size_t n,
+                                                        uint32_t* count)
+{
+    uint32_t c = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i + 1 < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        c += keys[i] > keys[i + 1] ? 1u : 0u;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    __shared__ uint32_t warpSum[8];
+    if ((threadIdx.x & 31) == 0) { warpSum[threadIdx.x >> 5] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t s = 0;
+        for (int w = 0; w < 8; ++w)
+        {
+            s += warpSum[w];
+        }
+        if (s) { atomicAdd(count, s); }
+    }
+}
+
+constexpr int kRepairTile    = 2048;
+constexpr int kRepairThreads = 256;
+
+/*! Stable sort of one tile of (key, value) pairs in shared memory, tile t covering [offset + t T, offset + (t+1) T),
+ *  skipped when the tile and its left neighbour pair are already in order. Bitonic network on (key, position in the
+ *  tile), so equal keys keep their order; positions past n are padded with the largest key. */
+__global__ void __launch_bounds__(kRepairThreads) repairTilesKernel(uint64_t* keys, uint32_t* vals, size_t n,
+                                                                   size_t offset)
+{
+    __shared__ uint64_t sk[kRepairTile];
+    __shared__ uint32_t sv[kRepairTile];
+    __shared__ uint16_t sp[kRepairTile];
+    size_t t0 = offset + size_t(blockIdx.x) * kRepairTile;
+    if (t0 >= n) { return; }
+    size_t len = min(size_t(kRepairTile), n - t0);
+    bool d     = false;
+    for (size_t q = threadIdx.x; q + 1 < len; q += kRepairThreads)
+    {
+        d = d || keys[t0 + q] > keys[t0 + q + 1];
+    }
+    if (__syncthreads_or(d) == 0) { return; }
+    for (int q = threadIdx.x; q < kRepairTile; q += kRepairThreads)
+    {
+        bool in = size_t(q) < len;
+        sk[q]   = in ? keys[t0 + q] : ~uint64_t(0);
+        sv[q]   = in ? vals[t0 + q] : 0u;
+        sp[q]   = uint16_t(q);
+    }
+    __syncthreads();
+    for (int size = 2; size <= kRepairTile; size <<= 1)
+    {
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+        {
+            for (int q = threadIdx.x; q < kRepairTile; q += kRepairThreads)
+            {
+                int p = q ^ stride;
+                if (p > q)
+                {
+                    bool up      = (q & size) == 0;
+                    bool greater = sk[q] > sk[p] || (sk[q] == sk[p] && sp[q] > sp[p]);
+                    if (greater == up)
+                    {
+                        uint64_t k = sk[q];
+                        sk[q]      = sk[p];
+                        sk[p]      = k;
+                        uint32_t v = sv[q];
+                        sv[q]      = sv[p];
+                        sv[p]      = v;
+                        uint16_t o = sp[q];
+                        sp[q]      = sp[p];
+                        sp[p]      = o;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (size_t q = threadIdx.x; q < len; q += kRepairThreads)
+    {
+        keys[t0 + q] = sk[q];
+        vals[t0 + q] = sv[q];
+    }
+}
+
 /*! One onesweep pass over bits [shift, shift+8).
  *
  * Shared memory: per-warp digit counters (8 x 256), the tile's exclusive digit prefix (256) and the tile index.
@@ -305,6 +393,49 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
     return err ? kErrCapacity : kOk;
 }
 
+int sortNearlySorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, size_t scratchBytes, bool* identity,
+                     cudaStream_t stream)
+{
+    *identity = false;
+    if (n == 0)
+    {
+        *identity = true;
+        return kOk;
+    }
+    if (n >= (size_t(1) << 30)) { return kErrArg; }
+    if (!scratch || scratchBytes < sortScratchBytes(n)) { return kErrCapacity; }
+    SortScratch s = carve(scratch, n);
+    iotaKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(values, n);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    unsigned blocks = unsigned(std::min<size_t>(ceilDiv(n, 256 * 8), size_t(smCount()) * 8));
+    auto countInversions = [&](uint32_t* out) -> int {
+        SPHB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(uint32_t), stream));
+        inversionsKernel<<<blocks, 256, 0, stream>>>(keys, n, s.counters);
+        SPHB_CUDA_TRY(cudaGetLastError());
+        SPHB_CUDA_TRY(cudaMemcpyAsync(out, s.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    };
+    uint32_t inv = 0;
+    SPHB_TRY(countInversions(&inv));
+    if (inv == 0)
+    {
+        *identity = true;
+        return kOk;
+    }
+    // sparse, local disorder: stable sorts of the dirty tiles, then of the tiles shifted by half a tile
+    size_t tiles = ceilDiv(n, size_t(kRepairTile));
+    repairTilesKernel<<<unsigned(tiles), kRepairThreads, 0, stream>>>(keys, values, n, 0);
+    repairTilesKernel<<<unsigned(ceilDiv(n, size_t(kRepairTile))), kRepairThreads, 0, stream>>>(keys, values, n,
+                                                                                               kRepairTile / 2);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    SPHB_TRY(countInversions(&inv));
+    if (inv == 0) { return kOk; }
+    // otherwise the full radix sort; the repaired sequence kept equal keys in their original order, so a stable
+    // sort of it is the stable sort of the original
+    return sortByKey(keys, values, n, false, scratch, scratchBytes, stream);
+}
+
 int sortByKeyAsync(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,
                    unsigned passMask, uint32_t* errorOut, cudaStream_t stream)
 {
@@ -438,4 +569,14 @@ extern "C" int sphb_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, int 
     if (n && (!keys || !values)) { return SPHB_ERR_ARG; }
     return sphb::sortByKey(keys, values, n, init_values != 0, scratch, scratch_bytes,
                            static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int sphb_sort_by_key_nearly_sorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch,
+                                              size_t scratch_bytes, int* identity, void* stream)
+{
+    if (!identity || (n && (!keys || !values))) { return SPHB_ERR_ARG; }
+    bool id = false;
+    int rc  = sphb::sortNearlySorted(keys, values, n, scratch, scratch_bytes, &id, static_cast<cudaStream_t>(stream));
+    *identity = id ? 1 : 0;
+    return rc;
 }

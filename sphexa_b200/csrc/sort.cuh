@@ -12,6 +12,13 @@ size_t sortScratchBytes(size_t n);
 int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,
               cudaStream_t stream);
 
+/*! The same stable sort for keys that are nearly in order (the previous step's order of slowly moving particles):
+ *  values are set to 0..n-1; if no adjacent pair is out of order, nothing moves and *identity is set; otherwise the
+ *  tiles that hold inversions are sorted in shared memory (two overlapping tilings), and the full radix sort runs
+ *  only if that left any inversion. The result equals sortByKey's. */
+int sortNearlySorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, size_t scratchBytes, bool* identity,
+                     cudaStream_t stream);
+
 /*! The same sort without any host synchronisation (stream-capturable): runs exactly the passes of passMask (bit p
  *  = byte p of the key, from the least significant) and ORs a look-back timeout into *errorOut (device) if set. */
 int sortByKeyAsync(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,

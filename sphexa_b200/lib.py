@@ -46,7 +46,7 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches",
             "sphb_sim_stream", "sphb_sim_load_state", "sphb_sim_store_state", "sphb_probe_fma_peak",
             "sphb_sort_by_key_static", "sphb_sort_by_key_static_max", "sphb_sim_set_fixed_dt",
-            "sphb_sim_set_params", "sphb_sim_step_vjp", "sphb_sim_tape_reserve", "sphb_sim_step_record",
+            "sphb_sim_set_params", "sphb_sim_step_vjp", "sphb_sort_by_key_nearly_sorted", "sphb_sim_tape_reserve", "sphb_sim_step_record",
             "sphb_sim_step_vjp_recorded", "sphb_ensemble_create", "sphb_ensemble_destroy",
             "sphb_ensemble_upload", "sphb_ensemble_initial_sync", "sphb_ensemble_rebuild_trees",
             "sphb_ensemble_set_threads", "sphb_ensemble_autotune", "sphb_ensemble_step", "sphb_ensemble_size",
@@ -95,6 +95,7 @@ def load() -> C.CDLL:
         "sphb_sim_set_fixed_dt": (C.c_int, [P, C.c_double]),
         "sphb_sim_set_params": (C.c_int, [P, C.POINTER(Params)]),
         "sphb_sim_step_vjp": (C.c_int, [P, P, P, C.POINTER(C.c_double)]),
+        "sphb_sort_by_key_nearly_sorted": (C.c_int, [P, P, S, P, S, C.POINTER(C.c_int), P]),
         "sphb_sim_tape_reserve": (C.c_int, [P, C.c_int]),
         "sphb_sim_step_record": (C.c_int, [P, C.c_int]),
         "sphb_sim_step_vjp_recorded": (C.c_int, [P, C.c_int, P, P, C.POINTER(C.c_double)]),

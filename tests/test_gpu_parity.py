@@ -304,3 +304,36 @@ def test_zero_length_calls(lib):
     assert lib.sphb_sort_by_key(L.ptr(k), L.ptr(v), 0, 1, None, 0, None) == L.SPHB_OK
     assert lib.sphb_sort_by_key_static(L.ptr(k), L.ptr(v), 0, 1, None) == L.SPHB_OK
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("n,shift,far", [(5000, 0, False), (100_003, 40, False), (300_000, 700, False),
+                                         (200_000, 30, True)])
+def test_sort_nearly_sorted(lib, n, shift, far):
+    """Keys that are sorted except for local shuffles (up to `shift` positions) and duplicates; with `far`, a few keys
+    also move across the whole array so that the tile repair cannot fix them and the full sort must run. The result
+    must be the stable sort: the keys in order and the permutation of numpy's stable argsort."""
+    import torch
+    from sphexa_b200 import lib as L
+    rng = np.random.default_rng(n + shift)
+    keys = np.sort(rng.integers(0, 2 ** 62, n, dtype=np.uint64))
+    keys[1::5] = keys[0::5][: keys[1::5].size]  # duplicates
+    keys = np.sort(keys)
+    if shift:
+        for _ in range(n // 500):
+            i = int(rng.integers(0, n - shift))
+            j = i + int(rng.integers(1, shift + 1))
+            keys[i], keys[j] = keys[j], keys[i]
+    if far:
+        keys[10], keys[n - 10] = keys[n - 10], keys[10]
+    dk = _dev(keys.view(np.int64), torch)
+    dv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    nbytes = lib.sphb_sort_by_key_scratch_bytes(n)
+    scratch = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    ident = C.c_int(-1)
+    L.check(lib.sphb_sort_by_key_nearly_sorted(L.ptr(dk), L.ptr(dv), n, L.ptr(scratch), nbytes, C.byref(ident),
+                                               None), "nearly sorted")
+    torch.cuda.synchronize()
+    perm = np.argsort(keys, kind="stable")
+    assert ident.value == (1 if shift == 0 and not far else 0)
+    assert np.array_equal(dk.cpu().numpy().view(np.uint64), keys[perm])
+    assert np.array_equal(dv.cpu().numpy().view(np.uint32), perm.astype(np.uint32))
