@@ -36,10 +36,10 @@ KERNEL_STAGES = ("sync", "neighbors", "xmass", "ve_def_gradh_eos", "iad_divv_cur
 #: DRAM bytes (read + write) per particle of one launch of a stage's kernel from an ncu capture, keyed by
 #: (stage, precision); scaled by the particle count of the run. From the capture of one steady-state launch each at
 #: Sedov 96^3 (884,736 particles), mixed precision: dram__bytes_read.sum + dram__bytes_write.sum / particles.
-NCU_TRAFFIC = {("neighbors", "mixed"): (39.10e6 + 302.53e6) / 884736,
-               ("iad_divv_curlv", "mixed"): (410.44e6 + 47.86e6) / 884736,
-               ("av_switches", "mixed"): (440.46e6 + 28.88e6) / 884736,
-               ("momentum_energy", "mixed"): (436.79e6 + 17.14e6) / 884736}
+NCU_TRAFFIC = {("neighbors", "mixed"): (39.81e6 + 295.46e6) / 884736,
+               ("iad_divv_curlv", "mixed"): (411.25e6 + 70.80e6) / 884736,
+               ("av_switches", "mixed"): (472.70e6 + 29.30e6) / 884736,
+               ("momentum_energy", "mixed"): (437.48e6 + 17.40e6) / 884736}
 
 
 def parse():
