@@ -327,6 +327,7 @@ def run_ours(args, ws, rank, local):
         if with_clocks:
             clocks.start()
         launches0 = sim.kernel_launches()
+        search0 = sim.search_stats()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -339,12 +340,14 @@ def run_ours(args, ws, rank, local):
         barrier_sync()
         clk = clocks.stop() if with_clocks else None
         launches = sim.kernel_launches() - launches0
+        search = {k: v - search0[k] for k, v in sim.search_stats().items()}
         ms_local = e0.elapsed_time(e1)
         ms = max_over_ranks(ms_local)
         nc = sim.get("nc").astype(np.int64)
         pairs = int(np.minimum(nc - 1, int(ic["params"]["ngmax"])).sum())
         snap = {f: sim.get(f) for f in SNAP_FIELDS}
-        res = {"ms_total": ms, "ms_local": ms_local, "stage_ms": {k: v / steps for k, v in stage_sum.items()}, "launches": launches,
+        res = {"ms_total": ms, "ms_local": ms_local, "stage_ms": {k: v / steps for k, v in stage_sum.items()},
+               "launches": launches, "search": search,
                "pairs": pairs, "clocks": clk, "snap": snap, "energy": energy, "ttot": sim.scalars()["ttot"]}
         if with_e2e:
             # per step: host->device copy of the whole particle state from pinned memory, the step, and the
@@ -414,6 +417,9 @@ def run_ours(args, ws, rank, local):
         "gpu_launches": main_leg["launches"],
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "neighbor_pairs_per_step": main_leg["pairs"],
+        "neighbor_search": dict(main_leg["search"], note=(
+            "timed steps: tree searches of every group, skin-row builds, steps served by the exact refilter of the "
+            "skin rows, groups deferred to the tree search; the lists are the tree search's either way")),
         "roofline": roofline,
         "roofline_step": {"t_roof_ms": round(t_roof, 4), "t_measured_ms": round(ms_step, 4),
                           "frac": t_roof / ms_step, "hbm_peak_gbs": hbm, "fma_peak_tflops": peak.value,

@@ -63,6 +63,9 @@ typedef struct
     uint32_t bucket_focus;  /* max particles per leaf of the neighbour-search tree (64)    */
     int av_clean;           /* 1: AV cleaning in MomentumEnergy (HydroVeProp<avClean = true>,
                                momentum_energy_kern.hpp:43-63,165-169); 0 (default): off   */
+    double nb_skin;         /* relative skin of the reused candidate lists (0.05); 0: search the
+                               tree every step. The lists are the same either way: every
+                               step keeps exactly the j with |x_i - x_j| < 2 h_i.           */
 } sphb_params;
 
 /*! Fill p with the reference defaults listed above (precision = SPHB_FP64). */
@@ -189,6 +192,12 @@ int sphb_sim_stage_times(sphb_sim* sim, float* out);
 
 /*! Number of kernels this library has launched in this process (for launch accounting). */
 uint64_t sphb_sim_kernel_launches(const sphb_sim* sim);
+
+/*! How the neighbour stage ran since creation: out[0] tree searches of every group, out[1] skin-row builds (each
+ *  also counted in out[0]), out[2] steps served by refiltering the skin rows, out[3] groups those steps deferred to
+ *  the tree search, out[4] domain syncs whose sort moved particles while rows were kept. No counterpart in the reference, which searches the tree every step
+ *  (sph/include/sph/find_neighbors.hpp:10-41); the lists are the same either way. */
+int sphb_sim_search_stats(const sphb_sim* sim, uint64_t* out);
 
 /*! The CUDA stream (a cudaStream_t) on which the simulation issues all its work. */
 void* sphb_sim_stream(sphb_sim* sim);

@@ -107,21 +107,24 @@ __device__ inline double4 ldPos(const double4* p)
     return make_double4(lo.x, lo.y, hi.x, hi.y);
 }
 
-//! d folded to the nearest periodic image: d - L * rint(d / L), rounded like the reference's uncontracted CPU code
-__device__ inline double minImage(double d, double len, double ilen, int periodic)
+//! what one launch of the search computes
+enum SearchKind : int
 {
-    if (!periodic) { return d; }
-    return __dsub_rn(d, __dmul_rn(len, rint(__dmul_rn(d, ilen))));
-}
+    kSearchAll,    // neighbour lists of every group, with the smoothing-length iteration
+    kSearchListed, // the same for the groups of a device-side list
+    kSearchSkin    // skin lists: every j within 2 h (1 + skin), no iteration, h read only
+};
 
-//! smoothing-length update h * 0.5 * (1 + 1023 ng0 / nc)^(1/10) (sph/include/sph/kernels.hpp:27-33)
-__device__ inline double updateH(unsigned ng0, unsigned nc, double h)
+//! launch inputs of the listed and skin searches
+struct SearchExtras
 {
-    double ratio = __ddiv_rn(__dmul_rn(1023.0, double(ng0)), double(nc));
-    return __dmul_rn(__dmul_rn(h, 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
-}
+    const unsigned* groups;
+    const unsigned* numListed;
+    SkinLists sl;
+    double onePlusSkin;
+};
 
-template<bool kBatched>
+template<bool kBatched, int kKind>
 __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const double* __restrict__ x,
                                                                   const double* __restrict__ y,
                                                                   const double* __restrict__ z,
@@ -130,14 +133,23 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                                                                   uint32_t* __restrict__ nidx,
                                                                   unsigned* __restrict__ ncOut, unsigned* status,
                                                                   const TreeView* __restrict__ views,
-                                                                  const uint8_t* __restrict__ inst)
+                                                                  const uint8_t* __restrict__ inst, SearchExtras ex)
 {
     __shared__ NbShared sh;
     const int warp         = threadIdx.x / kWarp;
     const int lane         = threadIdx.x & (kWarp - 1);
     const size_t numGroups = (n + kWarp - 1) / kWarp;
-    const size_t group     = size_t(blockIdx.x) * kNbWarps + warp;
+    size_t group           = size_t(blockIdx.x) * kNbWarps + warp;
+    if constexpr (kKind == kSearchListed)
+    {
+        if (group >= *ex.numListed) { return; }
+        group = ex.groups[group];
+    }
     if (group >= numGroups) { return; }
+    constexpr bool kSkin = kKind == kSearchSkin;
+    // the lists written: neighbour lists (ngmax entries) or skin rows (cap entries)
+    uint32_t* const outList  = kSkin ? ex.sl.rows : nidx;
+    const unsigned listCap   = kSkin ? ex.sl.cap : prm.ngmax;
 
     const size_t i = group * kWarp + lane;
     // an ensemble: the group's instance (its first slot is never padding) selects the tree; padding slots idle
@@ -150,7 +162,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
     double hi        = valid ? h[i] : 0.0;
 
     const unsigned ngmin = prm.ng0 / 4;
-    const unsigned ngPad = paddedNgmax(prm.ngmax);
+    const unsigned ngPad = kSkin ? ex.sl.cap : paddedNgmax(prm.ngmax);
     bool active          = valid;
     int updates          = 0;
     unsigned count       = 0;
@@ -165,8 +177,8 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
 
     while (__ballot_sync(0xffffffffu, active) != 0u && !overflow)
     {
-        const double radiusSq = __dmul_rn(__dmul_rn(4.0, hi), hi);
-        const double r        = 2.0 * hi;
+        const double radiusSq = searchRadiusSq(hi);
+        const double r        = kSkin ? __dmul_rn(2.0 * hi, ex.onePlusSkin) : 2.0 * hi;
         double blo[3], bhi[3];
         blo[0] = warpMin(active ? xi - r : INFINITY);
         blo[1] = warpMin(active ? yi - r : INFINITY);
@@ -221,7 +233,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         // this lane's chunk buffer and its store to the chunked list layout (nidxAt)
         uint32_t* chunk = sh.nbuf[warp][lane];
         auto storeChunk = [&](unsigned c) {
-            uint32_t* dst    = nidx + nidxAt(group, ngPad, c * kNbChunk, lane);
+            uint32_t* dst    = outList + nidxAt(group, ngPad, c * kNbChunk, lane);
             const uint4* src = reinterpret_cast<const uint4*>(chunk);
             uint4 a = src[0], b = src[1];
             // one 256-bit streaming store of the whole sector (the lists are next read once per J-loop)
@@ -259,19 +271,24 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 // difference itself (padding sits at the end of the last chunk)
                 maybe = numReal >= kWarp ? 0xffffffffu : ((1u << numReal) - 1u);
             }
-            // candidates too close to the search radius for FP32: the exact test of the reference (rare)
-            unsigned band = maybe & ~sure;
-            while (band)
+            if constexpr (kSkin)
             {
-                int k = __ffs(band) - 1;
-                band &= band - 1u;
-                int j = sh.cj[warp][k];
-                double4 pj = ldPos(pos + j);
-                double ex  = minImage(pj.x - xi, box.len[0], box.ilen[0], box.periodic[0]);
-                double ey  = minImage(pj.y - yi, box.len[1], box.ilen[1], box.periodic[1]);
-                double ez  = minImage(pj.z - zi, box.len[2], box.ilen[2], box.periodic[2]);
-                double d2  = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
-                if (d2 < radiusSq) { sure |= 1u << k; }
+                // a skin row keeps the whole uncertainty band: it must contain every j within R, a few more do no
+                // harm (the refilter tests each entry exactly)
+                sure = maybe;
+            }
+            else
+            {
+                // candidates too close to the search radius for FP32: the exact test of the reference (rare)
+                unsigned band = maybe & ~sure;
+                while (band)
+                {
+                    int k = __ffs(band) - 1;
+                    band &= band - 1u;
+                    int j      = sh.cj[warp][k];
+                    double4 pj = ldPos(pos + j);
+                    if (exactDistSq(pj.x, pj.y, pj.z, xi, yi, zi, box) < radiusSq) { sure |= 1u << k; }
+                }
             }
             // append the neighbours in candidate (= index) order
             while (sure)
@@ -280,7 +297,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 sure &= sure - 1u;
                 int j = sh.cj[warp][k];
                 if (size_t(j) == i) { continue; }
-                if (count < prm.ngmax)
+                if (count < listCap)
                 {
                     chunk[count % kNbChunk] = uint32_t(j);
                     if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
@@ -455,9 +472,10 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         if (overflow) { break; }
         if (numLeaves > 0) { flush(); }
         // the last, partly filled chunk of the list (entries past the count are never read)
-        if (active && count % kNbChunk != 0 && count < prm.ngmax) { storeChunk(count / kNbChunk); }
+        if (active && count % kNbChunk != 0 && count < listCap) { storeChunk(count / kNbChunk); }
 
-        // smoothing-length iteration
+        // smoothing-length iteration (skin rows: one pass at the given h)
+        if (kSkin) { active = false; }
         if (active)
         {
             unsigned ncSph = count + 1;
@@ -478,8 +496,16 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
     }
     if (valid)
     {
-        ncOut[i] = count + 1;
-        h[i]     = hi;
+        if constexpr (kSkin)
+        {
+            ex.sl.count[i]  = count;
+            ex.sl.radius[i] = __dmul_rn(2.0 * hi, ex.onePlusSkin);
+        }
+        else
+        {
+            ncOut[i] = count + 1;
+            h[i]     = hi;
+        }
     }
 }
 
@@ -527,16 +553,54 @@ int findNeighbors(const double* x, const double* y, const double* z, const doubl
     if ((views == nullptr) != (inst == nullptr)) { return kErrArg; }
     size_t numGroups = (n + kWarp - 1) / kWarp;
     unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
+    SearchExtras ex{};
     if (views)
     {
-        findNeighborsKernel<true><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm, nidx, nc, status,
-                                                                     views, inst);
+        findNeighborsKernel<true, kSearchAll><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm,
+                                                                                 nidx, nc, status, views, inst, ex);
     }
     else
     {
-        findNeighborsKernel<false><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm, nidx, nc, status,
-                                                                      nullptr, nullptr);
+        findNeighborsKernel<false, kSearchAll><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm,
+                                                                                  nidx, nc, status, nullptr, nullptr, ex);
     }
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int findNeighborsListed(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
+                        const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
+                        unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream)
+{
+    if (n == 0) { return kOk; }
+    if (!groups || !numListed) { return kErrArg; }
+    size_t numGroups = (n + kWarp - 1) / kWarp;
+    unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
+    SearchExtras ex{};
+    ex.groups    = groups;
+    ex.numListed = numListed;
+    findNeighborsKernel<false, kSearchListed><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm,
+                                                                                 nidx, nc, status, nullptr, nullptr, ex);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int buildSkinLists(const double* x, const double* y, const double* z, const double4* pos, const double* h, size_t n,
+                   const TreeView& tree, const DevBox& box, NeighborParams prm, double skin, SkinLists sl,
+                   unsigned* status, cudaStream_t stream)
+{
+    if (n == 0) { return kOk; }
+    if (!(skin > 0.0) || sl.cap == 0 || sl.cap % kNbChunk != 0) { return kErrArg; }
+    size_t numGroups = (n + kWarp - 1) / kWarp;
+    unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
+    SearchExtras ex{};
+    ex.sl          = sl;
+    ex.onePlusSkin = 1.0 + skin;
+    // the kernel writes h only in the iterating kinds, never in this one
+    findNeighborsKernel<false, kSearchSkin><<<blocks, kNbThreads, 0, stream>>>(
+        x, y, z, pos, const_cast<double*>(h), n, tree, box, prm, nullptr, nullptr, status, nullptr, nullptr, ex);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

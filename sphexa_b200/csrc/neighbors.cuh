@@ -48,6 +48,46 @@ struct NeighborParams
     int maxIterations; // smoothing-length updates (10 in the reference, sph/include/sph/find_neighbors.hpp:19)
 };
 
+//! d folded to the nearest periodic image: d - L * rint(d / L), rounded like the reference's uncontracted CPU code
+__device__ inline double minImage(double d, double len, double ilen, int periodic)
+{
+    if (!periodic) { return d; }
+    return __dsub_rn(d, __dmul_rn(len, rint(__dmul_rn(d, ilen))));
+}
+
+//! smoothing-length update h * 0.5 * (1 + 1023 ng0 / nc)^(1/10) (sph/include/sph/kernels.hpp:27-33)
+__device__ inline double updateH(unsigned ng0, unsigned nc, double h)
+{
+    double ratio = __ddiv_rn(__dmul_rn(1023.0, double(ng0)), double(nc));
+    return __dmul_rn(__dmul_rn(h, 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
+}
+
+//! the exact pair test of the reference (cstone/findneighbors.hpp:33-51): minimum-image squared distance, summed in
+//! the reference's order without contraction
+__device__ inline double exactDistSq(double xj, double yj, double zj, double xi, double yi, double zi,
+                                     const DevBox& box)
+{
+    double ex = minImage(xj - xi, box.len[0], box.ilen[0], box.periodic[0]);
+    double ey = minImage(yj - yi, box.len[1], box.ilen[1], box.periodic[1]);
+    double ez = minImage(zj - zi, box.len[2], box.ilen[2], box.periodic[2]);
+    return __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+}
+
+//! the reference's squared search radius (2h)^2 = 4 h h
+__device__ inline double searchRadiusSq(double h) { return __dmul_rn(__dmul_rn(4.0, h), h); }
+
+/*! Candidate lists kept across steps ("skin" lists): for every particle, each j whose distance was below
+ *  R_i = 2 h_i (1 + skin) when the lists were built, in ascending index order, at most `cap` of them (chunked like
+ *  the neighbour lists, with `cap` as the padded width). count[i] is the number found, which can exceed cap: the row
+ *  is then incomplete and never used. */
+struct SkinLists
+{
+    uint32_t* rows;
+    unsigned* count;
+    double* radius;
+    unsigned cap;
+};
+
 /*! Search all particles (x, y, z and the same coordinates packed as pos = (x, y, z, m)): updates h where the count left [ng0/4, ngmax+1], writes nc (count incl. self) and lists.
  *  status[0] is set to a non-zero value if a per-warp buffer overflowed (the search then returns SPHB_ERR_CAPACITY).
  *  An ensemble passes views (one tree per instance, on the device) and inst (instance per slot, kGhost for
@@ -56,5 +96,63 @@ int findNeighbors(const double* x, const double* y, const double* z, const doubl
                   const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
                   unsigned* status, cudaStream_t stream, const TreeView* views = nullptr,
                   const uint8_t* inst = nullptr);
+
+/*! The same search for the groups listed in groups[0 .. *numListed) only (a device count: the launch covers every
+ *  group and the warps past the count return at once). */
+int findNeighborsListed(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
+                        const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
+                        unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream);
+
+/*! Build the skin lists at the current positions and smoothing lengths: R_i = 2 h_i (1 + skin). The rows hold every
+ *  j within R_i (and possibly a few just outside it: the FP32 test keeps its whole uncertainty band). h is read only. */
+int buildSkinLists(const double* x, const double* y, const double* z, const double4* pos, const double* h, size_t n,
+                   const TreeView& tree, const DevBox& box, NeighborParams prm, double skin, SkinLists sl,
+                   unsigned* status, cudaStream_t stream);
+
+//! inputs of the per-step refilter of the skin lists (skin.cu)
+struct SkinFilterArgs
+{
+    const double4* pos; // current packed positions (x, y, z, m)
+    const int4* posq;   // fixed-point positions (mixed precision), or null: every candidate is tested in FP64
+    float qscale[3];    // fixed-point unit per axis as FP32
+    float qunit;        // the largest fixed-point unit (sets the width of the FP32 uncertainty band)
+    double* h;
+    unsigned* nc;
+    uint32_t* nidx;
+    SkinLists sl;
+    const double* xb; // positions at the build, by build index
+    const double* yb;
+    const double* zb;
+    const uint32_t* moved;   // bit i: index i holds another particle than at the build (null: none moved)
+    const unsigned* dispGrid; // per cell of a kSkinGrid^3 grid over the box: largest displacement (FP32 bits)
+    unsigned* worklist;       // groups the filter cannot serve, for findNeighborsListed
+    unsigned* numWorklist;
+    size_t n;
+    DevBox box;
+    NeighborParams prm;
+};
+
+//! cells per axis of the displacement grid
+constexpr int kSkinGrid = 32;
+
+/*! Largest displacement since the build per cell of the grid (cells by current position). buildOf maps the current
+ *  index to the build index (null: the identity). dispGrid must be zero on entry. */
+int skinDisplacement(const double4* pos, const double* xb, const double* yb, const double* zb,
+                     const uint32_t* buildOf, size_t n, const DevBox& box, unsigned* dispGrid, cudaStream_t stream);
+
+/*! After a sort that moved particles: buildNew[i] = buildOld[order[i]] (buildOld null: the identity) and bit i of
+ *  moved = (buildNew[i] != i). */
+int skinRemap(const uint32_t* order, const uint32_t* buildOld, uint32_t* buildNew, uint32_t* moved, size_t n,
+              cudaStream_t stream);
+
+//! *flag = 1 if a[i] != b[i] for some i < n, else 0 (device flag)
+int idsDiffer(const uint64_t* a, const uint64_t* b, size_t n, unsigned* flag, cudaStream_t stream);
+
+/*! Neighbour lists, counts and the smoothing-length iteration from the skin lists. A group is served only when its
+ *  rows are provably complete for the current positions and every h of its iteration:
+ *  2 h_i + |displacement of i| + (largest displacement of any particle near the group) <= R_i,
+ *  and no particle of the group or of its rows changed index since the build. The other groups are appended to the
+ *  worklist, untouched (h, nc unchanged), for the tree search. The results are those of findNeighbors. */
+int filterSkinLists(const SkinFilterArgs& a, cudaStream_t stream);
 
 } // namespace sphb

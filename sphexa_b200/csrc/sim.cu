@@ -1,5 +1,6 @@
 // The simulation object: particle dataset in HBM and the whole HydroVeProp step
 // (main/src/propagator/ve_hydro.hpp:126-220) at one rank, driven from the host.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -103,6 +104,23 @@ struct sphb_sim
     DeviceBuffer<char> tapeSlots;
     size_t tapeSlotBytes{0};
     int numTapeSlots{0};
+
+    // skin lists (neighbors.cuh): candidate rows kept across steps and refiltered exactly every step
+    DeviceBuffer<uint32_t> skinRows;
+    DeviceBuffer<unsigned> skinCount;
+    DeviceBuffer<double> skinRadius, skinXb, skinYb, skinZb;
+    DeviceBuffer<uint32_t> skinBuild, skinBuildAlt, skinMoved;
+    DeviceBuffer<unsigned> skinGrid;
+    DeviceBuffer<unsigned> skinWork; // [0]: number of deferred groups, then the groups
+    unsigned skinCap{0};
+    bool skinValid{false};    // rows match the particles' current indices (up to the tracked permutation)
+    bool skinAnyMoved{false}; // some index holds another particle than at the build (skinBuild, skinMoved valid)
+    bool skinFiltered{false}; // this step's lists came from the rows
+    int skinAge{0};           // steps since the build
+    int skinHoldoff{0};       // steps left of plain tree searches after rows proved short-lived
+    unsigned skinDeferredLast{0};
+    // tree searches of every group, row builds, refiltered steps, deferred groups, syncs that remapped the rows
+    uint64_t searchStats[5]{};
 
     cudaEvent_t ev[kNumStages + 1]{};
     float stageMs[kNumStages]{};
@@ -239,6 +257,15 @@ int syncDomain(sphb_sim& s)
     bool identity = false;
     SPHB_TRY(sortNearlySorted(s.keys.data(), s.order.data(), s.n, s.sortScratch.data(), s.sortScratch.capacity(),
                               &identity, st));
+    if (s.skinValid && !identity)
+    {
+        // the skin rows hold build indices: track which particle now sits at each index
+        SPHB_TRY(skinRemap(s.order.data(), s.skinAnyMoved ? s.skinBuild.data() : nullptr, s.skinBuildAlt.data(),
+                           s.skinMoved.data(), s.n, st));
+        s.skinBuild.swap(s.skinBuildAlt);
+        s.skinAnyMoved = true;
+        ++s.searchStats[4];
+    }
     SPHB_TRY(updateGlobalTree(s.gtree, s.keys.data(), s.n, s.ts, st));
 
     if (!identity)
@@ -408,6 +435,134 @@ int runChain(sphb_sim& s)
     return kOk;
 }
 
+TreeView treeView(sphb_sim& s)
+{
+    TreeView tv;
+    tv.childOffsets = s.ftree.tree.childOffsets.data();
+    tv.nodeToLeaf   = s.ftree.tree.nodeToLeaf.data();
+    tv.centers      = s.ftree.tree.centers.data();
+    tv.sizes        = s.ftree.tree.sizes.data();
+    tv.layout       = s.ftree.layout.data();
+    tv.blockLo      = s.blockLo.data();
+    tv.blockHi      = s.blockHi.data();
+    tv.numNodes     = s.ftree.tree.numNodes;
+    return tv;
+}
+
+int allocateSkin(sphb_sim& s)
+{
+    if (s.skinRows.data()) { return kOk; }
+    double grow = (1.0 + s.p.nb_skin) * (1.0 + s.p.nb_skin) * (1.0 + s.p.nb_skin);
+    s.skinCap   = paddedNgmax(unsigned(std::ceil(s.p.ngmax * grow * 1.1)));
+    size_t n = s.n;
+    SPHB_TRY(s.skinRows.reserve(s.numGroups() * size_t(s.skinCap) * kWarp));
+    SPHB_TRY(s.skinCount.reserve(n));
+    SPHB_TRY(s.skinRadius.reserve(n));
+    SPHB_TRY(s.skinXb.reserve(n));
+    SPHB_TRY(s.skinYb.reserve(n));
+    SPHB_TRY(s.skinZb.reserve(n));
+    SPHB_TRY(s.skinBuild.reserve(n));
+    SPHB_TRY(s.skinBuildAlt.reserve(n));
+    SPHB_TRY(s.skinMoved.reserve(s.numGroups()));
+    SPHB_TRY(s.skinGrid.reserve(size_t(kSkinGrid) * kSkinGrid * kSkinGrid));
+    SPHB_TRY(s.skinWork.reserve(s.numGroups() + 1));
+    return kOk;
+}
+
+/*! The neighbour stage: the tree search of every group (sph/include/sph/find_neighbors.hpp:10-41), or the exact
+ *  refilter of the skin rows plus the tree search of the groups the rows cannot serve. Rows are rebuilt when more
+ *  than a tenth of the groups were deferred in the previous step; rows that needed a rebuild within three steps
+ *  (particles moving fast everywhere) are dropped for 32 steps of plain tree searches. Every path gives the same
+ *  lists, counts and smoothing lengths. */
+int searchNeighbors(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    TreeView tv     = treeView(s);
+    NeighborParams np{s.p.ng0, s.p.ngmax, 10};
+    s.skinFiltered = false;
+    auto treeSearch = [&]() {
+        ++s.searchStats[0];
+        return findNeighbors(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
+                             s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), st);
+    };
+
+    bool useSkin = s.p.nb_skin > 0.0 && !s.taping;
+    if (!useSkin || s.skinHoldoff > 0)
+    {
+        if (s.skinHoldoff > 0) { --s.skinHoldoff; }
+        s.skinValid = false;
+        return treeSearch();
+    }
+    bool rebuild = !s.skinValid;
+    if (!rebuild && size_t(s.skinDeferredLast) * 10 > s.numGroups())
+    {
+        if (s.skinAge <= 3)
+        {
+            s.skinHoldoff = 32;
+            s.skinValid   = false;
+            return treeSearch();
+        }
+        rebuild = true;
+    }
+    if (rebuild)
+    {
+        SPHB_TRY(allocateSkin(s));
+        SPHB_TRY(treeSearch());
+        SkinLists sl{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap};
+        SPHB_TRY(buildSkinLists(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
+                                s.box, np, s.p.nb_skin, sl, s.status.data(), st));
+        size_t bytes = s.n * sizeof(double);
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.skinXb.data(), s.f[fX].data(), bytes, cudaMemcpyDeviceToDevice, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.skinYb.data(), s.f[fY].data(), bytes, cudaMemcpyDeviceToDevice, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.skinZb.data(), s.f[fZ].data(), bytes, cudaMemcpyDeviceToDevice, st));
+        s.skinValid        = true;
+        s.skinAnyMoved     = false;
+        s.skinAge          = 0;
+        s.skinDeferredLast = 0;
+        ++s.searchStats[1];
+        return kOk;
+    }
+
+    ++s.skinAge;
+    ++s.searchStats[2];
+    s.skinFiltered = true;
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.skinGrid.data(), 0, size_t(kSkinGrid) * kSkinGrid * kSkinGrid * sizeof(unsigned),
+                                  st));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.skinWork.data(), 0, sizeof(unsigned), st));
+    const uint32_t* buildOf = s.skinAnyMoved ? s.skinBuild.data() : nullptr;
+    SPHB_TRY(skinDisplacement(s.pos.data(), s.skinXb.data(), s.skinYb.data(), s.skinZb.data(), buildOf, s.n, s.box,
+                              s.skinGrid.data(), st));
+    SkinFilterArgs a{};
+    a.pos  = s.pos.data();
+    a.posq = s.mixed ? s.posq.data() : nullptr;
+    FixedFrame fr = fixedFrameOf(s.box);
+    double unitMax = 0;
+    for (int k = 0; k < 3; ++k)
+    {
+        a.qscale[k] = float(fr.unit[k]);
+        unitMax     = std::max(unitMax, fr.unit[k]);
+    }
+    a.qunit       = float(unitMax * (1.0 + 1e-6));
+    a.h           = s.f[fH].data();
+    a.nc          = s.nc.data();
+    a.nidx        = s.nidx.data();
+    a.sl          = SkinLists{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap};
+    a.xb          = s.skinXb.data();
+    a.yb          = s.skinYb.data();
+    a.zb          = s.skinZb.data();
+    a.moved       = s.skinAnyMoved ? s.skinMoved.data() : nullptr;
+    a.dispGrid    = s.skinGrid.data();
+    a.worklist    = s.skinWork.data() + 1;
+    a.numWorklist = s.skinWork.data();
+    a.n           = s.n;
+    a.box         = s.box;
+    a.prm         = np;
+    SPHB_TRY(filterSkinLists(a, st));
+    return findNeighborsListed(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
+                               s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), s.skinWork.data() + 1,
+                               s.skinWork.data(), st);
+}
+
 int computeForces(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
@@ -424,18 +579,7 @@ int computeForces(sphb_sim& s)
     SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
 
-    TreeView tv;
-    tv.childOffsets = s.ftree.tree.childOffsets.data();
-    tv.nodeToLeaf   = s.ftree.tree.nodeToLeaf.data();
-    tv.centers      = s.ftree.tree.centers.data();
-    tv.sizes        = s.ftree.tree.sizes.data();
-    tv.layout       = s.ftree.layout.data();
-    tv.blockLo      = s.blockLo.data();
-    tv.blockHi      = s.blockHi.data();
-    tv.numNodes     = s.ftree.tree.numNodes;
-    NeighborParams np{s.p.ng0, s.p.ngmax, 10};
-    SPHB_TRY(findNeighbors(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
-                           s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), st));
+    SPHB_TRY(searchNeighbors(s));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
 
     if (s.mixed) { SPHB_TRY(runChain<float>(s)); }
@@ -452,8 +596,15 @@ int computeForces(sphb_sim& s)
     SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(red, s.reduce.data(), sizeof(red), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    unsigned deferred = 0;
+    if (s.skinFiltered)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(&deferred, s.skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    }
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIntegrate], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    s.skinDeferredLast = deferred;
+    s.searchStats[3] += deferred;
     if (status) { return kErrCapacity; }
 
     double maxDivv = fromOrderedBits(red[0]);
@@ -652,6 +803,7 @@ extern "C" void sphb_default_params(sphb_params* p)
     p->precision      = SPHB_FP64;
     p->bucket_focus   = 64;
     p->av_clean       = 0;
+    p->nb_skin        = 0.05;
 }
 
 extern "C" const char* sphb_version(void) { return "sphb200 0.1 (sm_100a)"; }
@@ -661,6 +813,7 @@ extern "C" int sphb_sim_create(sphb_sim** out, size_t n, const sphb_box* box, co
     if (!out || !box || !params || n == 0 || n >= (size_t(1) << 30)) { return SPHB_ERR_ARG; }
     if (params->ng0 > params->ngmax || params->ngmax == 0 || params->bucket_focus == 0) { return SPHB_ERR_ARG; }
     if (params->precision != SPHB_FP64 && params->precision != SPHB_MIXED) { return SPHB_ERR_ARG; }
+    if (!(params->nb_skin >= 0.0 && params->nb_skin <= 1.0)) { return SPHB_ERR_ARG; }
     for (int k = 0; k < 3; ++k)
     {
         if (!(box->hi[k] > box->lo[k])) { return SPHB_ERR_ARG; }
@@ -713,6 +866,7 @@ extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const u
     SPHB_TRY(initFocusTree(s->ftree, s->p.bucket_focus, s->ts, s->stream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->boxFirstCall = true;
+    s->skinValid    = false;
     s->minDt        = s->p.minDt;
     s->minDt_m1     = s->p.minDt_m1;
     s->ttot         = 0;
@@ -726,6 +880,7 @@ extern "C" int sphb_sim_initial_sync(sphb_sim* s)
 {
     if (!s) { return SPHB_ERR_ARG; }
     if (!s->uploaded) { return SPHB_ERR_STATE; }
+    s->skinValid = false;
     SPHB_TRY(syncDomain(*s));
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SPHB_OK;
@@ -854,6 +1009,7 @@ extern "C" int sphb_sim_set_field(sphb_sim* s, const char* name, const double* i
     void* ptr = nullptr;
     int kind  = 0;
     if (!findField(s, name, &ptr, &kind)) { return SPHB_ERR_ARG; }
+    s->skinValid = false;
     size_t n = s->n;
     std::vector<double> src(n);
     SPHB_CUDA_TRY(cudaMemcpy(src.data(), in, n * sizeof(double),
@@ -944,6 +1100,13 @@ extern "C" int sphb_sim_stage_times(sphb_sim* s, float* out)
 
 extern "C" uint64_t sphb_sim_kernel_launches(const sphb_sim*) { return launchCounter(); }
 
+extern "C" int sphb_sim_search_stats(const sphb_sim* s, uint64_t* out)
+{
+    if (!s || !out) { return SPHB_ERR_ARG; }
+    std::memcpy(out, s->searchStats, sizeof(s->searchStats));
+    return SPHB_OK;
+}
+
 extern "C" void* sphb_sim_stream(sphb_sim* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
 
 extern "C" int sphb_sim_load_state(sphb_sim* s, const double* const* fields, const uint64_t* id, int on_device)
@@ -956,7 +1119,20 @@ extern "C" int sphb_sim_load_state(sphb_sim* s, const double* const* fields, con
         if (!fields[k]) { return SPHB_ERR_ARG; }
         SPHB_CUDA_TRY(cudaMemcpyAsync(s->f[k].data(), fields[k], s->n * sizeof(double), kind, s->stream));
     }
-    SPHB_CUDA_TRY(cudaMemcpyAsync(s->id.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
+    if (!s->skinValid)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s->id.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
+        return SPHB_OK;
+    }
+    // the skin rows stay usable when every index holds the same particle as before (positions and h may differ
+    // arbitrarily: the next refilter checks them against the build)
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s->idAlt.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
+    SPHB_TRY(idsDiffer(s->id.data(), s->idAlt.data(), s->n, s->skinWork.data(), s->stream));
+    unsigned differ = 1;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&differ, s->skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    s->id.swap(s->idAlt);
+    if (differ) { s->skinValid = false; }
     return SPHB_OK;
 }
 
@@ -995,7 +1171,9 @@ extern "C" int sphb_sim_set_params(sphb_sim* s, const sphb_params* p)
     {
         return SPHB_ERR_ARG;
     }
+    if (!(p->nb_skin >= 0.0) || (s->skinRows.data() && p->nb_skin != s->p.nb_skin)) { return SPHB_ERR_ARG; }
     double minDt = s->p.minDt, minDtM1 = s->p.minDt_m1;
+    s->skinValid  = false;
     s->p          = *p;
     s->p.minDt    = minDt;
     s->p.minDt_m1 = minDtM1;
@@ -1012,6 +1190,7 @@ extern "C" int sphb_sim_step_vjp(sphb_sim* s, const double* const* adj_post, dou
     }
     if (!s->uploaded || !(s->fixedDt > 0) || s->p.av_clean) { return SPHB_ERR_STATE; }
     if (!s->hPre.data()) { SPHB_TRY(allocateAdjoint(*s)); }
+    s->skinValid = false;
     // the chain arrays of the recomputed step and of its adjoint both carry the tape pointers
     s->taping = true;
     int rc    = computeForces(*s);
@@ -1061,6 +1240,7 @@ extern "C" int sphb_sim_step_vjp_recorded(sphb_sim* s, int slot, const double* c
         if (!adj_post[f] || !adj_pre[f] || adj_post[f] == adj_pre[f]) { return SPHB_ERR_ARG; }
     }
     if (!s->uploaded || !(s->fixedDt > 0) || slot >= s->numTapeSlots) { return SPHB_ERR_STATE; }
+    s->skinValid = false;
     SPHB_TRY(copyTape(*s, slot, false));
     s->taping = true;
     int rc = s->mixed ? runStepVjp<float>(*s, adj_post, adj_pre, alphamax_bar)

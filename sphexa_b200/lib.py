@@ -35,7 +35,7 @@ class Params(C.Structure):
                 ("Kcour", C.c_double), ("Krho", C.c_double), ("alphamin", C.c_double), ("alphamax", C.c_double),
                 ("decay_constant", C.c_double), ("sinc_index", C.c_double), ("minDt", C.c_double),
                 ("minDt_m1", C.c_double), ("precision", C.c_int), ("bucket_focus", C.c_uint32),
-                ("av_clean", C.c_int)]
+                ("av_clean", C.c_int), ("nb_skin", C.c_double)]
 
 
 #: every extern "C" symbol of include/sphb200.h
@@ -44,6 +44,7 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sim_upload", "sphb_sim_initial_sync", "sphb_sim_compute_forces", "sphb_sim_integrate",
             "sphb_sim_step", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
             "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches",
+            "sphb_sim_search_stats",
             "sphb_sim_stream", "sphb_sim_load_state", "sphb_sim_store_state", "sphb_probe_fma_peak",
             "sphb_sort_by_key_static", "sphb_sort_by_key_static_max", "sphb_sim_set_fixed_dt",
             "sphb_sim_set_params", "sphb_sim_step_vjp", "sphb_sort_by_key_nearly_sorted", "sphb_sim_tape_reserve", "sphb_sim_step_record",
@@ -86,6 +87,7 @@ def load() -> C.CDLL:
         "sphb_sim_neighbors": (C.c_int, [P, P]),
         "sphb_sim_stage_times": (C.c_int, [P, P]),
         "sphb_sim_kernel_launches": (C.c_uint64, [P]),
+        "sphb_sim_search_stats": (C.c_int, [P, P]),
         "sphb_sim_stream": (C.c_void_p, [P]),
         "sphb_sim_load_state": (C.c_int, [P, P, P, C.c_int]),
         "sphb_sim_store_state": (C.c_int, [P, P, P, C.c_int]),
@@ -160,4 +162,6 @@ def make_params(p: dict, precision: int = SPHB_FP64, bucket: int = 64) -> Params
     prm.precision = int(precision)
     prm.bucket_focus = int(bucket)
     prm.av_clean = int(bool(p.get("avClean", False)))
+    if "nbSkin" in p:
+        prm.nb_skin = float(p["nbSkin"])
     return prm

@@ -109,6 +109,14 @@ class Simulation:
         L.check(self.lib.sphb_sim_stage_times(self.h, L.ptr(out)), "stage_times")
         return dict(zip(STAGE_NAMES, out.tolist()))
 
+    def search_stats(self) -> dict:
+        """How the neighbour stage ran: tree searches of every group, skin-row builds, steps served from the skin
+        rows, groups those steps deferred to the tree search, and syncs that moved particles while rows were kept."""
+        out = np.zeros(5, dtype=np.uint64)
+        L.check(self.lib.sphb_sim_search_stats(self.h, L.ptr(out)), "search_stats")
+        return dict(zip(("tree_searches", "skin_builds", "skin_steps", "deferred_groups", "remapped_syncs"),
+                        (int(v) for v in out)))
+
     def kernel_launches(self) -> int:
         return int(self.lib.sphb_sim_kernel_launches(self.h))
 
