@@ -41,8 +41,9 @@ struct NbShared
     alignas(16) float cy[kNbWarps][kWarp];
     alignas(16) float cz[kNbWarps][kWarp];
     int cj[kNbWarps][kWarp];
-    // per lane: the neighbours of the list chunk being filled, written out as one 32-byte sector when full
-    alignas(16) uint32_t nbuf[kNbWarps][kWarp][kNbChunk];
+    // per lane: the neighbours of the list chunk being filled, written out as one 32-byte sector when full; lane
+    // minor, so that the lanes' appends fall into distinct banks
+    uint32_t nbuf[kNbWarps][kNbChunk][kWarp];
 };
 
 /*! Half width of the band |d^2 - (2h)^2| < band * (2h)^2 in which the FP32 distance cannot decide and the exact FP64
@@ -177,8 +178,9 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
 
     while (__ballot_sync(0xffffffffu, active) != 0u && !overflow)
     {
-        const double radiusSq = searchRadiusSq(hi);
         const double r        = kSkin ? __dmul_rn(2.0 * hi, ex.onePlusSkin) : 2.0 * hi;
+        // the exact test: (2h)^2 as the reference computes it, or R^2 for skin rows
+        const double radiusSq = kSkin ? __dmul_rn(r, r) : searchRadiusSq(hi);
         double blo[3], bhi[3];
         blo[0] = warpMin(active ? xi - r : INFINITY);
         blo[1] = warpMin(active ? yi - r : INFINITY);
@@ -231,14 +233,13 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         int numLeaves = 0;
 
         // this lane's chunk buffer and its store to the chunked list layout (nidxAt)
-        uint32_t* chunk = sh.nbuf[warp][lane];
+        uint32_t* chunk = &sh.nbuf[warp][0][lane];
         auto storeChunk = [&](unsigned c) {
-            uint32_t* dst    = outList + nidxAt(group, ngPad, c * kNbChunk, lane);
-            const uint4* src = reinterpret_cast<const uint4*>(chunk);
-            uint4 a = src[0], b = src[1];
+            uint32_t* dst = outList + nidxAt(group, ngPad, c * kNbChunk, lane);
             // one 256-bit streaming store of the whole sector (the lists are next read once per J-loop)
-            asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(a.x), "r"(a.y),
-                         "r"(a.z), "r"(a.w), "r"(b.x), "r"(b.y), "r"(b.z), "r"(b.w)
+            asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(chunk[0]),
+                         "r"(chunk[kWarp]), "r"(chunk[2 * kWarp]), "r"(chunk[3 * kWarp]), "r"(chunk[4 * kWarp]),
+                         "r"(chunk[5 * kWarp]), "r"(chunk[6 * kWarp]), "r"(chunk[7 * kWarp])
                          : "memory");
         };
 
@@ -271,24 +272,15 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 // difference itself (padding sits at the end of the last chunk)
                 maybe = numReal >= kWarp ? 0xffffffffu : ((1u << numReal) - 1u);
             }
-            if constexpr (kSkin)
+            // candidates too close to the search radius for FP32: the exact test of the reference (rare)
+            unsigned band = maybe & ~sure;
+            while (band)
             {
-                // a skin row keeps the whole uncertainty band: it must contain every j within R, a few more do no
-                // harm (the refilter tests each entry exactly)
-                sure = maybe;
-            }
-            else
-            {
-                // candidates too close to the search radius for FP32: the exact test of the reference (rare)
-                unsigned band = maybe & ~sure;
-                while (band)
-                {
-                    int k = __ffs(band) - 1;
-                    band &= band - 1u;
-                    int j      = sh.cj[warp][k];
-                    double4 pj = ldPos(pos + j);
-                    if (exactDistSq(pj.x, pj.y, pj.z, xi, yi, zi, box) < radiusSq) { sure |= 1u << k; }
-                }
+                int k = __ffs(band) - 1;
+                band &= band - 1u;
+                int j      = sh.cj[warp][k];
+                double4 pj = ldPos(pos + j);
+                if (exactDistSq(pj.x, pj.y, pj.z, xi, yi, zi, box) < radiusSq) { sure |= 1u << k; }
             }
             // append the neighbours in candidate (= index) order
             while (sure)
@@ -299,7 +291,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 if (size_t(j) == i) { continue; }
                 if (count < listCap)
                 {
-                    chunk[count % kNbChunk] = uint32_t(j);
+                    chunk[(count % kNbChunk) * kWarp] = uint32_t(j);
                     if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
                 }
                 ++count;
@@ -471,8 +463,12 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         }
         if (overflow) { break; }
         if (numLeaves > 0) { flush(); }
-        // the last, partly filled chunk of the list (entries past the count are never read)
-        if (active && count % kNbChunk != 0 && count < listCap) { storeChunk(count / kNbChunk); }
+        // the last, partly filled chunk of the list (entries past the count, or past the capacity, are never read)
+        if (active)
+        {
+            unsigned kept = min(count, listCap);
+            if (kept % kNbChunk != 0) { storeChunk(kept / kNbChunk); }
+        }
 
         // smoothing-length iteration (skin rows: one pass at the given h)
         if (kSkin) { active = false; }

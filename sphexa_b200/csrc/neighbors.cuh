@@ -103,8 +103,8 @@ int findNeighborsListed(const double* x, const double* y, const double* z, const
                         const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
                         unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream);
 
-/*! Build the skin lists at the current positions and smoothing lengths: R_i = 2 h_i (1 + skin). The rows hold every
- *  j within R_i (and possibly a few just outside it: the FP32 test keeps its whole uncertainty band). h is read only. */
+/*! Build the skin lists at the current positions and smoothing lengths: R_i = 2 h_i (1 + skin). Row i holds exactly
+ *  the j != i whose FP64 minimum-image squared distance is below R_i * R_i, ascending. h is read only. */
 int buildSkinLists(const double* x, const double* y, const double* z, const double4* pos, const double* h, size_t n,
                    const TreeView& tree, const DevBox& box, NeighborParams prm, double skin, SkinLists sl,
                    unsigned* status, cudaStream_t stream);
@@ -125,8 +125,11 @@ struct SkinFilterArgs
     const double* zb;
     const uint32_t* moved;   // bit i: index i holds another particle than at the build (null: none moved)
     const unsigned* dispGrid; // per cell of a kSkinGrid^3 grid over the box: largest displacement (FP32 bits)
-    unsigned* worklist;       // groups the filter cannot serve, for findNeighborsListed
+    unsigned* groupD;         // per group: the check's result (D as FP32 bits, or all ones: deferred)
+    unsigned* worklist;       // groups the check defers, for findNeighborsListed
     unsigned* numWorklist;
+    unsigned* worklist2;      // groups whose smoothing-length iteration leaves their rows
+    unsigned* numWorklist2;
     size_t n;
     DevBox box;
     NeighborParams prm;
@@ -148,11 +151,14 @@ int skinRemap(const uint32_t* order, const uint32_t* buildOld, uint32_t* buildNe
 //! *flag = 1 if a[i] != b[i] for some i < n, else 0 (device flag)
 int idsDiffer(const uint64_t* a, const uint64_t* b, size_t n, unsigned* flag, cudaStream_t stream);
 
-/*! Neighbour lists, counts and the smoothing-length iteration from the skin lists. A group is served only when its
- *  rows are provably complete for the current positions and every h of its iteration:
- *  2 h_i + |displacement of i| + (largest displacement of any particle near the group) <= R_i,
- *  and no particle of the group or of its rows changed index since the build. The other groups are appended to the
- *  worklist, untouched (h, nc unchanged), for the tree search. The results are those of findNeighbors. */
+/*! Decide per group whether the skin rows can serve it: only when they are provably complete for the current
+ *  positions and h, 2 h_i + |displacement of i| + (largest displacement of any particle near the group) <= R_i, and
+ *  no particle of the group or of its rows changed index since the build. The others go to the worklist, untouched
+ *  (h, nc unchanged), for the tree search. */
+int checkSkinGroups(const SkinFilterArgs& a, cudaStream_t stream);
+
+/*! Neighbour lists, counts and the smoothing-length iteration from the skin rows, for the groups the check kept. A
+ *  group whose new h leaves its rows goes to worklist2, untouched. The results are those of findNeighbors. */
 int filterSkinLists(const SkinFilterArgs& a, cudaStream_t stream);
 
 } // namespace sphb

@@ -111,7 +111,10 @@ struct sphb_sim
     DeviceBuffer<double> skinRadius, skinXb, skinYb, skinZb;
     DeviceBuffer<uint32_t> skinBuild, skinBuildAlt, skinMoved;
     DeviceBuffer<unsigned> skinGrid;
-    DeviceBuffer<unsigned> skinWork; // [0]: number of deferred groups, then the groups
+    DeviceBuffer<unsigned> skinWork; // [0], [1]: deferred by the check / by the iteration, then the two lists
+    DeviceBuffer<unsigned> skinGroupD;
+    cudaStream_t sideStream{nullptr}; // the tree search of deferred groups, beside the refilter
+    cudaEvent_t skinFork{nullptr}, skinJoin{nullptr};
     unsigned skinCap{0};
     bool skinValid{false};    // rows match the particles' current indices (up to the tracked permutation)
     bool skinAnyMoved{false}; // some index holds another particle than at the build (skinBuild, skinMoved valid)
@@ -465,7 +468,14 @@ int allocateSkin(sphb_sim& s)
     SPHB_TRY(s.skinBuildAlt.reserve(n));
     SPHB_TRY(s.skinMoved.reserve(s.numGroups()));
     SPHB_TRY(s.skinGrid.reserve(size_t(kSkinGrid) * kSkinGrid * kSkinGrid));
-    SPHB_TRY(s.skinWork.reserve(s.numGroups() + 1));
+    SPHB_TRY(s.skinWork.reserve(2 * s.numGroups() + 2));
+    SPHB_TRY(s.skinGroupD.reserve(s.numGroups()));
+    // highest priority, so that the few long tree searches start before the refilter fills the GPU
+    int leastPriority = 0, greatestPriority = 0;
+    SPHB_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority));
+    SPHB_CUDA_TRY(cudaStreamCreateWithPriority(&s.sideStream, cudaStreamNonBlocking, greatestPriority));
+    SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.skinFork, cudaEventDisableTiming));
+    SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.skinJoin, cudaEventDisableTiming));
     return kOk;
 }
 
@@ -528,7 +538,7 @@ int searchNeighbors(sphb_sim& s)
     s.skinFiltered = true;
     SPHB_CUDA_TRY(cudaMemsetAsync(s.skinGrid.data(), 0, size_t(kSkinGrid) * kSkinGrid * kSkinGrid * sizeof(unsigned),
                                   st));
-    SPHB_CUDA_TRY(cudaMemsetAsync(s.skinWork.data(), 0, sizeof(unsigned), st));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.skinWork.data(), 0, 2 * sizeof(unsigned), st));
     const uint32_t* buildOf = s.skinAnyMoved ? s.skinBuild.data() : nullptr;
     SPHB_TRY(skinDisplacement(s.pos.data(), s.skinXb.data(), s.skinYb.data(), s.skinZb.data(), buildOf, s.n, s.box,
                               s.skinGrid.data(), st));
@@ -542,25 +552,38 @@ int searchNeighbors(sphb_sim& s)
         a.qscale[k] = float(fr.unit[k]);
         unitMax     = std::max(unitMax, fr.unit[k]);
     }
-    a.qunit       = float(unitMax * (1.0 + 1e-6));
-    a.h           = s.f[fH].data();
-    a.nc          = s.nc.data();
-    a.nidx        = s.nidx.data();
-    a.sl          = SkinLists{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap};
-    a.xb          = s.skinXb.data();
-    a.yb          = s.skinYb.data();
-    a.zb          = s.skinZb.data();
-    a.moved       = s.skinAnyMoved ? s.skinMoved.data() : nullptr;
-    a.dispGrid    = s.skinGrid.data();
-    a.worklist    = s.skinWork.data() + 1;
-    a.numWorklist = s.skinWork.data();
-    a.n           = s.n;
-    a.box         = s.box;
-    a.prm         = np;
+    a.qunit        = float(unitMax * (1.0 + 1e-6));
+    a.h            = s.f[fH].data();
+    a.nc           = s.nc.data();
+    a.nidx         = s.nidx.data();
+    a.sl           = SkinLists{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap};
+    a.xb           = s.skinXb.data();
+    a.yb           = s.skinYb.data();
+    a.zb           = s.skinZb.data();
+    a.moved        = s.skinAnyMoved ? s.skinMoved.data() : nullptr;
+    a.dispGrid     = s.skinGrid.data();
+    a.groupD       = s.skinGroupD.data();
+    a.numWorklist  = s.skinWork.data();
+    a.numWorklist2 = s.skinWork.data() + 1;
+    a.worklist     = s.skinWork.data() + 2;
+    a.worklist2    = s.skinWork.data() + 2 + s.numGroups();
+    a.n            = s.n;
+    a.box          = s.box;
+    a.prm          = np;
+    SPHB_TRY(checkSkinGroups(a, st));
+    // the tree search of the deferred groups runs on the side stream while the refilter serves the others (the two
+    // write disjoint groups)
+    SPHB_CUDA_TRY(cudaEventRecord(s.skinFork, st));
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.sideStream, s.skinFork, 0));
+    SPHB_TRY(findNeighborsListed(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n,
+                                 tv, s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), a.worklist,
+                                 a.numWorklist, s.sideStream));
+    SPHB_CUDA_TRY(cudaEventRecord(s.skinJoin, s.sideStream));
     SPHB_TRY(filterSkinLists(a, st));
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(st, s.skinJoin, 0));
     return findNeighborsListed(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
-                               s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), s.skinWork.data() + 1,
-                               s.skinWork.data(), st);
+                               s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), a.worklist2, a.numWorklist2,
+                               st);
 }
 
 int computeForces(sphb_sim& s)
@@ -596,15 +619,15 @@ int computeForces(sphb_sim& s)
     SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(red, s.reduce.data(), sizeof(red), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    unsigned deferred = 0;
+    unsigned deferred[2] = {0, 0};
     if (s.skinFiltered)
     {
-        SPHB_CUDA_TRY(cudaMemcpyAsync(&deferred, s.skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(deferred, s.skinWork.data(), sizeof(deferred), cudaMemcpyDeviceToHost, st));
     }
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIntegrate], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
-    s.skinDeferredLast = deferred;
-    s.searchStats[3] += deferred;
+    s.skinDeferredLast = deferred[0] + deferred[1];
+    s.searchStats[3] += s.skinDeferredLast;
     if (status) { return kErrCapacity; }
 
     double maxDivv = fromOrderedBits(red[0]);
@@ -846,6 +869,13 @@ extern "C" int sphb_sim_destroy(sphb_sim* s)
         if (e) { cudaEventDestroy(e); }
     }
     if (s->stream) { cudaStreamDestroy(s->stream); }
+    if (s->sideStream)
+    {
+        cudaStreamSynchronize(s->sideStream);
+        cudaStreamDestroy(s->sideStream);
+    }
+    if (s->skinFork) { cudaEventDestroy(s->skinFork); }
+    if (s->skinJoin) { cudaEventDestroy(s->skinJoin); }
     delete s;
     return SPHB_OK;
 }

@@ -13,7 +13,10 @@
 // current positions, so it sees every particle that can be near. A relative margin of 1e-9 covers the rounding of
 // the FP64 displacement and distance arithmetic. Indices must not have changed either: a row stores build indices,
 // so a group is served only when none of its particles and none of its rows' entries moved to another index since
-// the build (tracked through the sort permutations). Every other group goes to a worklist for the tree search.
+// the build. The sort permutations are composed into a current-to-build index map; a particle at another index than
+// at the build puts an infinite displacement into the grid cell of its build position, which lies within
+// R_i + d_i of x_i for every row i that lists it, so every group whose rows can hold it is deferred. Every deferred
+// group goes to a worklist for the tree search.
 // Entries are tested with the reference's exact FP64 expression (FP64 chain) or in FP32 from the fixed-point
 // coordinates with an uncertainty band around the radius inside which the exact FP64 test decides (mixed chain), so
 // the lists, counts and smoothing lengths are those of the tree search bit for bit.
@@ -107,6 +110,15 @@ __global__ void skinDisplacementKernel(const double4* __restrict__ pos, const do
         bits = __float_as_uint(__double2float_ru(d));
         cell = (cellOf(p.x, box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(p.y, box.lo[1], box.ilen[1])) * kSkinGrid +
                cellOf(p.z, box.lo[2], box.ilen[2]);
+        if (b != i)
+        {
+            // this particle sits at another index than at the build, so every row that lists it is stale: an
+            // infinite displacement at its build position defers each group whose rows can hold it
+            int cb = (cellOf(xb[b], box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(yb[b], box.lo[1], box.ilen[1])) *
+                         kSkinGrid +
+                     cellOf(zb[b], box.lo[2], box.ilen[2]);
+            atomicMax(grid + cb, __float_as_uint(INFINITY));
+        }
     }
     // consecutive particles are close in space: a warp whose particles share one cell issues a single atomic
     int cell0 = __shfl_sync(0xffffffffu, cell, 0);
@@ -134,35 +146,27 @@ __global__ void skinRemapKernel(const uint32_t* __restrict__ order, const uint32
     if ((threadIdx.x & (kWarp - 1)) == 0 && i < n) { moved[i / kWarp] = m; }
 }
 
-/*! One warp per group of 32 consecutive particles, one lane per particle: the neighbour lists come out in the same
- *  chunked layout, written as whole sectors, as from the tree search. */
-template<bool kFixed>
-__global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArgs a)
+//! groupD entry of a group deferred by the check
+constexpr unsigned kDeferred = 0xffffffffu;
+
+/*! Whether the group's rows can serve every particle of the group at its current h (and D, the largest displacement
+ *  near the group, for the later checks of the smoothing-length iteration). One warp, one lane per particle. */
+__device__ inline bool checkGroup(const SkinFilterArgs& a, int lane, bool valid, const double4& pi, double Ri, double di,
+                                  unsigned rowCount, double hi, size_t i, float* Dout)
 {
-    __shared__ alignas(16) uint32_t nbuf[kFilterWarps][kWarp][kNbChunk];
-    const int warp         = threadIdx.x / kWarp;
-    const int lane         = threadIdx.x & (kWarp - 1);
-    const size_t numGroups = (a.n + kWarp - 1) / kWarp;
-    const size_t group     = size_t(blockIdx.x) * kFilterWarps + warp;
-    if (group >= numGroups) { return; }
-    const size_t i   = group * kWarp + lane;
-    const bool valid = i < a.n;
+    bool ok = !valid || (rowCount <= a.sl.cap && !(a.moved && bitSet(a.moved, i)));
 
-    double4 pi = valid ? loadPos(a.pos + i) : make_double4(0, 0, 0, 0);
-    double hi  = valid ? a.h[i] : 0.0;
-    double Ri  = valid ? a.sl.radius[i] : 0.0;
-    unsigned rowCount = valid ? a.sl.count[i] : 0u;
-    double di  = valid ? displacement(pi.x, pi.y, pi.z, a.xb[i], a.yb[i], a.zb[i], a.box) : 0.0;
-    bool ok    = !valid || (rowCount <= a.sl.cap && !(a.moved && bitSet(a.moved, i)));
-
-    // the largest displacement of any particle that can now be within R_i of a particle of the group
+    // The largest displacement of any particle that can now be within R_i of a particle of the group. The region
+    // also holds the build position of every particle in the group's rows (within R_i of the build position of i,
+    // which is d_i away), so a particle of the rows that changed index marks it infinite.
+    const double reach = valid ? (Ri + di) * kSkinMargin : 0.0;
     double lo[3], hb[3];
-    lo[0] = warpMinD(valid ? pi.x - Ri : INFINITY);
-    lo[1] = warpMinD(valid ? pi.y - Ri : INFINITY);
-    lo[2] = warpMinD(valid ? pi.z - Ri : INFINITY);
-    hb[0] = warpMaxD(valid ? pi.x + Ri : -INFINITY);
-    hb[1] = warpMaxD(valid ? pi.y + Ri : -INFINITY);
-    hb[2] = warpMaxD(valid ? pi.z + Ri : -INFINITY);
+    lo[0] = warpMinD(valid ? pi.x - reach : INFINITY);
+    lo[1] = warpMinD(valid ? pi.y - reach : INFINITY);
+    lo[2] = warpMinD(valid ? pi.z - reach : INFINITY);
+    hb[0] = warpMaxD(valid ? pi.x + reach : -INFINITY);
+    hb[1] = warpMaxD(valid ? pi.y + reach : -INFINITY);
+    hb[2] = warpMaxD(valid ? pi.z + reach : -INFINITY);
     int c0[3], span[3];
     int numCells = 1;
 #pragma unroll
@@ -202,19 +206,67 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
         }
         dmax = max(dmax, __ldg(a.dispGrid + (c[0] * kSkinGrid + c[1]) * kSkinGrid + c[2]));
     }
-    const double D = double(__uint_as_float(warpMaxU(dmax)));
+    const float D = __uint_as_float(warpMaxU(dmax));
+    *Dout         = D;
+    ok            = ok && (!valid || (2.0 * hi + di + double(D)) * kSkinMargin <= Ri);
+    return __all_sync(0xffffffffu, ok);
+}
+
+/*! The check of every group before the refilter: deferred groups go to the worklist at once, so that their tree
+ *  search can run beside the refilter of the others. groupD receives D, or kDeferred. */
+__global__ void __launch_bounds__(kFilterThreads) skinCheckKernel(SkinFilterArgs a)
+{
+    const int warp         = threadIdx.x / kWarp;
+    const int lane         = threadIdx.x & (kWarp - 1);
+    const size_t numGroups = (a.n + kWarp - 1) / kWarp;
+    const size_t group     = size_t(blockIdx.x) * kFilterWarps + warp;
+    if (group >= numGroups) { return; }
+    const size_t i    = group * kWarp + lane;
+    const bool valid  = i < a.n;
+    double4 pi        = valid ? loadPos(a.pos + i) : make_double4(0, 0, 0, 0);
+    double hi         = valid ? a.h[i] : 0.0;
+    double Ri         = valid ? a.sl.radius[i] : 0.0;
+    unsigned rowCount = valid ? a.sl.count[i] : 0u;
+    double di         = valid ? displacement(pi.x, pi.y, pi.z, a.xb[i], a.yb[i], a.zb[i], a.box) : 0.0;
+    float D;
+    bool ok = checkGroup(a, lane, valid, pi, Ri, di, rowCount, hi, i, &D);
+    if (lane == 0)
+    {
+        a.groupD[group] = ok ? __float_as_uint(D) : kDeferred;
+        if (!ok) { a.worklist[atomicAdd(a.numWorklist, 1u)] = unsigned(group); }
+    }
+}
+
+/*! One warp per group of 32 consecutive particles, one lane per particle: the neighbour lists come out in the same
+ *  chunked layout, written as whole sectors, as from the tree search. Groups the check deferred are skipped; a group
+ *  whose smoothing-length iteration leaves its rows goes to the second worklist. */
+template<bool kFixed>
+__global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArgs a)
+{
+    // per lane: a ring of two list chunks, the one being filled and the next (lane minor: the lanes' appends fall
+    // into distinct banks); one row chunk adds at most eight neighbours, so it completes at most one list chunk
+    __shared__ uint32_t nbuf[kFilterWarps][2 * kNbChunk][kWarp];
+    const int warp         = threadIdx.x / kWarp;
+    const int lane         = threadIdx.x & (kWarp - 1);
+    const size_t numGroups = (a.n + kWarp - 1) / kWarp;
+    const size_t group     = size_t(blockIdx.x) * kFilterWarps + warp;
+    if (group >= numGroups) { return; }
+    const unsigned gD = __ldg(a.groupD + group);
+    if (gD == kDeferred) { return; }
+    const double D   = double(__uint_as_float(gD));
+    const size_t i   = group * kWarp + lane;
+    const bool valid = i < a.n;
+
+    double4 pi = valid ? loadPos(a.pos + i) : make_double4(0, 0, 0, 0);
+    double hi  = valid ? a.h[i] : 0.0;
+    double Ri  = valid ? a.sl.radius[i] : 0.0;
+    unsigned rowCount = valid ? a.sl.count[i] : 0u;
+    double di  = valid ? displacement(pi.x, pi.y, pi.z, a.xb[i], a.yb[i], a.zb[i], a.box) : 0.0;
 
     auto covered = [&](double h) { return (2.0 * h + di + D) * kSkinMargin <= Ri; };
-    ok = ok && (!valid || covered(hi));
-
-    auto defer = [&]() {
-        if (lane == 0) { a.worklist[atomicAdd(a.numWorklist, 1u)] = unsigned(group); }
+    auto defer   = [&]() {
+        if (lane == 0) { a.worklist2[atomicAdd(a.numWorklist2, 1u)] = unsigned(group); }
     };
-    if (!__all_sync(0xffffffffu, ok))
-    {
-        defer();
-        return;
-    }
 
     const unsigned ngmin  = a.prm.ng0 / 4;
     const unsigned ngPad  = paddedNgmax(a.prm.ngmax);
@@ -224,13 +276,13 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
     {
         if (valid) { qi = __ldg(a.posq + i); }
     }
-    uint32_t* chunk = nbuf[warp][lane];
+    uint32_t* ring = &nbuf[warp][0][lane];
     auto storeChunk = [&](unsigned c) {
-        uint32_t* dst    = a.nidx + nidxAt(group, ngPad, c * kNbChunk, lane);
-        const uint4* src = reinterpret_cast<const uint4*>(chunk);
-        uint4 u = src[0], v = src[1];
-        asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(u.x), "r"(u.y),
-                     "r"(u.z), "r"(u.w), "r"(v.x), "r"(v.y), "r"(v.z), "r"(v.w)
+        uint32_t* dst       = a.nidx + nidxAt(group, ngPad, c * kNbChunk, lane);
+        const uint32_t* src = ring + (c % 2) * kNbChunk * kWarp;
+        asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(src[0]),
+                     "r"(src[kWarp]), "r"(src[2 * kWarp]), "r"(src[3 * kWarp]), "r"(src[4 * kWarp]),
+                     "r"(src[5 * kWarp]), "r"(src[6 * kWarp]), "r"(src[7 * kWarp])
                      : "memory");
     };
 
@@ -251,51 +303,69 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
             const float band = 2.0e-6f + 8.0f * u + 8.0f * u * u;
             const float r2lo = r2f * (1.f - band);
             const float r2hi = r2f * (1.f + band);
-            count            = 0;
+            count           = 0;
+            unsigned stored = 0; // list chunks written
             for (unsigned c = 0; c < rowLen; c += kNbChunk)
             {
                 const uint32_t* src = a.sl.rows + nidxAt(group, a.sl.cap, c, lane);
                 uint4 e0 = __ldg(reinterpret_cast<const uint4*>(src));
                 uint4 e1 = __ldg(reinterpret_cast<const uint4*>(src) + 1);
                 uint32_t e[kNbChunk] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-#pragma unroll
-                for (unsigned k = 0; k < kNbChunk; ++k)
+                // entries past the row's end (garbage in its last chunk) are replaced by i and masked out, so that
+                // all eight gathers are issued together
+                unsigned in = 0u;
+                if constexpr (kFixed)
                 {
-                    if (c + k >= rowLen) { break; }
-                    const uint32_t j = e[k];
-                    if (a.moved && bitSet(a.moved, j)) { bad = true; }
-                    bool in;
-                    if constexpr (kFixed)
+                    unsigned band = 0u;
+#pragma unroll
+                    for (unsigned k = 0; k < kNbChunk; ++k)
                     {
+                        const bool real = c + k < rowLen;
+                        const uint32_t j = real ? e[k] : uint32_t(i);
                         int4 qj  = __ldg(a.posq + j);
                         float dx = float(int(unsigned(qi.x) - unsigned(qj.x))) * a.qscale[0];
                         float dy = float(int(unsigned(qi.y) - unsigned(qj.y))) * a.qscale[1];
                         float dz = float(int(unsigned(qi.z) - unsigned(qj.z))) * a.qscale[2];
                         float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        in       = d2 < r2lo;
-                        if (!in && d2 < r2hi)
+                        in |= unsigned(real && d2 < r2lo) << k;
+                        band |= unsigned(real && d2 >= r2lo && d2 < r2hi) << k;
+                    }
+                    // too close to the radius for FP32: the exact test of the reference (rare)
+#pragma unroll
+                    for (unsigned k = 0; k < kNbChunk; ++k)
+                    {
+                        if ((band >> k) & 1u)
                         {
-                            double4 pj = loadPos(a.pos + j);
-                            in         = exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq;
+                            double4 pj = loadPos(a.pos + e[k]);
+                            if (exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq) { in |= 1u << k; }
                         }
                     }
-                    else
+                }
+                else
+                {
+#pragma unroll
+                    for (unsigned k = 0; k < kNbChunk; ++k)
                     {
-                        double4 pj = loadPos(a.pos + j);
-                        in         = exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq;
+                        const bool real = c + k < rowLen;
+                        double4 pj      = loadPos(a.pos + (real ? e[k] : uint32_t(i)));
+                        in |= unsigned(real && exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq) << k;
                     }
-                    if (in)
+                }
+                // append the neighbours in row (= index) order
+#pragma unroll
+                for (unsigned k = 0; k < kNbChunk; ++k)
+                {
+                    if ((in >> k) & 1u)
                     {
-                        if (count < a.prm.ngmax)
-                        {
-                            chunk[count % kNbChunk] = j;
-                            if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
-                        }
+                        if (count < a.prm.ngmax) { ring[(count % (2 * kNbChunk)) * kWarp] = e[k]; }
                         ++count;
                     }
                 }
+                if (min(count, a.prm.ngmax) / kNbChunk > stored) { storeChunk(stored++); }
             }
-            if (count % kNbChunk != 0 && count < a.prm.ngmax) { storeChunk(count / kNbChunk); }
+            // the last, partly filled chunk (entries past the count, or past ngmax, are never read)
+            const unsigned kept = min(count, a.prm.ngmax);
+            if (kept % kNbChunk != 0) { storeChunk(kept / kNbChunk); }
 
             // smoothing-length iteration, as in the tree search; a new h must stay covered by the row
             unsigned ncSph = count + 1;
@@ -357,6 +427,18 @@ int skinRemap(const uint32_t* order, const uint32_t* buildOld, uint32_t* buildNe
 {
     if (n == 0) { return kOk; }
     skinRemapKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(order, buildOld, buildNew, moved, n);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int checkSkinGroups(const SkinFilterArgs& a, cudaStream_t stream)
+{
+    if (a.n == 0) { return kOk; }
+    if (a.sl.cap == 0 || a.sl.cap % kNbChunk != 0) { return kErrArg; }
+    size_t numGroups = (a.n + kWarp - 1) / kWarp;
+    unsigned blocks  = unsigned((numGroups + kFilterWarps - 1) / kFilterWarps);
+    skinCheckKernel<<<blocks, kFilterThreads, 0, stream>>>(a);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

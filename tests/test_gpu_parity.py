@@ -293,6 +293,36 @@ def test_h_iteration_and_ragged_sizes_vs_reference(lib, ref, side, scale, ng0, n
         g.integrate()
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_clump_over_ngmax_vs_reference(lib, ref, precision):
+    """A clump of 180 particles within 1e-7 of one point keeps more than ngmax = 150 neighbours through all ten
+    smoothing-length iterations: the lists must hold the first ngmax in index order, as the reference's do, including
+    the last, partly filled list chunk."""
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(16)
+    rng = np.random.default_rng(5)
+    extra = 180
+    n0 = ic["x"].size
+    for f in ("x", "y", "z"):
+        ic[f] = np.concatenate([ic[f], 0.1 + rng.uniform(-1e-7, 1e-7, extra)])
+    for f in ("h", "m", "temp", "vx", "vy", "vz", "x_m1", "y_m1", "z_m1", "du_m1", "alpha"):
+        ic[f] = np.concatenate([ic[f], np.full(extra, ic[f][0])])
+    ic["id"] = np.arange(n0 + extra, dtype=np.uint64)
+    r = ref.RefSim(ic)
+    g = Simulation(ic, precision)
+    r.compute_forces()
+    g.compute_forces()
+    ncr = r.get("nc").astype(np.int64)
+    assert np.array_equal(g.get("nc").astype(np.int64), ncr)
+    assert int(ncr.max()) - 1 > 150
+    assert _max_rel(g.get("h"), r.get("h")) < 1e-14
+    nbr, nbg = r.neighbors(), g.neighbors()
+    for i in range(g.n):
+        k = min(ncr[i] - 1, 150)
+        assert np.array_equal(nbg[i, :k], nbr[i, :k]), i
+
+
 def test_zero_length_calls(lib):
     import torch
     from sphexa_b200 import lib as L
