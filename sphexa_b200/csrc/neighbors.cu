@@ -44,6 +44,7 @@ struct NbShared
     // per lane: the neighbours of the list chunk being filled, written out as one 32-byte sector when full; lane
     // minor, so that the lanes' appends fall into distinct banks
     uint32_t nbuf[kNbWarps][kNbChunk][kWarp];
+    uint16_t dbuf[kNbWarps][kNbChunk][kWarp]; // skin rows: the quantised build distance of each entry
 };
 
 /*! Half width of the band |d^2 - (2h)^2| < band * (2h)^2 in which the FP32 distance cannot decide and the exact FP64
@@ -233,9 +234,20 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
         int numLeaves = 0;
 
         // this lane's chunk buffer and its store to the chunked list layout (nidxAt)
-        uint32_t* chunk = &sh.nbuf[warp][0][lane];
+        uint32_t* chunk     = &sh.nbuf[warp][0][lane];
+        uint16_t* dchunk    = &sh.dbuf[warp][0][lane];
+        const double qScale = kSkinDistUnits / r; // skin rows: distance -> units of R / kSkinDistUnits
         auto storeChunk = [&](unsigned c) {
             uint32_t* dst = outList + nidxAt(group, ngPad, c * kNbChunk, lane);
+            if constexpr (kSkin)
+            {
+                uint4 d;
+                d.x = unsigned(dchunk[0]) | (unsigned(dchunk[kWarp]) << 16);
+                d.y = unsigned(dchunk[2 * kWarp]) | (unsigned(dchunk[3 * kWarp]) << 16);
+                d.z = unsigned(dchunk[4 * kWarp]) | (unsigned(dchunk[5 * kWarp]) << 16);
+                d.w = unsigned(dchunk[6 * kWarp]) | (unsigned(dchunk[7 * kWarp]) << 16);
+                *reinterpret_cast<uint4*>(ex.sl.dist + nidxAt(group, ngPad, c * kNbChunk, lane)) = d;
+            }
             // one 256-bit streaming store of the whole sector (the lists are next read once per J-loop)
             asm volatile("st.global.cs.v8.u32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"l"(dst), "r"(chunk[0]),
                          "r"(chunk[kWarp]), "r"(chunk[2 * kWarp]), "r"(chunk[3 * kWarp]), "r"(chunk[4 * kWarp]),
@@ -291,6 +303,13 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 if (size_t(j) == i) { continue; }
                 if (count < listCap)
                 {
+                    if constexpr (kSkin)
+                    {
+                        // the build distance, from the reference's FP64 expression, for the refilter's bounds
+                        double4 pj = ldPos(pos + j);
+                        double q   = rint(sqrt(exactDistSq(pj.x, pj.y, pj.z, xi, yi, zi, box)) * qScale);
+                        dchunk[(count % kNbChunk) * kWarp] = uint16_t(fmin(q, kSkinDistUnits));
+                    }
                     chunk[(count % kNbChunk) * kWarp] = uint32_t(j);
                     if (count % kNbChunk == kNbChunk - 1) { storeChunk(count / kNbChunk); }
                 }

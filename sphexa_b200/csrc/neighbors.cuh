@@ -79,14 +79,19 @@ __device__ inline double searchRadiusSq(double h) { return __dmul_rn(__dmul_rn(4
 /*! Candidate lists kept across steps ("skin" lists): for every particle, each j whose distance was below
  *  R_i = 2 h_i (1 + skin) when the lists were built, in ascending index order, at most `cap` of them (chunked like
  *  the neighbour lists, with `cap` as the padded width). count[i] is the number found, which can exceed cap: the row
- *  is then incomplete and never used. */
+ *  is then incomplete and never used. dist holds, beside each entry, its distance at the build in units of
+ *  R_i / kSkinDistUnits, rounded to nearest (16 bits, same chunked layout). */
 struct SkinLists
 {
     uint32_t* rows;
     unsigned* count;
     double* radius;
     unsigned cap;
+    uint16_t* dist;
 };
+
+//! units of the quantised build distance per R_i
+constexpr double kSkinDistUnits = 65535.0;
 
 /*! Search all particles (x, y, z and the same coordinates packed as pos = (x, y, z, m)): updates h where the count left [ng0/4, ngmax+1], writes nc (count incl. self) and lists.
  *  status[0] is set to a non-zero value if a per-warp buffer overflowed (the search then returns SPHB_ERR_CAPACITY).

@@ -107,6 +107,7 @@ struct sphb_sim
 
     // skin lists (neighbors.cuh): candidate rows kept across steps and refiltered exactly every step
     DeviceBuffer<uint32_t> skinRows;
+    DeviceBuffer<uint16_t> skinDist;
     DeviceBuffer<unsigned> skinCount;
     DeviceBuffer<double> skinRadius, skinXb, skinYb, skinZb;
     DeviceBuffer<uint32_t> skinBuild, skinBuildAlt, skinMoved;
@@ -459,6 +460,7 @@ int allocateSkin(sphb_sim& s)
     s.skinCap   = paddedNgmax(unsigned(std::ceil(s.p.ngmax * grow * 1.1)));
     size_t n = s.n;
     SPHB_TRY(s.skinRows.reserve(s.numGroups() * size_t(s.skinCap) * kWarp));
+    SPHB_TRY(s.skinDist.reserve(s.numGroups() * size_t(s.skinCap) * kWarp));
     SPHB_TRY(s.skinCount.reserve(n));
     SPHB_TRY(s.skinRadius.reserve(n));
     SPHB_TRY(s.skinXb.reserve(n));
@@ -518,7 +520,7 @@ int searchNeighbors(sphb_sim& s)
     {
         SPHB_TRY(allocateSkin(s));
         SPHB_TRY(treeSearch());
-        SkinLists sl{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap};
+        SkinLists sl{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap, s.skinDist.data()};
         SPHB_TRY(buildSkinLists(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.pos.data(), s.f[fH].data(), s.n, tv,
                                 s.box, np, s.p.nb_skin, sl, s.status.data(), st));
         size_t bytes = s.n * sizeof(double);
@@ -556,7 +558,8 @@ int searchNeighbors(sphb_sim& s)
     a.h            = s.f[fH].data();
     a.nc           = s.nc.data();
     a.nidx         = s.nidx.data();
-    a.sl           = SkinLists{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap};
+    a.sl           = SkinLists{s.skinRows.data(), s.skinCount.data(), s.skinRadius.data(), s.skinCap,
+                               s.skinDist.data()};
     a.xb           = s.skinXb.data();
     a.yb           = s.skinYb.data();
     a.zb           = s.skinZb.data();

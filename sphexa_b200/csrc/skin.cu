@@ -110,15 +110,15 @@ __global__ void skinDisplacementKernel(const double4* __restrict__ pos, const do
         bits = __float_as_uint(__double2float_ru(d));
         cell = (cellOf(p.x, box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(p.y, box.lo[1], box.ilen[1])) * kSkinGrid +
                cellOf(p.z, box.lo[2], box.ilen[2]);
-        if (b != i)
-        {
-            // this particle sits at another index than at the build, so every row that lists it is stale: an
-            // infinite displacement at its build position defers each group whose rows can hold it
-            int cb = (cellOf(xb[b], box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(yb[b], box.lo[1], box.ilen[1])) *
-                         kSkinGrid +
-                     cellOf(zb[b], box.lo[2], box.ilen[2]);
-            atomicMax(grid + cb, __float_as_uint(INFINITY));
-        }
+        // The displacement also goes to the cell of the build position, which every group whose rows list this
+        // particle checks: the refilter decides most entries from their build distance and these bounds. A particle
+        // at another index than at the build makes those rows stale: infinite there.
+        int cb = (cellOf(xb[b], box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(yb[b], box.lo[1], box.ilen[1])) *
+                     kSkinGrid +
+                 cellOf(zb[b], box.lo[2], box.ilen[2]);
+        unsigned atBuild = b != i ? __float_as_uint(INFINITY) : bits;
+        if (cb != cell && atBuild != 0u) { atomicMax(grid + cb, atBuild); }
+        else if (cb == cell) { bits = max(bits, atBuild); }
     }
     // consecutive particles are close in space: a warp whose particles share one cell issues a single atomic
     int cell0 = __shfl_sync(0xffffffffu, cell, 0);
@@ -303,6 +303,15 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
             const float band = 2.0e-6f + 8.0f * u + 8.0f * u * u;
             const float r2lo = r2f * (1.f - band);
             const float r2hi = r2f * (1.f + band);
+            // Most entries are decided from their quantised build distance q (units of Ri / kSkinDistUnits, the true
+            // build distance within (q +- 0.5) units): now |x_i - x_j| lies within d_i + D of it, so entries with
+            // q <= qIn are surely inside 2 h_i and entries with q >= qOut surely outside, by a relative margin of
+            // 1e-9 that covers the FP64 rounding of the exact test. Only the rest are gathered and tested.
+            const double unit = Ri / kSkinDistUnits;
+            const double tIn  = (2.0 * hi * (1.0 - 1e-9) - di - D) / unit - 0.501;
+            const double tOut = (2.0 * hi * (1.0 + 1e-9) + di + D) / unit + 0.501;
+            const int qIn     = tIn > 0.0 ? int(ceil(tIn)) - 1 : -1;               // largest q < tIn
+            const int qOut    = tOut < kSkinDistUnits ? int(floor(tOut)) + 1 : 65536; // smallest q > tOut
             count           = 0;
             unsigned stored = 0; // list chunks written
             for (unsigned c = 0; c < rowLen; c += kNbChunk)
@@ -310,45 +319,47 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
                 const uint32_t* src = a.sl.rows + nidxAt(group, a.sl.cap, c, lane);
                 uint4 e0 = __ldg(reinterpret_cast<const uint4*>(src));
                 uint4 e1 = __ldg(reinterpret_cast<const uint4*>(src) + 1);
+                uint4 dq = __ldg(reinterpret_cast<const uint4*>(a.sl.dist + nidxAt(group, a.sl.cap, c, lane)));
                 uint32_t e[kNbChunk] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
-                // entries past the row's end (garbage in its last chunk) are replaced by i and masked out, so that
-                // all eight gathers are issued together
-                unsigned in = 0u;
-                if constexpr (kFixed)
+                int q[kNbChunk] = {int(dq.x & 0xffffu), int(dq.x >> 16), int(dq.y & 0xffffu), int(dq.y >> 16),
+                                   int(dq.z & 0xffffu), int(dq.z >> 16), int(dq.w & 0xffffu), int(dq.w >> 16)};
+                // entries past the row's end (garbage in its last chunk) are masked out
+                unsigned in = 0u, test = 0u;
+#pragma unroll
+                for (unsigned k = 0; k < kNbChunk; ++k)
                 {
-                    unsigned band = 0u;
+                    const bool real = c + k < rowLen;
+                    in |= unsigned(real && q[k] <= qIn) << k;
+                    test |= unsigned(real && q[k] > qIn && q[k] < qOut) << k;
+                }
+                if (test)
+                {
 #pragma unroll
                     for (unsigned k = 0; k < kNbChunk; ++k)
                     {
-                        const bool real = c + k < rowLen;
-                        const uint32_t j = real ? e[k] : uint32_t(i);
-                        int4 qj  = __ldg(a.posq + j);
-                        float dx = float(int(unsigned(qi.x) - unsigned(qj.x))) * a.qscale[0];
-                        float dy = float(int(unsigned(qi.y) - unsigned(qj.y))) * a.qscale[1];
-                        float dz = float(int(unsigned(qi.z) - unsigned(qj.z))) * a.qscale[2];
-                        float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        in |= unsigned(real && d2 < r2lo) << k;
-                        band |= unsigned(real && d2 >= r2lo && d2 < r2hi) << k;
-                    }
-                    // too close to the radius for FP32: the exact test of the reference (rare)
-#pragma unroll
-                    for (unsigned k = 0; k < kNbChunk; ++k)
-                    {
-                        if ((band >> k) & 1u)
+                        if (!((test >> k) & 1u)) { continue; }
+                        bool inside;
+                        if constexpr (kFixed)
+                        {
+                            // FP32 from the fixed-point coordinates, the exact FP64 test inside the band
+                            int4 qj  = __ldg(a.posq + e[k]);
+                            float dx = float(int(unsigned(qi.x) - unsigned(qj.x))) * a.qscale[0];
+                            float dy = float(int(unsigned(qi.y) - unsigned(qj.y))) * a.qscale[1];
+                            float dz = float(int(unsigned(qi.z) - unsigned(qj.z))) * a.qscale[2];
+                            float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            inside   = d2 < r2lo;
+                            if (!inside && d2 < r2hi)
+                            {
+                                double4 pj = loadPos(a.pos + e[k]);
+                                inside     = exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq;
+                            }
+                        }
+                        else
                         {
                             double4 pj = loadPos(a.pos + e[k]);
-                            if (exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq) { in |= 1u << k; }
+                            inside     = exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq;
                         }
-                    }
-                }
-                else
-                {
-#pragma unroll
-                    for (unsigned k = 0; k < kNbChunk; ++k)
-                    {
-                        const bool real = c + k < rowLen;
-                        double4 pj      = loadPos(a.pos + (real ? e[k] : uint32_t(i)));
-                        in |= unsigned(real && exactDistSq(pj.x, pj.y, pj.z, pi.x, pi.y, pi.z, a.box) < radiusSq) << k;
+                        in |= unsigned(inside) << k;
                     }
                 }
                 // append the neighbours in row (= index) order
