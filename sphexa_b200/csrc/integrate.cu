@@ -2,6 +2,7 @@
 // smoothing-length update, coordinate min/max and the conservation reductions.
 #include "hydro.cuh"
 #include "integrate.cuh"
+#include "neighbors.cuh"
 #include "primitives.cuh"
 
 namespace sphb
@@ -30,6 +31,49 @@ __global__ void packPosKernel(const double* x, const double* y, const double* z,
     {
         posq[i] = make_int4(quantiseFixed(x[i], fr.lo[0], fr.invUnit[0]), quantiseFixed(y[i], fr.lo[1], fr.invUnit[1]),
                             quantiseFixed(z[i], fr.lo[2], fr.invUnit[2]), __float_as_int(float(m[i])));
+    }
+}
+
+/*! packPosKernel and the bounding boxes of the runs of kBlockSize consecutive particles (computeBlockBoxes) in one
+ *  pass over the coordinates: the lanes of a run reduce their box with shuffles (runs start at multiples of
+ *  kBlockSize, and so do lane groups of kBlockSize in a block of a multiple of 32 threads). */
+__global__ void packPosBoxesKernel(const double* x, const double* y, const double* z, const double* m, size_t n,
+                                   double4* pos, int4* posq, FixedFrame fr, DevBox box, float4* boxLo, float4* boxHi)
+{
+    size_t i   = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    bool valid = i < n;
+    double p[3] = {0.0, 0.0, 0.0};
+    if (valid)
+    {
+        p[0] = x[i];
+        p[1] = y[i];
+        p[2] = z[i];
+        double mi = m[i];
+        if (pos) { pos[i] = make_double4(p[0], p[1], p[2], mi); }
+        if (posq)
+        {
+            posq[i] = make_int4(quantiseFixed(p[0], fr.lo[0], fr.invUnit[0]), quantiseFixed(p[1], fr.lo[1], fr.invUnit[1]),
+                                quantiseFixed(p[2], fr.lo[2], fr.invUnit[2]), __float_as_int(float(mi)));
+        }
+    }
+    double l[3], u[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+    {
+        l[k] = valid ? p[k] - box.lo[k] : INFINITY;
+        u[k] = valid ? p[k] - box.lo[k] : -INFINITY;
+#pragma unroll
+        for (int off = 1; off < kBlockSize; off <<= 1)
+        {
+            l[k] = fmin(l[k], __shfl_xor_sync(0xffffffffu, l[k], off));
+            u[k] = fmax(u[k], __shfl_xor_sync(0xffffffffu, u[k], off));
+        }
+    }
+    if (valid && i % kBlockSize == 0)
+    {
+        size_t c = i / kBlockSize;
+        boxLo[c] = make_float4(__double2float_rd(l[0]), __double2float_rd(l[1]), __double2float_rd(l[2]), 0.f);
+        boxHi[c] = make_float4(__double2float_ru(u[0]), __double2float_ru(u[1]), __double2float_ru(u[2]), 0.f);
     }
 }
 
@@ -196,6 +240,18 @@ FixedFrame fixedFrameOf(const DevBox& box)
         fr.unit[k]    = span / 4294967296.0;
     }
     return fr;
+}
+
+int packPositionsAndBoxes(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
+                          int4* posq, const DevBox& box, float4* boxLo, float4* boxHi, cudaStream_t s)
+{
+    if (n == 0) { return kOk; }
+    static_assert(256 % kBlockSize == 0 && kWarp % kBlockSize == 0, "runs must not straddle warps");
+    packPosBoxesKernel<<<ceilDiv(n, 256), 256, 0, s>>>(x, y, z, m, n, pos, posq, fixedFrameOf(box), box, boxLo,
+                                                       boxHi);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
 }
 
 int packPositions(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,

@@ -33,6 +33,10 @@ FixedFrame fixedFrameOf(const DevBox& box);
 int packPositions(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
                   int4* posq, const DevBox& box, cudaStream_t s);
 
+//! packPositions and, in the same pass, the bounding boxes of computeBlockBoxes (neighbors.cuh)
+int packPositionsAndBoxes(const double* x, const double* y, const double* z, const double* m, size_t n, double4* pos,
+                          int4* posq, const DevBox& box, float4* boxLo, float4* boxHi, cudaStream_t s);
+
 template<class T>
 int launchPositions(size_t n, const IntegrateArrays<T>& a, const DevBox& box, double dt, double dtm1, double cv,
                     cudaStream_t s);

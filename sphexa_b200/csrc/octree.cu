@@ -516,6 +516,7 @@ int initGlobalTree(GlobalTree& g, unsigned bucket, cudaStream_t stream)
     g.bucket    = bucket;
     g.numLeaves = 1;
     g.firstCall = true;
+    g.hostStale = true;
     SPHB_TRY(g.leaves.reserve(2));
     SPHB_TRY(g.counts.reserve(1));
     setLeavesKernel<<<1, 1, 0, stream>>>(g.leaves.data(), g.counts.data(), bucket - 1);
@@ -537,14 +538,22 @@ int globalTreeStep(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s
     countLaunch();
     SPHB_TRY(exclusiveScan(s.ints.data(), s.ints.data(), L + 1, s.scanTmp.data(), stream));
     int newL = 0;
+    unsigned anyOp = 0;
     SPHB_CUDA_TRY(cudaMemcpyAsync(&newL, s.ints.data() + L, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&anyOp, s.flags.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
-    SPHB_TRY(g.leavesAlt.reserve(newL + 1));
-    rebalanceKernel<<<ceilDiv(L + 1, 256), 256, 0, stream>>>(g.leaves.data(), L, s.ints.data(), g.leavesAlt.data());
-    countLaunch();
-    SPHB_CUDA_TRY(cudaGetLastError());
-    g.leaves.swap(g.leavesAlt);
-    g.numLeaves = newL;
+    if (anyOp)
+    {
+        // every op 1 would give the same leaves: the rebalance runs only when a node splits or merges
+        SPHB_TRY(g.leavesAlt.reserve(newL + 1));
+        rebalanceKernel<<<ceilDiv(L + 1, 256), 256, 0, stream>>>(g.leaves.data(), L, s.ints.data(),
+                                                                 g.leavesAlt.data());
+        countLaunch();
+        SPHB_CUDA_TRY(cudaGetLastError());
+        g.leaves.swap(g.leavesAlt);
+        g.numLeaves = newL;
+        g.hostStale = true;
+    }
     SPHB_TRY(g.counts.reserve(newL));
     SPHB_TRY(computeLeafCounts(g.leaves.data(), newL, keys, n, g.counts.data(), stream));
     maxCountKernel<<<ceilDiv(newL, 256), 256, 0, stream>>>(g.counts.data(), newL, s.flags.data());
@@ -560,6 +569,7 @@ int globalTreeStep(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s
 
 int updateGlobalTree(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s, cudaStream_t stream)
 {
+    if (g.hostLeaves.empty()) { g.hostStale = true; }
     unsigned maxCount = 0;
     SPHB_TRY(globalTreeStep(g, keys, n, s, stream, &maxCount));
     if (g.firstCall || maxCount >= 8 * g.bucket)
@@ -572,10 +582,15 @@ int updateGlobalTree(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch&
             if (++guard > 64) { return kErrNotConverged; }
         } while (maxCount > g.bucket);
     }
-    g.hostLeaves.resize(g.numLeaves + 1);
-    SPHB_CUDA_TRY(cudaMemcpyAsync(g.hostLeaves.data(), g.leaves.data(), (g.numLeaves + 1) * sizeof(uint64_t),
-                                  cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    if (g.hostStale)
+    {
+        // the host copy of the leaves (mandatory keys of a failed focus update) follows only changes
+        g.hostLeaves.resize(g.numLeaves + 1);
+        SPHB_CUDA_TRY(cudaMemcpyAsync(g.hostLeaves.data(), g.leaves.data(), (g.numLeaves + 1) * sizeof(uint64_t),
+                                      cudaMemcpyDeviceToHost, stream));
+        SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+        g.hostStale = false;
+    }
     return kOk;
 }
 
@@ -636,6 +651,12 @@ int focusUpdateTree(FocusTree& f, const GlobalTree& g, TreeScratch& s, cudaStrea
     bool conv       = flags[1] == 0;
     if (status == kCancelMerge) { conv = flags[2] == 0; }
     else if (status == kRebalance) { conv = false; }
+    if (status != kFailed && flags[2] == 0 && newL == L)
+    {
+        // every leaf keeps its op 1: the leaves, and so the linked octree, stay as they are
+        *converged = conv;
+        return kOk;
+    }
 
     SPHB_TRY(f.leavesAlt.reserve(newL + 1));
     rebalanceKernel<<<ceilDiv(L + 1, 256), 256, 0, stream>>>(f.leaves.data(), L, leafOps, f.leavesAlt.data());

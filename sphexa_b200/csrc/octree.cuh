@@ -63,6 +63,7 @@ struct GlobalTree
     unsigned bucket{0};
     bool firstCall{true};
     std::vector<uint64_t> hostLeaves;
+    bool hostStale{true}; // hostLeaves lag the device leaves
 };
 
 int initGlobalTree(GlobalTree& g, unsigned bucket, cudaStream_t stream);

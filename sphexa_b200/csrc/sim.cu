@@ -307,10 +307,9 @@ int syncDomain(sphb_sim& s)
     SPHB_TRY(focusUpdateTree(s.ftree, s.gtree, s.ts, st, &converged));
     SPHB_TRY(focusUpdateCounts(s.ftree, s.keys.data(), s.n, s.ts, st));
     SPHB_TRY(computeGeoCenters(s.ftree.tree, s.box, st));
-    SPHB_TRY(packPositions(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n, s.pos.data(),
-                           s.mixed ? s.posq.data() : nullptr, s.box, st));
-    SPHB_TRY(computeBlockBoxes(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.n, s.box, s.blockLo.data(),
-                               s.blockHi.data(), st));
+    SPHB_TRY(packPositionsAndBoxes(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n,
+                                   s.pos.data(), s.mixed ? s.posq.data() : nullptr, s.box, s.blockLo.data(),
+                                   s.blockHi.data(), st));
     return kOk;
 }
 
