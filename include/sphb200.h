@@ -289,6 +289,12 @@ int sphb_ensemble_autotune(sphb_ensemble* ens, int* threads5_out);
 /*! Advance every instance by steps steps; use_graph != 0 replays one captured step (captured on first use). */
 int sphb_ensemble_step(sphb_ensemble* ens, int steps, int use_graph);
 
+/*! How the neighbour stage ran since the last upload or initial sync (the mode of each step is chosen on the
+ *  device from the skin rows' state, sphb_params.nb_skin of the first instance): out[0] tree searches of every group,
+ *  out[1] skin-row builds (each also counted in out[0]), out[2] steps served by refiltering the rows, out[3] groups
+ *  deferred to the tree search. All zero when nb_skin is 0. No counterpart in the reference. */
+int sphb_ensemble_search_stats(sphb_ensemble* ens, uint64_t* out);
+
 /*! Number of particles of instance k. */
 size_t sphb_ensemble_size(const sphb_ensemble* ens, int k);
 

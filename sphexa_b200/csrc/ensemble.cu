@@ -114,6 +114,16 @@ struct sphb_ensemble
     DeviceBuffer<double> alphaBackup, hBackup;
     uint64_t launchesPerStep{0};
 
+    // skin rows (neighbors.cuh): kept across steps and refiltered; the mode of each step is chosen on the device
+    bool skin{false};
+    unsigned skinCap{0};
+    DeviceBuffer<uint32_t> skinRows;
+    DeviceBuffer<uint16_t> skinDist;
+    DeviceBuffer<unsigned> skinCount;
+    DeviceBuffer<double> skinRadius, skinXb, skinYb, skinZb;
+    DeviceBuffer<uint32_t> skinBuild, skinBuildTmp, skinMoved;
+    DeviceBuffer<unsigned> skinGrid, skinWork, skinGroupD, skinCtl;
+
     int threads[kJLoops]{128, 128, 128, 128, 128};
     cudaGraphExec_t graph{nullptr};
     bool uploaded{false};
@@ -287,6 +297,27 @@ int allocate(sphb_ensemble& e)
     SPHB_TRY(e.status.reserve(4));
     SPHB_TRY(e.views.reserve(m));
     SPHB_TRY(e.leafDescs.reserve(m));
+    e.skin = e.p.nb_skin > 0.0;
+    if (e.skin)
+    {
+        double grow = (1.0 + e.p.nb_skin) * (1.0 + e.p.nb_skin) * (1.0 + e.p.nb_skin);
+        e.skinCap   = paddedNgmax(unsigned(std::ceil(e.p.ngmax * grow * 1.1)));
+        size_t groups = n / kWarp;
+        SPHB_TRY(e.skinRows.reserve(groups * size_t(e.skinCap) * kWarp));
+        SPHB_TRY(e.skinDist.reserve(groups * size_t(e.skinCap) * kWarp));
+        SPHB_TRY(e.skinCount.reserve(n));
+        SPHB_TRY(e.skinRadius.reserve(n));
+        SPHB_TRY(e.skinXb.reserve(n));
+        SPHB_TRY(e.skinYb.reserve(n));
+        SPHB_TRY(e.skinZb.reserve(n));
+        SPHB_TRY(e.skinBuild.reserve(n));
+        SPHB_TRY(e.skinBuildTmp.reserve(n));
+        SPHB_TRY(e.skinMoved.reserve(groups));
+        SPHB_TRY(e.skinGrid.reserve(size_t(kSkinCells) * size_t(m)));
+        SPHB_TRY(e.skinWork.reserve(2 * groups));
+        SPHB_TRY(e.skinGroupD.reserve(groups));
+        SPHB_TRY(e.skinCtl.reserve(kCtlWords));
+    }
 
     std::vector<double> wh(kTableSize), whd(kTableSize);
     e.K = sincKernelTables(e.p.sinc_index, wh.data(), whd.data(), kTableSize);
@@ -378,6 +409,13 @@ int syncBatched(sphb_ensemble& e, bool withLayout)
     dst[15] = e.keys.data();
     SPHB_TRY(gather8(e.order.data(), n, 16, src, dst, st));
     countLaunch(6);
+    if (e.skin)
+    {
+        // the skin rows hold build indices: compose this sort into the current-to-build map
+        SPHB_TRY(skinRemap(e.order.data(), e.skinBuild.data(), e.skinBuildTmp.data(), e.skinMoved.data(), n, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(e.skinBuild.data(), e.skinBuildTmp.data(), n * sizeof(uint32_t),
+                                      cudaMemcpyDeviceToDevice, st));
+    }
     if (withLayout)
     {
         dim3 grid(unsigned(ceilDiv(size_t(e.maxLeaves) + 1, 256)), unsigned(e.num));
@@ -595,6 +633,81 @@ int integrateBatched(sphb_ensemble& e)
     return kOk;
 }
 
+//! rows invalid, counters zero (a new state)
+int resetSkin(sphb_ensemble& e)
+{
+    if (!e.skin) { return kOk; }
+    unsigned ctl[kCtlWords] = {};
+    ctl[kCtlGroups]         = unsigned(e.slots / kWarp);
+    SPHB_CUDA_TRY(cudaMemcpyAsync(e.skinCtl.data(), ctl, sizeof(ctl), cudaMemcpyHostToDevice, e.stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(e.stream));
+    return kOk;
+}
+
+/*! The neighbour stage with skin rows, every step the same launches (graph-replayable): skinDecide picks the mode on
+ *  the device, and each launch returns at once unless the mode is its own. The lists are those of the tree search. */
+int searchBatchedSkin(sphb_ensemble& e, const NeighborParams& np)
+{
+    cudaStream_t st      = e.stream;
+    size_t n             = e.slots;
+    size_t groups        = n / kWarp;
+    unsigned* ctl        = e.skinCtl.data();
+    const unsigned* mode = ctl + kCtlMode;
+    TreeView dummy{};
+    SPHB_TRY(skinDecide(ctl, st));
+    SPHB_TRY(findNeighbors(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy, e.box,
+                           np, e.nidx.data(), e.nc.data(), e.status.data(), st, e.views.data(), e.inst.data(), mode,
+                           (1u << kSkinModeTree) | (1u << kSkinModeBuild)));
+    SkinLists sl{e.skinRows.data(), e.skinCount.data(), e.skinRadius.data(), e.skinCap, e.skinDist.data()};
+    SPHB_TRY(buildSkinLists(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy, e.box,
+                            np, e.p.nb_skin, sl, e.status.data(), st, e.views.data(), e.inst.data(), mode,
+                            1u << kSkinModeBuild));
+    SPHB_TRY(skinCommit(e.f[0].data(), e.f[1].data(), e.f[2].data(), n, e.skinXb.data(), e.skinYb.data(),
+                        e.skinZb.data(), e.skinBuild.data(), e.skinMoved.data(), ctl, st));
+    SPHB_CUDA_TRY(cudaMemsetAsync(e.skinGrid.data(), 0, size_t(kSkinCells) * size_t(e.num) * sizeof(unsigned), st));
+    SPHB_TRY(skinDisplacement(e.pos.data(), e.skinXb.data(), e.skinYb.data(), e.skinZb.data(), e.skinBuild.data(), n,
+                              e.box, e.skinGrid.data(), st, e.inst.data(), mode));
+    SkinFilterArgs a{};
+    a.pos  = e.pos.data();
+    a.posq = e.mixed ? e.posq.data() : nullptr;
+    FixedFrame fr  = fixedFrameOf(e.box);
+    double unitMax = 0;
+    for (int k = 0; k < 3; ++k)
+    {
+        a.qscale[k] = float(fr.unit[k]);
+        unitMax     = std::max(unitMax, fr.unit[k]);
+    }
+    a.qunit        = float(unitMax * (1.0 + 1e-6));
+    a.h            = e.f[3].data();
+    a.nc           = e.nc.data();
+    a.nidx         = e.nidx.data();
+    a.sl           = sl;
+    a.xb           = e.skinXb.data();
+    a.yb           = e.skinYb.data();
+    a.zb           = e.skinZb.data();
+    a.moved        = e.skinMoved.data();
+    a.dispGrid     = e.skinGrid.data();
+    a.groupD       = e.skinGroupD.data();
+    a.numWorklist  = ctl + kCtlDeferredA;
+    a.numWorklist2 = ctl + kCtlDeferredB;
+    a.worklist     = e.skinWork.data();
+    a.worklist2    = e.skinWork.data() + groups;
+    a.n            = n;
+    a.box          = e.box;
+    a.prm          = np;
+    a.inst         = e.inst.data();
+    a.gate         = mode;
+    SPHB_TRY(checkSkinGroups(a, st));
+    // the deferred counts stay zero unless the mode is the refilter, and then the listed searches see them
+    SPHB_TRY(findNeighborsListed(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy,
+                                 e.box, np, e.nidx.data(), e.nc.data(), e.status.data(), a.worklist, a.numWorklist, st,
+                                 e.views.data(), e.inst.data()));
+    SPHB_TRY(filterSkinLists(a, st));
+    return findNeighborsListed(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy,
+                               e.box, np, e.nidx.data(), e.nc.data(), e.status.data(), a.worklist2, a.numWorklist2,
+                               st, e.views.data(), e.inst.data());
+}
+
 //! one whole step for every instance, without host synchronisation (capturable)
 int stepBatched(sphb_ensemble& e)
 {
@@ -605,8 +718,13 @@ int stepBatched(sphb_ensemble& e)
     countLaunch();
     TreeView dummy{};
     NeighborParams np{e.p.ng0, e.p.ngmax, 10};
-    SPHB_TRY(findNeighbors(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy, e.box, np,
-                           e.nidx.data(), e.nc.data(), e.status.data(), st, e.views.data(), e.inst.data()));
+    if (e.skin) { SPHB_TRY(searchBatchedSkin(e, np)); }
+    else
+    {
+        SPHB_TRY(findNeighbors(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.pos.data(), e.f[3].data(), n, dummy,
+                               e.box, np, e.nidx.data(), e.nc.data(), e.status.data(), st, e.views.data(),
+                               e.inst.data()));
+    }
     if (e.mixed) { SPHB_TRY(runChainBatched<float>(e)); }
     else { SPHB_TRY(runChainBatched<double>(e)); }
     consBatchKernel<<<ceilDiv(n, 256), 256, 0, st>>>(n, e.inst.data(), e.f[0].data(), e.f[1].data(), e.f[2].data(),
@@ -807,7 +925,7 @@ extern "C" int sphb_ensemble_upload(sphb_ensemble* e, int k, const double* const
     SPHB_CUDA_TRY(cudaStreamSynchronize(e->stream));
     e->uploaded = true;
     e->synced   = false;
-    return SPHB_OK;
+    return resetSkin(*e);
 }
 
 extern "C" int sphb_ensemble_initial_sync(sphb_ensemble* e)
@@ -815,6 +933,7 @@ extern "C" int sphb_ensemble_initial_sync(sphb_ensemble* e)
     if (!e || !e->uploaded) { return e ? SPHB_ERR_STATE : SPHB_ERR_ARG; }
     SPHB_CUDA_TRY(cudaMemsetAsync(e->status.data(), 0, 4 * sizeof(unsigned), e->stream));
     initReduceKernel<<<ceilDiv(size_t(e->num), 64), 64, 0, e->stream>>>(e->num, e->reduce.data(), e->cons.data());
+    SPHB_TRY(resetSkin(*e));
     SPHB_TRY(syncBatched(*e, false));
     SPHB_TRY(rebuildTrees(*e));
     SPHB_TRY(checkStatus(*e));
@@ -925,6 +1044,22 @@ extern "C" int sphb_ensemble_autotune(sphb_ensemble* e, int* threads_out)
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
     if (threads_out) { std::copy(e->threads, e->threads + kJLoops, threads_out); }
     return dropGraph(*e);
+}
+
+extern "C" int sphb_ensemble_search_stats(sphb_ensemble* e, uint64_t* out)
+{
+    if (!e || !out) { return SPHB_ERR_ARG; }
+    unsigned ctl[kCtlWords] = {};
+    if (e->skin)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(ctl, e->skinCtl.data(), sizeof(ctl), cudaMemcpyDeviceToHost, e->stream));
+        SPHB_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    }
+    out[0] = ctl[kCtlTreeSearches];
+    out[1] = ctl[kCtlBuilds];
+    out[2] = ctl[kCtlFilterSteps];
+    out[3] = ctl[kCtlDeferredTotal] + ctl[kCtlDeferredA] + ctl[kCtlDeferredB];
+    return SPHB_OK;
 }
 
 extern "C" size_t sphb_ensemble_size(const sphb_ensemble* e, int k)

@@ -124,6 +124,8 @@ struct SearchExtras
     const unsigned* numListed;
     SkinLists sl;
     double onePlusSkin;
+    const unsigned* gate; // if set: the launch runs only when bit *gate of gateMask is set (a device-side mode)
+    unsigned gateMask;
 };
 
 template<bool kBatched, int kKind>
@@ -138,6 +140,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                                                                   const uint8_t* __restrict__ inst, SearchExtras ex)
 {
     __shared__ NbShared sh;
+    if (ex.gate && !((ex.gateMask >> __ldg(ex.gate)) & 1u)) { return; }
     const int warp         = threadIdx.x / kWarp;
     const int lane         = threadIdx.x & (kWarp - 1);
     const size_t numGroups = (n + kWarp - 1) / kWarp;
@@ -562,13 +565,16 @@ int computeBlockBoxes(const double* x, const double* y, const double* z, size_t 
 
 int findNeighbors(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
                   const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
-                  unsigned* status, cudaStream_t stream, const TreeView* views, const uint8_t* inst)
+                  unsigned* status, cudaStream_t stream, const TreeView* views, const uint8_t* inst,
+                  const unsigned* gate, unsigned gateMask)
 {
     if (n == 0) { return kOk; }
     if ((views == nullptr) != (inst == nullptr)) { return kErrArg; }
     size_t numGroups = (n + kWarp - 1) / kWarp;
     unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
     SearchExtras ex{};
+    ex.gate     = gate;
+    ex.gateMask = gateMask;
     if (views)
     {
         findNeighborsKernel<true, kSearchAll><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm,
@@ -586,17 +592,27 @@ int findNeighbors(const double* x, const double* y, const double* z, const doubl
 
 int findNeighborsListed(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
                         const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
-                        unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream)
+                        unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream,
+                        const TreeView* views, const uint8_t* inst)
 {
     if (n == 0) { return kOk; }
-    if (!groups || !numListed) { return kErrArg; }
+    if (!groups || !numListed || (views == nullptr) != (inst == nullptr)) { return kErrArg; }
     size_t numGroups = (n + kWarp - 1) / kWarp;
     unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
     SearchExtras ex{};
     ex.groups    = groups;
     ex.numListed = numListed;
-    findNeighborsKernel<false, kSearchListed><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box, prm,
-                                                                                 nidx, nc, status, nullptr, nullptr, ex);
+    if (views)
+    {
+        findNeighborsKernel<true, kSearchListed><<<blocks, kNbThreads, 0, stream>>>(x, y, z, pos, h, n, tree, box,
+                                                                                    prm, nidx, nc, status, views, inst,
+                                                                                    ex);
+    }
+    else
+    {
+        findNeighborsKernel<false, kSearchListed><<<blocks, kNbThreads, 0, stream>>>(
+            x, y, z, pos, h, n, tree, box, prm, nidx, nc, status, nullptr, nullptr, ex);
+    }
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -604,18 +620,32 @@ int findNeighborsListed(const double* x, const double* y, const double* z, const
 
 int buildSkinLists(const double* x, const double* y, const double* z, const double4* pos, const double* h, size_t n,
                    const TreeView& tree, const DevBox& box, NeighborParams prm, double skin, SkinLists sl,
-                   unsigned* status, cudaStream_t stream)
+                   unsigned* status, cudaStream_t stream, const TreeView* views, const uint8_t* inst,
+                   const unsigned* gate, unsigned gateMask)
 {
     if (n == 0) { return kOk; }
-    if (!(skin > 0.0) || sl.cap == 0 || sl.cap % kNbChunk != 0) { return kErrArg; }
+    if (!(skin > 0.0) || sl.cap == 0 || sl.cap % kNbChunk != 0 || (views == nullptr) != (inst == nullptr))
+    {
+        return kErrArg;
+    }
     size_t numGroups = (n + kWarp - 1) / kWarp;
     unsigned blocks  = unsigned((numGroups + kNbWarps - 1) / kNbWarps);
     SearchExtras ex{};
     ex.sl          = sl;
     ex.onePlusSkin = 1.0 + skin;
+    ex.gate        = gate;
+    ex.gateMask    = gateMask;
     // the kernel writes h only in the iterating kinds, never in this one
-    findNeighborsKernel<false, kSearchSkin><<<blocks, kNbThreads, 0, stream>>>(
-        x, y, z, pos, const_cast<double*>(h), n, tree, box, prm, nullptr, nullptr, status, nullptr, nullptr, ex);
+    if (views)
+    {
+        findNeighborsKernel<true, kSearchSkin><<<blocks, kNbThreads, 0, stream>>>(
+            x, y, z, pos, const_cast<double*>(h), n, tree, box, prm, nullptr, nullptr, status, views, inst, ex);
+    }
+    else
+    {
+        findNeighborsKernel<false, kSearchSkin><<<blocks, kNbThreads, 0, stream>>>(
+            x, y, z, pos, const_cast<double*>(h), n, tree, box, prm, nullptr, nullptr, status, nullptr, nullptr, ex);
+    }
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

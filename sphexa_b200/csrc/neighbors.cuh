@@ -93,26 +93,30 @@ struct SkinLists
 //! units of the quantised build distance per R_i
 constexpr double kSkinDistUnits = 65535.0;
 
-/*! Search all particles (x, y, z and the same coordinates packed as pos = (x, y, z, m)): updates h where the count left [ng0/4, ngmax+1], writes nc (count incl. self) and lists.
+/*! Search all particles (x, y, z and the same coordinates packed as pos = (x, y, z, m)): updates h where the count
+ *  left [ng0/4, ngmax+1], writes nc (count incl. self) and lists. With gate set, the launch does nothing unless bit
+ *  *gate of gateMask is set (a mode chosen on the device, for a captured graph).
  *  status[0] is set to a non-zero value if a per-warp buffer overflowed (the search then returns SPHB_ERR_CAPACITY).
  *  An ensemble passes views (one tree per instance, on the device) and inst (instance per slot, kGhost for
  *  padding): each group searches its instance's tree, padding slots are skipped. */
 int findNeighbors(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
                   const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
                   unsigned* status, cudaStream_t stream, const TreeView* views = nullptr,
-                  const uint8_t* inst = nullptr);
+                  const uint8_t* inst = nullptr, const unsigned* gate = nullptr, unsigned gateMask = 0);
 
 /*! The same search for the groups listed in groups[0 .. *numListed) only (a device count: the launch covers every
  *  group and the warps past the count return at once). */
 int findNeighborsListed(const double* x, const double* y, const double* z, const double4* pos, double* h, size_t n,
                         const TreeView& tree, const DevBox& box, NeighborParams prm, uint32_t* nidx, unsigned* nc,
-                        unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream);
+                        unsigned* status, const unsigned* groups, const unsigned* numListed, cudaStream_t stream,
+                        const TreeView* views = nullptr, const uint8_t* inst = nullptr);
 
 /*! Build the skin lists at the current positions and smoothing lengths: R_i = 2 h_i (1 + skin). Row i holds exactly
  *  the j != i whose FP64 minimum-image squared distance is below R_i * R_i, ascending. h is read only. */
 int buildSkinLists(const double* x, const double* y, const double* z, const double4* pos, const double* h, size_t n,
                    const TreeView& tree, const DevBox& box, NeighborParams prm, double skin, SkinLists sl,
-                   unsigned* status, cudaStream_t stream);
+                   unsigned* status, cudaStream_t stream, const TreeView* views = nullptr,
+                   const uint8_t* inst = nullptr, const unsigned* gate = nullptr, unsigned gateMask = 0);
 
 //! inputs of the per-step refilter of the skin lists (skin.cu)
 struct SkinFilterArgs
@@ -129,7 +133,8 @@ struct SkinFilterArgs
     const double* yb;
     const double* zb;
     const uint32_t* moved;   // bit i: index i holds another particle than at the build (null: none moved)
-    const unsigned* dispGrid; // per cell of a kSkinGrid^3 grid over the box: largest displacement (FP32 bits)
+    const unsigned* dispGrid; // per cell of a kSkinGrid^3 grid over the box: largest displacement (FP32 bits);
+                              // an ensemble: one grid per instance, instance k at dispGrid + k kSkinCells
     unsigned* groupD;         // per group: the check's result (D as FP32 bits, or all ones: deferred)
     unsigned* worklist;       // groups the check defers, for findNeighborsListed
     unsigned* numWorklist;
@@ -138,15 +143,43 @@ struct SkinFilterArgs
     size_t n;
     DevBox box;
     NeighborParams prm;
+    const uint8_t* inst;   // an ensemble: instance per slot (kGhost: padding, skipped), else null
+    const unsigned* gate;  // if set: the launch runs only when *gate == kSkinModeFilter
 };
 
-//! cells per axis of the displacement grid
-constexpr int kSkinGrid = 32;
+//! neighbour-stage modes of a simulation stepped without host reads (ensemble), chosen on the device
+enum SkinMode : unsigned
+{
+    kSkinModeTree   = 0, // tree search of every group, no rows
+    kSkinModeBuild  = 1, // tree search of every group and a build of the rows
+    kSkinModeFilter = 2  // refilter of the rows, tree search of the deferred groups
+};
+
+//! words of the device-side control block of skinDecide
+enum SkinCtl : int
+{
+    kCtlMode, kCtlValid, kCtlAge, kCtlHoldoff, kCtlDeferredA, kCtlDeferredB, kCtlGroups, kCtlDeferredTotal,
+    kCtlTreeSearches, kCtlBuilds, kCtlFilterSteps, kCtlWords
+};
+
+/*! Choose this step's mode into ctl[kCtlMode] from the previous step's deferred counts (ctl[kCtlDeferredA/B], which
+ *  the check and the filter increment as worklist counters and which this call resets). */
+int skinDecide(unsigned* ctl, cudaStream_t stream);
+
+//! in a build step (ctl[kCtlMode] == kSkinModeBuild): record build positions and the identity index map
+int skinCommit(const double* x, const double* y, const double* z, size_t n, double* xb, double* yb, double* zb,
+               uint32_t* buildOf, uint32_t* moved, unsigned* ctl, cudaStream_t stream);
+
+//! cells per axis of the displacement grid, and cells per grid (an ensemble has one grid per instance)
+constexpr int kSkinGrid  = 32;
+constexpr int kSkinCells = kSkinGrid * kSkinGrid * kSkinGrid;
 
 /*! Largest displacement since the build per cell of the grid (cells by current position). buildOf maps the current
- *  index to the build index (null: the identity). dispGrid must be zero on entry. */
+ *  index to the build index (null: the identity). dispGrid must be zero on entry. With inst (an ensemble), each
+ *  instance has its own grid (instance k at dispGrid + k kSkinCells): members do not interact. */
 int skinDisplacement(const double4* pos, const double* xb, const double* yb, const double* zb,
-                     const uint32_t* buildOf, size_t n, const DevBox& box, unsigned* dispGrid, cudaStream_t stream);
+                     const uint32_t* buildOf, size_t n, const DevBox& box, unsigned* dispGrid, cudaStream_t stream,
+                     const uint8_t* inst = nullptr, const unsigned* gate = nullptr);
 
 /*! After a sort that moved particles: buildNew[i] = buildOld[order[i]] (buildOld null: the identity) and bit i of
  *  moved = (buildNew[i] != i). */

@@ -23,6 +23,8 @@
 #include "neighbors.cuh"
 #include "primitives.cuh"
 
+#include <algorithm>
+
 namespace sphb
 {
 
@@ -95,10 +97,12 @@ __device__ inline int cellOf(double v, double lo, double ilen)
 __global__ void skinDisplacementKernel(const double4* __restrict__ pos, const double* __restrict__ xb,
                                        const double* __restrict__ yb, const double* __restrict__ zb,
                                        const uint32_t* __restrict__ buildOf, size_t n, DevBox box,
-                                       unsigned* __restrict__ grid)
+                                       unsigned* __restrict__ grid, const uint8_t* __restrict__ inst,
+                                       const unsigned* gate)
 {
+    if (gate && __ldg(gate) != kSkinModeFilter) { return; }
     size_t i   = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-    bool valid = i < n;
+    bool valid = i < n && !(inst && inst[i] == kGhost);
     unsigned bits = 0u;
     int cell      = -1;
     if (valid)
@@ -108,12 +112,15 @@ __global__ void skinDisplacementKernel(const double4* __restrict__ pos, const do
         double d  = displacement(p.x, p.y, p.z, xb[b], yb[b], zb[b], box);
         // rounded up, so that the grid bounds the FP64 value
         bits = __float_as_uint(__double2float_ru(d));
-        cell = (cellOf(p.x, box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(p.y, box.lo[1], box.ilen[1])) * kSkinGrid +
+        const int gridBase = inst ? int(inst[i]) * kSkinCells : 0;
+        cell = gridBase + (cellOf(p.x, box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(p.y, box.lo[1], box.ilen[1])) *
+                              kSkinGrid +
                cellOf(p.z, box.lo[2], box.ilen[2]);
         // The displacement also goes to the cell of the build position, which every group whose rows list this
         // particle checks: the refilter decides most entries from their build distance and these bounds. A particle
         // at another index than at the build makes those rows stale: infinite there.
-        int cb = (cellOf(xb[b], box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(yb[b], box.lo[1], box.ilen[1])) *
+        int cb = gridBase +
+                 (cellOf(xb[b], box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(yb[b], box.lo[1], box.ilen[1])) *
                      kSkinGrid +
                  cellOf(zb[b], box.lo[2], box.ilen[2]);
         unsigned atBuild = b != i ? __float_as_uint(INFINITY) : bits;
@@ -155,6 +162,8 @@ __device__ inline bool checkGroup(const SkinFilterArgs& a, int lane, bool valid,
                                   unsigned rowCount, double hi, size_t i, float* Dout)
 {
     bool ok = !valid || (rowCount <= a.sl.cap && !(a.moved && bitSet(a.moved, i)));
+    // an ensemble: the grid of the group's instance (the group's first slot is never padding)
+    const unsigned* grid = a.dispGrid + (a.inst ? size_t(a.inst[i - lane]) * kSkinCells : 0);
 
     // The largest displacement of any particle that can now be within R_i of a particle of the group. The region
     // also holds the build position of every particle in the group's rows (within R_i of the build position of i,
@@ -204,7 +213,7 @@ __device__ inline bool checkGroup(const SkinFilterArgs& a, int lane, bool valid,
             c[k] = c0[k] + q[k];
             if (a.box.periodic[k]) { c[k] = ((c[k] % kSkinGrid) + kSkinGrid) % kSkinGrid; }
         }
-        dmax = max(dmax, __ldg(a.dispGrid + (c[0] * kSkinGrid + c[1]) * kSkinGrid + c[2]));
+        dmax = max(dmax, __ldg(grid + (c[0] * kSkinGrid + c[1]) * kSkinGrid + c[2]));
     }
     const float D = __uint_as_float(warpMaxU(dmax));
     *Dout         = D;
@@ -220,9 +229,9 @@ __global__ void __launch_bounds__(kFilterThreads) skinCheckKernel(SkinFilterArgs
     const int lane         = threadIdx.x & (kWarp - 1);
     const size_t numGroups = (a.n + kWarp - 1) / kWarp;
     const size_t group     = size_t(blockIdx.x) * kFilterWarps + warp;
-    if (group >= numGroups) { return; }
+    if (group >= numGroups || (a.gate && __ldg(a.gate) != kSkinModeFilter)) { return; }
     const size_t i    = group * kWarp + lane;
-    const bool valid  = i < a.n;
+    const bool valid  = i < a.n && !(a.inst && a.inst[i] == kGhost);
     double4 pi        = valid ? loadPos(a.pos + i) : make_double4(0, 0, 0, 0);
     double hi         = valid ? a.h[i] : 0.0;
     double Ri         = valid ? a.sl.radius[i] : 0.0;
@@ -250,12 +259,12 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
     const int lane         = threadIdx.x & (kWarp - 1);
     const size_t numGroups = (a.n + kWarp - 1) / kWarp;
     const size_t group     = size_t(blockIdx.x) * kFilterWarps + warp;
-    if (group >= numGroups) { return; }
+    if (group >= numGroups || (a.gate && __ldg(a.gate) != kSkinModeFilter)) { return; }
     const unsigned gD = __ldg(a.groupD + group);
     if (gD == kDeferred) { return; }
     const double D   = double(__uint_as_float(gD));
     const size_t i   = group * kWarp + lane;
-    const bool valid = i < a.n;
+    const bool valid = i < a.n && !(a.inst && a.inst[i] == kGhost);
 
     double4 pi = valid ? loadPos(a.pos + i) : make_double4(0, 0, 0, 0);
     double hi  = valid ? a.h[i] : 0.0;
@@ -403,6 +412,66 @@ __global__ void __launch_bounds__(kFilterThreads) skinFilterKernel(SkinFilterArg
     }
 }
 
+/*! The row policy of a simulation stepped without host reads (an ensemble in a captured graph), on one thread: the
+ *  same rules as the host policy of a single simulation (rebuild when more than a tenth of the groups were deferred
+ *  in the previous step; rows rebuilt within three steps of the last build give way to 32 steps of tree searches). */
+__global__ void skinDecideKernel(unsigned* ctl)
+{
+    unsigned deferred = ctl[kCtlDeferredA] + ctl[kCtlDeferredB];
+    ctl[kCtlDeferredTotal] += deferred;
+    ctl[kCtlDeferredA] = 0;
+    ctl[kCtlDeferredB] = 0;
+    unsigned mode;
+    if (ctl[kCtlHoldoff] > 0)
+    {
+        --ctl[kCtlHoldoff];
+        ctl[kCtlValid] = 0;
+        mode           = kSkinModeTree;
+    }
+    else if (!ctl[kCtlValid]) { mode = kSkinModeBuild; }
+    else if (size_t(deferred) * 10 > size_t(ctl[kCtlGroups]))
+    {
+        if (ctl[kCtlAge] <= 3)
+        {
+            ctl[kCtlHoldoff] = 32;
+            ctl[kCtlValid]   = 0;
+            mode             = kSkinModeTree;
+        }
+        else { mode = kSkinModeBuild; }
+    }
+    else { mode = kSkinModeFilter; }
+    if (mode == kSkinModeFilter)
+    {
+        ++ctl[kCtlAge];
+        ++ctl[kCtlFilterSteps];
+    }
+    else { ++ctl[kCtlTreeSearches]; }
+    if (mode == kSkinModeBuild) { ++ctl[kCtlBuilds]; }
+    ctl[kCtlMode] = mode;
+}
+
+//! after a build: build positions = current positions, build index = current index, rows valid
+__global__ void skinCommitKernel(const double* __restrict__ x, const double* __restrict__ y,
+                                 const double* __restrict__ z, size_t n, double* xb, double* yb, double* zb,
+                                 uint32_t* buildOf, uint32_t* moved, unsigned* ctl)
+{
+    if (__ldg(ctl + kCtlMode) != kSkinModeBuild) { return; }
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i < n)
+    {
+        xb[i]      = x[i];
+        yb[i]      = y[i];
+        zb[i]      = z[i];
+        buildOf[i] = uint32_t(i);
+        if (i % kWarp == 0) { moved[i / kWarp] = 0u; }
+    }
+    if (i == 0)
+    {
+        ctl[kCtlValid] = 1;
+        ctl[kCtlAge]   = 0;
+    }
+}
+
 __global__ void idsDifferKernel(const uint64_t* __restrict__ a, const uint64_t* __restrict__ b, size_t n,
                                 unsigned* flag)
 {
@@ -423,11 +492,31 @@ int idsDiffer(const uint64_t* a, const uint64_t* b, size_t n, unsigned* flag, cu
     return kOk;
 }
 
+int skinDecide(unsigned* ctl, cudaStream_t stream)
+{
+    skinDecideKernel<<<1, 1, 0, stream>>>(ctl);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+int skinCommit(const double* x, const double* y, const double* z, size_t n, double* xb, double* yb, double* zb,
+               uint32_t* buildOf, uint32_t* moved, unsigned* ctl, cudaStream_t stream)
+{
+    skinCommitKernel<<<ceilDiv(std::max<size_t>(n, 1), 256), 256, 0, stream>>>(x, y, z, n, xb, yb, zb, buildOf, moved,
+                                                                               ctl);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
 int skinDisplacement(const double4* pos, const double* xb, const double* yb, const double* zb,
-                     const uint32_t* buildOf, size_t n, const DevBox& box, unsigned* dispGrid, cudaStream_t stream)
+                     const uint32_t* buildOf, size_t n, const DevBox& box, unsigned* dispGrid, cudaStream_t stream,
+                     const uint8_t* inst, const unsigned* gate)
 {
     if (n == 0) { return kOk; }
-    skinDisplacementKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(pos, xb, yb, zb, buildOf, n, box, dispGrid);
+    skinDisplacementKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(pos, xb, yb, zb, buildOf, n, box, dispGrid, inst,
+                                                                gate);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

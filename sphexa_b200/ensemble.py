@@ -71,6 +71,13 @@ class Ensemble:
     def stream(self):
         return self.lib.sphb_ensemble_stream(self.h)
 
+    def search_stats(self) -> dict:
+        """How the neighbour stage ran since the initial sync: tree searches of every group, skin-row builds, steps
+        served from the skin rows, and groups those steps deferred to the tree search."""
+        out = np.zeros(4, dtype=np.uint64)
+        L.check(self.lib.sphb_ensemble_search_stats(self.h, L.ptr(out)), "sphb_ensemble_search_stats")
+        return dict(zip(("tree_searches", "skin_builds", "skin_steps", "deferred_groups"), (int(v) for v in out)))
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.sphb_ensemble_destroy(self.h)

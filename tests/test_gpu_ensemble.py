@@ -60,3 +60,39 @@ def test_autotune_then_graph_steps(cuda_device):
             assert np.array_equal(ens.get(k, f), sim.get(f)), (k, f)
         sim.close()
     ens.close()
+
+
+def test_ensemble_skin_rows_match_tree_searches(cuda_device):
+    """The ensemble's skin rows (mode chosen on the device every replay of the captured step) against single
+    simulations that search the tree every step: identical states after 12 steps. One member has a stirred region,
+    so that some of its groups are deferred (each member has its own displacement grid, so the others are not) and
+    its particles change index between steps."""
+    import copy
+    from sphexa_b200.ensemble import Ensemble
+    from sphexa_b200.simulation import Simulation
+    ics = _ics()
+    rng = np.random.default_rng(9)
+    st = ics[1]
+    inside = np.sqrt(st["x"] ** 2 + st["y"] ** 2 + st["z"] ** 2) < 0.08
+    for k in ("vx", "vy", "vz"):
+        v = np.zeros_like(st["x"])
+        v[inside] = rng.uniform(-20.0, 20.0, inside.sum())
+        st[k] = v
+    st["params"] = dict(st["params"], minDt=1e-4, minDt_m1=1e-4)
+    steps = 12
+    ens = Ensemble(ics, "mixed")
+    assert ens.step(steps, graph=True) == 0
+    stats = ens.search_stats()
+    assert stats["skin_steps"] >= 5 and stats["deferred_groups"] > 0, stats
+    for k, ic in enumerate(ics):
+        plain = copy.deepcopy(ic)
+        plain["params"]["nbSkin"] = 0.0
+        sim = Simulation(plain, "mixed")
+        for _ in range(steps):
+            sim.step()
+        assert sim.search_stats()["skin_steps"] == 0
+        for f in FIELDS:
+            assert np.array_equal(ens.get(k, f), sim.get(f)), (k, f)
+        sim.close()
+    ens.close()
+    print(stats)
