@@ -299,8 +299,10 @@ __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArra
  *  f_a tA_b with f = (v_j - v_i) xm_j and tA = -(C_i r) W, i.e. dV_ab = -sum_c C_bc M_ac with
  *  M_ac = sum_j f_a r_c W: M is accumulated in the same pass as tau, and C_i, known only after the pass, is applied
  *  to the nine sums at the end. Same quantities, one gather of each neighbour instead of two. */
+// at most 80 registers (three 256-thread blocks per SM), as MomentumEnergy: measured 1.04 -> 0.95 ms at 128^3 against
+// 87 registers
 template<int kMode>
-__global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvFusedKernel(ChainArrays<float> a,
+__global__ void __launch_bounds__(kChainMaxThreads, 3) iadDivvCurlvFusedKernel(ChainArrays<float> a,
                                                                               HydroConsts<float> k, DevBox box)
 {
     using T = float;
@@ -552,8 +554,11 @@ __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays
 // artificial_viscosity sph/include/sph/kernels.hpp:71-85) with the Courant time step per particle
 // (tsKCourant, kernels.hpp:10-17) reduced to the minimum.
 // ---------------------------------------------------------------------------------------------------------------
+// FP32 without AV cleaning: at most 80 registers (three 256-thread blocks per SM) keeps more warps resident for the
+// gathers; measured 2.11 -> 2.05 ms at 128^3 against 96 registers (the AV-cleaning form would spill)
 template<class T, int kMode>
-__global__ void __launch_bounds__(kChainMaxThreads) momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode & kModeAvClean)) ? 3 : 1)
+    momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
     bool valid   = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
