@@ -163,6 +163,40 @@ int sphb_sim_integrate(sphb_sim* sim);
 /*! compute_forces + integrate. */
 int sphb_sim_step(sphb_sim* sim);
 
+/* The force computation one stage at a time, for a caller that runs its own code between the stages as the
+ * reference's propagator does (HydroVeProp::computeForces, ve_hydro.hpp:126-203, exchanges halos between them).
+ * sphb_sim_compute_forces runs exactly these eight calls. Each stage must follow the previous one of the same force
+ * computation (else SPHB_ERR_STATE); sphb_sim_sync may start a new one at any time, and sphb_sim_integrate needs
+ * sphb_sim_conserved to have completed. */
+
+/*! Domain::sync (cstone/domain/domain.hpp:165-213): box, keys, sort, gather, trees, packed positions. */
+int sphb_sim_sync(sphb_sim* sim);
+
+/*! The neighbour search with the smoothing-length iteration (sph/include/sph/find_neighbors.hpp:10-41; GPU:
+ *  computeXMass's traversal, sph/include/sph/hydro_ve/xmass_gpu.cu:78-92). */
+int sphb_sim_find_neighbors(sphb_sim* sim);
+
+/*! sph::gpu::computeXMass (sph/include/sph/hydro_ve/xmass_gpu.cu, xmass_kern.hpp:50-79). */
+int sphb_sim_xmass(sphb_sim* sim);
+
+/*! sph::gpu::computeVeDefGradh + computeEOS (ve_def_gradh_kern.hpp:43-90, hydro_ve/eos.hpp:52-94). */
+int sphb_sim_ve_def_gradh_eos(sphb_sim* sim);
+
+/*! sph::gpu::computeIadDivvCurlv (iad_kern.hpp:43-110, divv_curlv_kern.hpp:43-123). */
+int sphb_sim_iad_divv_curlv(sphb_sim* sim);
+
+/*! sph::gpu::computeAVswitches (av_switches_kern.hpp:43-137); uses the current minDt. */
+int sphb_sim_av_switches(sphb_sim* sim);
+
+/*! sph::gpu::computeMomentumEnergy (momentum_energy_kern.hpp:65-222). If min_dt_courant is not NULL it receives
+ *  the minimum Courant time step (momentum_energy_gpu.cu:109-116), which costs one device synchronisation. */
+int sphb_sim_momentum_energy(sphb_sim* sim, double* min_dt_courant);
+
+/*! computeConservedQuantities (conserved_quantities.hpp:117-175) and the time-step reductions; completes the force
+ *  computation. If out is not NULL it receives {kinetic energy, internal energy, total energy, |linear momentum|,
+ *  |angular momentum|}. */
+int sphb_sim_conserved(sphb_sim* sim, double* out);
+
 /*! Number of owned particles. */
 size_t sphb_sim_size(const sphb_sim* sim);
 

@@ -43,6 +43,7 @@ enum Status : int
     kErrCuda       = SPHB_ERR_CUDA,
     kErrCapacity   = SPHB_ERR_CAPACITY,
     kErrNotConverged = SPHB_ERR_NOT_CONVERGED,
+    kErrState        = SPHB_ERR_STATE,
 };
 
 #define SPHB_CUDA_TRY(expr)                                                                                            \

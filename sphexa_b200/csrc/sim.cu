@@ -90,6 +90,7 @@ struct sphb_sim
     uint64_t iteration{1};
     bool uploaded{false};
     bool forcesDone{false};
+    int nextStage{0}; // the stage of the force computation that may run next (StageOrder), 0 = the domain sync
 
     // fixed time step (> 0) instead of computeTimestep; required by the step adjoint
     double fixedDt{0};
@@ -416,26 +417,26 @@ HydroConsts<T> hydroConsts(const sphb_sim& s)
 }
 
 template<class T>
-int runChain(sphb_sim& s)
+int runChainStage(sphb_sim& s, int stage)
 {
-    cudaStream_t st     = s.stream;
-    ChainArrays<T> a    = chainArrays<T>(s);
-    HydroConsts<T> k    = hydroConsts<T>(s);
-    SPHB_TRY(launchXMass(a, k, s.box, st));
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sVeDefGradh], st));
-    SPHB_TRY(launchVeDefGradhEos(a, k, s.box, st));
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIad], st));
-    SPHB_TRY(launchIadDivvCurlv(a, k, s.box, st));
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sAV], st));
-    if (s.taping)
+    cudaStream_t st  = s.stream;
+    ChainArrays<T> a = chainArrays<T>(s);
+    HydroConsts<T> k = hydroConsts<T>(s);
+    switch (stage)
     {
-        SPHB_CUDA_TRY(cudaMemcpyAsync(s.alphaPre.data(), s.f[fAlpha].data(), s.n * sizeof(double),
-                                      cudaMemcpyDeviceToDevice, st));
+    case sXMass: return launchXMass(a, k, s.box, st);
+    case sVeDefGradh: return launchVeDefGradhEos(a, k, s.box, st);
+    case sIad: return launchIadDivvCurlv(a, k, s.box, st);
+    case sAV:
+        if (s.taping)
+        {
+            SPHB_CUDA_TRY(cudaMemcpyAsync(s.alphaPre.data(), s.f[fAlpha].data(), s.n * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, st));
+        }
+        return launchAVswitches(a, k, s.box, s.minDt, st);
+    case sMomentum: return launchMomentumEnergy(a, k, s.box, st);
+    default: return kErrArg;
     }
-    SPHB_TRY(launchAVswitches(a, k, s.box, s.minDt, st));
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sMomentum], st));
-    SPHB_TRY(launchMomentumEnergy(a, k, s.box, st));
-    return kOk;
 }
 
 TreeView treeView(sphb_sim& s)
@@ -588,29 +589,38 @@ int searchNeighbors(sphb_sim& s)
                                st);
 }
 
-int computeForces(sphb_sim& s)
+/*! One stage of HydroVeProp::computeForces (ve_hydro.hpp:126-203), in the reference's order: the domain sync, the
+ *  neighbour search with the h iteration, XMass, VeDefGradh + EOS, IAD + divv/curlv, AV switches, MomentumEnergy, and
+ *  the conserved sums with the time-step reductions (which complete the force computation). Each stage records the
+ *  CUDA event that starts its stage time. */
+int runStage(sphb_sim& s, int stage)
 {
     cudaStream_t st = s.stream;
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sSync], st));
-    SPHB_TRY(syncDomain(s));
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sNeighbors], st));
-    if (s.taping)
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[stage], st));
+    switch (stage)
     {
-        SPHB_CUDA_TRY(cudaMemcpyAsync(s.hPre.data(), s.f[fH].data(), s.n * sizeof(double), cudaMemcpyDeviceToDevice,
-                                      st));
+    case sSync: return syncDomain(s);
+    case sNeighbors:
+    {
+        if (s.taping)
+        {
+            SPHB_CUDA_TRY(cudaMemcpyAsync(s.hPre.data(), s.f[fH].data(), s.n * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, st));
+        }
+        unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
+        SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
+        return searchNeighbors(s);
+    }
+    case sXMass:
+    case sVeDefGradh:
+    case sIad:
+    case sAV:
+    case sMomentum: return s.mixed ? runChainStage<float>(s, stage) : runChainStage<double>(s, stage);
+    case sConserved: break;
+    default: return kErrArg;
     }
 
-    unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
-    SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
-    SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
-
-    SPHB_TRY(searchNeighbors(s));
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
-
-    if (s.mixed) { SPHB_TRY(runChain<float>(s)); }
-    else { SPHB_TRY(runChain<double>(s)); }
-
-    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sConserved], st));
     double cv = idealGasCv(s.p.mui, s.p.gamma);
     SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
                            s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
@@ -642,6 +652,28 @@ int computeForces(sphb_sim& s)
     s.angmom       = std::sqrt(cons[5] * cons[5] + cons[6] * cons[6] + cons[7] * cons[7]);
     s.totalNeighbors = cons[8];
     s.forcesDone     = true;
+    return kOk;
+}
+
+/*! The stage ABI's ordering rule: stage k runs only after stage k-1 of the same force computation (the sync after
+ *  the previous integration, or at any time to start over). A failed stage leaves the computation to restart. */
+int runStageChecked(sphb_sim& s, int stage)
+{
+    if (stage != sSync && stage != s.nextStage) { return kErrState; }
+    s.forcesDone = false;
+    s.nextStage  = sSync;
+    int rc       = runStage(s, stage);
+    if (rc != kOk) { return rc; }
+    s.nextStage = stage == sConserved ? int(sSync) : stage + 1;
+    return kOk;
+}
+
+int computeForces(sphb_sim& s)
+{
+    for (int stage = sSync; stage <= sConserved; ++stage)
+    {
+        SPHB_TRY(runStageChecked(s, stage));
+    }
     return kOk;
 }
 
@@ -899,6 +931,7 @@ extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const u
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
     s->boxFirstCall = true;
     s->skinValid    = false;
+    s->nextStage    = sSync;
     s->minDt        = s->p.minDt;
     s->minDt_m1     = s->p.minDt_m1;
     s->ttot         = 0;
@@ -937,6 +970,45 @@ extern "C" int sphb_sim_step(sphb_sim* s)
     int rc = sphb_sim_compute_forces(s);
     if (rc != SPHB_OK) { return rc; }
     return sphb_sim_integrate(s);
+}
+
+namespace
+{
+
+int stageEntry(sphb_sim* s, int stage)
+{
+    if (!s) { return SPHB_ERR_ARG; }
+    if (!s->uploaded) { return SPHB_ERR_STATE; }
+    return runStageChecked(*s, stage);
+}
+
+} // namespace
+
+extern "C" int sphb_sim_sync(sphb_sim* s) { return stageEntry(s, sSync); }
+extern "C" int sphb_sim_find_neighbors(sphb_sim* s) { return stageEntry(s, sNeighbors); }
+extern "C" int sphb_sim_xmass(sphb_sim* s) { return stageEntry(s, sXMass); }
+extern "C" int sphb_sim_ve_def_gradh_eos(sphb_sim* s) { return stageEntry(s, sVeDefGradh); }
+extern "C" int sphb_sim_iad_divv_curlv(sphb_sim* s) { return stageEntry(s, sIad); }
+extern "C" int sphb_sim_av_switches(sphb_sim* s) { return stageEntry(s, sAV); }
+
+extern "C" int sphb_sim_momentum_energy(sphb_sim* s, double* min_dt_courant)
+{
+    int rc = stageEntry(s, sMomentum);
+    if (rc != SPHB_OK || !min_dt_courant) { return rc; }
+    unsigned long long bits = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&bits, s->reduce.data() + 1, sizeof(bits), cudaMemcpyDeviceToHost, s->stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    *min_dt_courant = fromOrderedBits(bits);
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_conserved(sphb_sim* s, double* out)
+{
+    int rc = stageEntry(s, sConserved);
+    if (rc != SPHB_OK || !out) { return rc; }
+    double v[5] = {s->ecin, s->eint, s->etot, s->linmom, s->angmom};
+    std::memcpy(out, v, sizeof(v));
+    return SPHB_OK;
 }
 
 extern "C" size_t sphb_sim_size(const sphb_sim* s) { return s ? s->n : 0; }

@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsphb200.so")
 
 SPHB_OK = 0
+SPHB_ERR_ARG, SPHB_ERR_CUDA, SPHB_ERR_CAPACITY, SPHB_ERR_NOT_CONVERGED, SPHB_ERR_STATE = 1, 2, 3, 4, 5
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "capacity exhausted", 4: "smoothing length not converged",
           5: "call out of order"}
 SPHB_FP64 = 0
@@ -42,7 +43,9 @@ class Params(C.Structure):
 EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sphb_sort_by_key_scratch_bytes",
             "sphb_sort_by_key", "sphb_gather8", "sphb_compute_octree", "sphb_sim_create", "sphb_sim_destroy",
             "sphb_sim_upload", "sphb_sim_initial_sync", "sphb_sim_compute_forces", "sphb_sim_integrate",
-            "sphb_sim_step", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
+            "sphb_sim_step", "sphb_sim_sync", "sphb_sim_find_neighbors", "sphb_sim_xmass",
+            "sphb_sim_ve_def_gradh_eos", "sphb_sim_iad_divv_curlv", "sphb_sim_av_switches", "sphb_sim_momentum_energy",
+            "sphb_sim_conserved", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
             "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches",
             "sphb_sim_search_stats",
             "sphb_sim_stream", "sphb_sim_load_state", "sphb_sim_store_state", "sphb_probe_fma_peak",
@@ -79,6 +82,14 @@ def load() -> C.CDLL:
         "sphb_sim_compute_forces": (C.c_int, [P]),
         "sphb_sim_integrate": (C.c_int, [P]),
         "sphb_sim_step": (C.c_int, [P]),
+        "sphb_sim_sync": (C.c_int, [P]),
+        "sphb_sim_find_neighbors": (C.c_int, [P]),
+        "sphb_sim_xmass": (C.c_int, [P]),
+        "sphb_sim_ve_def_gradh_eos": (C.c_int, [P]),
+        "sphb_sim_iad_divv_curlv": (C.c_int, [P]),
+        "sphb_sim_av_switches": (C.c_int, [P]),
+        "sphb_sim_momentum_energy": (C.c_int, [P, P]),
+        "sphb_sim_conserved": (C.c_int, [P, P]),
         "sphb_sim_size": (S, [P]),
         "sphb_sim_get_field": (C.c_int, [P, C.c_char_p, P, C.c_int]),
         "sphb_sim_set_field": (C.c_int, [P, C.c_char_p, P, C.c_int]),

@@ -57,6 +57,36 @@ class Simulation:
     def compute_forces(self):
         L.check(self.lib.sphb_sim_compute_forces(self.h), "sphb_sim_compute_forces")
 
+    # the force computation one stage at a time (HydroVeProp::computeForces order)
+    def sync(self):
+        L.check(self.lib.sphb_sim_sync(self.h), "sphb_sim_sync")
+
+    def find_neighbors(self):
+        L.check(self.lib.sphb_sim_find_neighbors(self.h), "sphb_sim_find_neighbors")
+
+    def xmass(self):
+        L.check(self.lib.sphb_sim_xmass(self.h), "sphb_sim_xmass")
+
+    def ve_def_gradh_eos(self):
+        L.check(self.lib.sphb_sim_ve_def_gradh_eos(self.h), "sphb_sim_ve_def_gradh_eos")
+
+    def iad_divv_curlv(self):
+        L.check(self.lib.sphb_sim_iad_divv_curlv(self.h), "sphb_sim_iad_divv_curlv")
+
+    def av_switches(self):
+        L.check(self.lib.sphb_sim_av_switches(self.h), "sphb_sim_av_switches")
+
+    def momentum_energy(self) -> float:
+        """Returns the minimum Courant time step of the particles."""
+        dt = C.c_double()
+        L.check(self.lib.sphb_sim_momentum_energy(self.h, C.byref(dt)), "sphb_sim_momentum_energy")
+        return dt.value
+
+    def conserved(self) -> dict:
+        out = np.empty(5)
+        L.check(self.lib.sphb_sim_conserved(self.h, L.ptr(out)), "sphb_sim_conserved")
+        return dict(zip(("ecin", "eint", "etot", "linmom", "angmom"), out.tolist()))
+
     def integrate(self) -> int:
         rc = self.lib.sphb_sim_integrate(self.h)
         if rc not in (L.SPHB_OK, 4):

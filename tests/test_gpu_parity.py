@@ -323,6 +323,43 @@ def test_clump_over_ngmax_vs_reference(lib, ref, precision):
         assert np.array_equal(nbg[i, :k], nbr[i, :k]), i
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_stage_calls_match_compute_forces(lib, precision):
+    """The force computation called one stage at a time through the C ABI gives the same state, bit for bit, as
+    sphb_sim_compute_forces; a stage out of order is refused with SPHB_ERR_STATE and leaves the state usable."""
+    from sphexa_b200 import ic as icm
+    from sphexa_b200 import lib as L
+    from sphexa_b200.ic import CONSERVED_FIELDS
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(20)
+    a = Simulation(ic, precision)
+    b = Simulation(ic, precision)
+    for step in range(3):
+        a.compute_forces()
+        b.sync()
+        with pytest.raises(L.SphbError) as err:
+            b.xmass()
+        assert err.value.code == L.SPHB_ERR_STATE
+        b.sync()
+        b.find_neighbors()
+        b.xmass()
+        b.ve_def_gradh_eos()
+        b.iad_divv_curlv()
+        b.av_switches()
+        dt = b.momentum_energy()
+        cons = b.conserved()
+        sa = a.scalars()
+        assert dt == sa["minDtCourant"] and cons["etot"] == sa["etot"], step
+        for f in ("nc", "xm", "kx", "divv", "alpha", "ax", "du"):
+            assert np.array_equal(a.get(f), b.get(f)), (step, f)
+        a.integrate()
+        b.integrate()
+    for f in CONSERVED_FIELDS:
+        assert np.array_equal(a.get(f), b.get(f)), f
+    with pytest.raises(L.SphbError):
+        b.integrate()  # the next force computation has not run
+
+
 def test_zero_length_calls(lib):
     import torch
     from sphexa_b200 import lib as L
