@@ -33,19 +33,11 @@ __host__ __device__ inline uint64_t hilbertKey(unsigned px, unsigned py, unsigne
         py ^= 0u - ((xi & (yi | zi)) | (yi & nz));
         pz ^= 0u - ((xi & ny & nz) | (yi & nz));
 
-        if (zi)
-        {
-            unsigned t = px;
-            px         = py;
-            py         = pz;
-            pz         = t;
-        }
-        else if (!yi)
-        {
-            unsigned t = px;
-            px         = pz;
-            pz         = t;
-        }
+        // permute: zi rotates (x, y, z) -> (y, z, x); otherwise !yi swaps x and z (selects, no divergent branch)
+        unsigned t0 = px, t1 = py, t2 = pz;
+        px          = zi ? t1 : (yi ? t0 : t2);
+        py          = zi ? t2 : t1;
+        pz          = zi ? t0 : (yi ? t2 : t0);
     }
     return key;
 }

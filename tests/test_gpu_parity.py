@@ -151,9 +151,14 @@ def test_sedov_multi_step_fp64_vs_reference(lib, ref):
     ic = icm.sedov(20)
     r = ref.RefSim(ic)
     g = Simulation(ic, "fp64")
-    for _ in range(5):
+    for step in range(5):
         r.step()
         g.step()
+        # the cornerstone trees evolve as the reference's, step by step (including steps whose rebalance keeps every
+        # leaf and skips the rebuild)
+        lr, cr, yr = r.tree()
+        lg, cg, yg = g.tree()
+        assert np.array_equal(lg, lr) and np.array_equal(cg, cr) and np.array_equal(yg, yr), step
     sr, sg = r.scalars(), g.scalars()
     assert abs(sg["minDt"] - sr["minDt"]) <= 1e-9 * sr["minDt"]
     assert abs(sg["etot"] - sr["etot"]) <= 1e-9 * abs(sr["etot"])

@@ -44,13 +44,15 @@ def _run(a, b, steps):
     assert a.scalars()["ttot"] == b.scalars()["ttot"]
 
 
-def _stirred(side, seed=3, radius=0.15, speed=20.0):
-    """Sedov lattice with random velocities inside a sphere around the centre: particles there cross each other
-    (indices change between steps) while the rest is at rest."""
+def _stirred(side, seed=3, radius=0.15, speed=20.0, centre=(0.0, 0.0, 0.0)):
+    """Sedov lattice with random velocities inside a sphere (minimum image around `centre`): particles there cross
+    each other (indices change between steps) while the rest is at rest."""
     from sphexa_b200 import ic as icm
     ic = icm.sedov(side, seed=seed)
     rng = np.random.default_rng(seed)
-    r = np.sqrt(ic["x"] ** 2 + ic["y"] ** 2 + ic["z"] ** 2)
+    d = [ic[k] - c for k, c in zip(("x", "y", "z"), centre)]
+    d = [v - np.round(v) for v in d]
+    r = np.sqrt(d[0] ** 2 + d[1] ** 2 + d[2] ** 2)
     inside = r < radius
     for k in ("vx", "vy", "vz"):
         v = np.zeros_like(r)
@@ -80,6 +82,16 @@ def test_skin_stirred(cuda_device, precision):
     st = a.search_stats()
     print(st)
     assert st["skin_steps"] >= 5 and st["deferred_groups"] > 0 and st["remapped_syncs"] > 0, st
+
+
+def test_skin_stirred_across_the_periodic_boundary(cuda_device):
+    """The stirred region sits on the corner of the periodic box: displacements, grid cells and the region of each
+    group wrap around."""
+    a, b = _pair(_stirred(40, radius=0.08, centre=(0.5, 0.5, 0.5)), "mixed")
+    _run(a, b, 16)
+    st = a.search_stats()
+    print(st)
+    assert st["skin_steps"] >= 5 and st["deferred_groups"] > 0, st
 
 
 def test_skin_stirred_wide(cuda_device):
