@@ -591,6 +591,8 @@ def ensemble_leg(num=64, steps=20) -> dict:
     torch.cuda.synchronize()
     t_ens = time.perf_counter() - t0
     launches = None
+    stage_ms = {k: round(v, 4) for k, v in ens.stage_times().items()}  # the last step
+    search = ens.search_stats()
     finals = {k: ens.get(k, "x") for k in (0, num - 1)}
     ens.close()
 
@@ -611,7 +613,7 @@ def ensemble_leg(num=64, steps=20) -> dict:
                         f"total, blast energy U[0.5,2], gamma in {{1.4, 5/3}}, {steps} steps, mixed precision",
             "instances": num, "particles": total, "steps": steps,
             "ensemble": {"seconds": t_ens, "particle_steps_per_s": total * steps / t_ens, "status": rc,
-                         "autotuned_threads": choice},
+                         "autotuned_threads": choice, "stage_ms_last_step": stage_ms, "neighbor_search": search},
             "sequential": {"seconds": t_seq, "particle_steps_per_s": total * steps / t_seq},
             "speedup": t_seq / t_ens, "first_and_last_member_bit_identical": same}
 

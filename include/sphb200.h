@@ -323,6 +323,11 @@ int sphb_ensemble_autotune(sphb_ensemble* ens, int* threads5_out);
 /*! Advance every instance by steps steps; use_graph != 0 replays one captured step (captured on first use). */
 int sphb_ensemble_step(sphb_ensemble* ens, int steps, int use_graph);
 
+/*! Stage times in ms of the last step (9 floats: sync, neighbours, XMass, VeDefGradh + EOS, IAD + divv/curlv, AV
+ *  switches, MomentumEnergy, conserved sums, integration), from CUDA events recorded inside the step. Waits for the
+ *  stream. SPHB_ERR_STATE before the first step. No counterpart in the reference. */
+int sphb_ensemble_stage_times(sphb_ensemble* ens, float* out);
+
 /*! How the neighbour stage ran since the last upload or initial sync (the mode of each step is chosen on the
  *  device from the skin rows' state, sphb_params.nb_skin of the first instance): out[0] tree searches of every group,
  *  out[1] skin-row builds (each also counted in out[0]), out[2] steps served by refiltering the rows, out[3] groups

@@ -124,6 +124,10 @@ struct sphb_ensemble
     DeviceBuffer<uint32_t> skinBuild, skinBuildTmp, skinMoved;
     DeviceBuffer<unsigned> skinGrid, skinWork, skinGroupD, skinCtl;
 
+    // stage times of the last step (same stages as a single simulation's, sim.cu), recorded inside the graph
+    static constexpr int kStages = 9;
+    cudaEvent_t ev[kStages + 1]{};
+
     int threads[kJLoops]{128, 128, 128, 128, 128};
     cudaGraphExec_t graph{nullptr};
     bool uploaded{false};
@@ -197,44 +201,66 @@ __global__ void initReduceKernel(int num, unsigned long long* reduce, double* co
     }
 }
 
-//! per-instance sums of eKin, eInt, P, L, nc (conserved_quantities.hpp:117-175): warp sums, one atomic per warp
+//! warps of the per-instance sums below: a few per SM, each over a contiguous run of 32-slot chunks
+constexpr int kConsWarps = 148 * 16;
+
+/*! Per-instance sums of eKin, eInt, P, L, nc (conserved_quantities.hpp:117-175). Each warp walks a contiguous run
+ *  of 32-slot chunks (a chunk never spans two instances), keeps per-lane sums and adds them to the instance's slots
+ *  with one atomic per component when the instance changes or the run ends: about (warps + instances) x 9 atomics
+ *  per step instead of one set per warp of particles. */
 __global__ void consBatchKernel(size_t n, const uint8_t* __restrict__ inst, const double* x, const double* y,
                                 const double* z, const double* vx, const double* vy, const double* vz,
                                 const double* m, const double* temp, const unsigned* nc, const double* cv,
                                 double* cons)
 {
-    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
-    double acc[kNumCons] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    uint8_t q            = kGhost;
-    if (i < n) { q = inst[i]; }
-    if (q != kGhost)
+    const int lane          = threadIdx.x & 31;
+    const size_t numChunks  = (n + 31) / 32;
+    const size_t warpId     = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) / 32;
+    const size_t numWarps   = size_t(gridDim.x) * blockDim.x / 32;
+    const size_t perWarp    = (numChunks + numWarps - 1) / numWarps;
+    const size_t c0         = warpId * perWarp;
+    const size_t c1         = min(numChunks, c0 + perWarp);
+    double acc[kNumCons]    = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    uint8_t cur             = kGhost;
+    auto flush = [&]() {
+#pragma unroll
+        for (int c = 0; c < kNumCons; ++c)
+        {
+            double v = acc[c];
+            for (int o = 16; o > 0; o >>= 1)
+            {
+                v += __shfl_xor_sync(0xffffffffu, v, o);
+            }
+            if (lane == 0 && cur != kGhost) { atomicAdd(cons + kNumCons * cur + c, v); }
+            acc[c] = 0.0;
+        }
+    };
+    for (size_t c = c0; c < c1; ++c)
     {
+        // the chunk's instance: its first slot (never padding when the chunk holds any particle)
+        uint8_t cq = inst[c * 32];
+        if (cq != cur)
+        {
+            flush();
+            cur = cq;
+        }
+        size_t i  = c * 32 + lane;
+        uint8_t q = i < n ? inst[i] : kGhost;
+        if (q == kGhost) { continue; }
         double mi   = m[i];
         double X[3] = {x[i], y[i], z[i]};
         double V[3] = {vx[i], vy[i], vz[i]};
-        acc[0]      = mi * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
-        acc[1]      = cv[q] * temp[i] * mi;
-        acc[2]      = mi * V[0];
-        acc[3]      = mi * V[1];
-        acc[4]      = mi * V[2];
-        acc[5]      = mi * (X[1] * V[2] - X[2] * V[1]);
-        acc[6]      = mi * (X[2] * V[0] - X[0] * V[2]);
-        acc[7]      = mi * (X[0] * V[1] - X[1] * V[0]);
-        acc[8]      = double(nc[i]);
+        acc[0] += mi * (V[0] * V[0] + V[1] * V[1] + V[2] * V[2]);
+        acc[1] += cv[q] * temp[i] * mi;
+        acc[2] += mi * V[0];
+        acc[3] += mi * V[1];
+        acc[4] += mi * V[2];
+        acc[5] += mi * (X[1] * V[2] - X[2] * V[1]);
+        acc[6] += mi * (X[2] * V[0] - X[0] * V[2]);
+        acc[7] += mi * (X[0] * V[1] - X[1] * V[0]);
+        acc[8] += double(nc[i]);
     }
-    // the warp's instance: its first slot (never padding when the warp holds any particle)
-    size_t first = blockIdx.x * size_t(blockDim.x) + (threadIdx.x & ~31u);
-    uint8_t wq   = first < n ? inst[first] : kGhost;
-#pragma unroll
-    for (int c = 0; c < kNumCons; ++c)
-    {
-        double v = acc[c];
-        for (int o = 16; o > 0; o >>= 1)
-        {
-            v += __shfl_xor_sync(0xffffffffu, v, o);
-        }
-        if ((threadIdx.x & 31) == 0 && wq != kGhost) { atomicAdd(cons + kNumCons * wq + c, v); }
-    }
+    flush();
 }
 
 __global__ void orFlagsKernel(const unsigned* src, unsigned* dst, int count)
@@ -297,6 +323,10 @@ int allocate(sphb_ensemble& e)
     SPHB_TRY(e.status.reserve(4));
     SPHB_TRY(e.views.reserve(m));
     SPHB_TRY(e.leafDescs.reserve(m));
+    for (auto& ev : e.ev)
+    {
+        SPHB_CUDA_TRY(cudaEventCreate(&ev));
+    }
     e.skin = e.p.nb_skin > 0.0;
     if (e.skin)
     {
@@ -423,10 +453,8 @@ int syncBatched(sphb_ensemble& e, bool withLayout)
         countLaunch();
         SPHB_CUDA_TRY(cudaGetLastError());
     }
-    SPHB_TRY(packPositions(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.f[4].data(), n, e.pos.data(),
-                           e.mixed ? e.posq.data() : nullptr, e.box, st));
-    SPHB_TRY(computeBlockBoxes(e.f[0].data(), e.f[1].data(), e.f[2].data(), n, e.box, e.blockLo.data(),
-                               e.blockHi.data(), st));
+    SPHB_TRY(packPositionsAndBoxes(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.f[4].data(), n, e.pos.data(),
+                                   e.mixed ? e.posq.data() : nullptr, e.box, e.blockLo.data(), e.blockHi.data(), st));
     return kOk;
 }
 
@@ -580,6 +608,16 @@ HydroConsts<T> constsOf(const sphb_ensemble& e)
 }
 
 //! the J-loops in chain order with the tuned block sizes; which < 0: all, else only that one
+//! record the event that starts a stage time; inside a stream capture it becomes an event-record node of the graph
+cudaError_t stageMark(sphb_ensemble& e, int k)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t err            = cudaStreamIsCapturing(e.stream, &cs);
+    if (err != cudaSuccess) { return err; }
+    return cs == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(e.ev[k], e.stream, cudaEventRecordExternal)
+                                               : cudaEventRecord(e.ev[k], e.stream);
+}
+
 template<class T>
 int runChainBatched(sphb_ensemble& e, int which = -1)
 {
@@ -591,10 +629,16 @@ int runChainBatched(sphb_ensemble& e, int which = -1)
         b.threads        = e.threads[q];
         return b;
     };
+    auto mark = [&](int stage) { return which < 0 ? stageMark(e, stage) : cudaSuccess; };
+    SPHB_CUDA_TRY(mark(2));
     if (which < 0 || which == 0) { SPHB_TRY(launchXMass(with(0), k, e.box, st)); }
+    SPHB_CUDA_TRY(mark(3));
     if (which < 0 || which == 1) { SPHB_TRY(launchVeDefGradhEos(with(1), k, e.box, st)); }
+    SPHB_CUDA_TRY(mark(4));
     if (which < 0 || which == 2) { SPHB_TRY(launchIadDivvCurlv(with(2), k, e.box, st)); }
+    SPHB_CUDA_TRY(mark(5));
     if (which < 0 || which == 3) { SPHB_TRY(launchAVswitches(with(3), k, e.box, 0.0, st)); }
+    SPHB_CUDA_TRY(mark(6));
     if (which < 0 || which == 4) { SPHB_TRY(launchMomentumEnergy(with(4), k, e.box, st)); }
     return kOk;
 }
@@ -713,7 +757,9 @@ int stepBatched(sphb_ensemble& e)
 {
     cudaStream_t st = e.stream;
     size_t n        = e.slots;
+    SPHB_CUDA_TRY(stageMark(e, 0));
     SPHB_TRY(syncBatched(e, true));
+    SPHB_CUDA_TRY(stageMark(e, 1));
     initReduceKernel<<<ceilDiv(size_t(e.num), 64), 64, 0, st>>>(e.num, e.reduce.data(), e.cons.data());
     countLaunch();
     TreeView dummy{};
@@ -727,12 +773,15 @@ int stepBatched(sphb_ensemble& e)
     }
     if (e.mixed) { SPHB_TRY(runChainBatched<float>(e)); }
     else { SPHB_TRY(runChainBatched<double>(e)); }
-    consBatchKernel<<<ceilDiv(n, 256), 256, 0, st>>>(n, e.inst.data(), e.f[0].data(), e.f[1].data(), e.f[2].data(),
+    SPHB_CUDA_TRY(stageMark(e, 7));
+    consBatchKernel<<<kConsWarps / 8, 256, 0, st>>>(n, e.inst.data(), e.f[0].data(), e.f[1].data(), e.f[2].data(),
                                                      e.f[6].data(), e.f[7].data(), e.f[8].data(), e.f[4].data(),
                                                      e.f[5].data(), e.nc.data(), e.cv.data(), e.cons.data());
     countLaunch();
+    SPHB_CUDA_TRY(stageMark(e, 8));
     if (e.mixed) { SPHB_TRY(integrateBatched<float>(e)); }
     else { SPHB_TRY(integrateBatched<double>(e)); }
+    SPHB_CUDA_TRY(stageMark(e, 9));
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
 }
@@ -884,6 +933,10 @@ extern "C" int sphb_ensemble_destroy(sphb_ensemble* e)
     if (!e) { return SPHB_ERR_ARG; }
     if (e->stream) { cudaStreamSynchronize(e->stream); }
     dropGraph(*e);
+    for (auto& ev : e->ev)
+    {
+        if (ev) { cudaEventDestroy(ev); }
+    }
     if (e->stream) { cudaStreamDestroy(e->stream); }
     delete e;
     return SPHB_OK;
@@ -1044,6 +1097,18 @@ extern "C" int sphb_ensemble_autotune(sphb_ensemble* e, int* threads_out)
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
     if (threads_out) { std::copy(e->threads, e->threads + kJLoops, threads_out); }
     return dropGraph(*e);
+}
+
+extern "C" int sphb_ensemble_stage_times(sphb_ensemble* e, float* out)
+{
+    if (!e || !out) { return SPHB_ERR_ARG; }
+    if (e->steps == 0) { return SPHB_ERR_STATE; }
+    SPHB_CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int k = 0; k < sphb_ensemble::kStages; ++k)
+    {
+        SPHB_CUDA_TRY(cudaEventElapsedTime(&out[k], e->ev[k], e->ev[k + 1]));
+    }
+    return SPHB_OK;
 }
 
 extern "C" int sphb_ensemble_search_stats(sphb_ensemble* e, uint64_t* out)

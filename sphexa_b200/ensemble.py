@@ -71,6 +71,13 @@ class Ensemble:
     def stream(self):
         return self.lib.sphb_ensemble_stream(self.h)
 
+    def stage_times(self) -> dict:
+        """Stage times in ms of the last step (CUDA events recorded inside the step)."""
+        from .simulation import STAGE_NAMES
+        out = np.empty(len(STAGE_NAMES), dtype=np.float32)
+        L.check(self.lib.sphb_ensemble_stage_times(self.h, L.ptr(out)), "sphb_ensemble_stage_times")
+        return dict(zip(STAGE_NAMES, out.tolist()))
+
     def search_stats(self) -> dict:
         """How the neighbour stage ran since the initial sync: tree searches of every group, skin-row builds, steps
         served from the skin rows, and groups those steps deferred to the tree search."""

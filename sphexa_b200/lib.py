@@ -54,6 +54,7 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sim_step_vjp_recorded", "sphb_ensemble_create", "sphb_ensemble_destroy",
             "sphb_ensemble_upload", "sphb_ensemble_initial_sync", "sphb_ensemble_rebuild_trees",
             "sphb_ensemble_set_threads", "sphb_ensemble_autotune", "sphb_ensemble_step", "sphb_ensemble_size", "sphb_ensemble_search_stats",
+            "sphb_ensemble_stage_times",
             "sphb_ensemble_get_field", "sphb_ensemble_scalars", "sphb_ensemble_stream")
 
 _lib = None
@@ -122,6 +123,7 @@ def load() -> C.CDLL:
         "sphb_ensemble_step": (C.c_int, [P, C.c_int, C.c_int]),
         "sphb_ensemble_size": (S, [P, C.c_int]),
         "sphb_ensemble_search_stats": (C.c_int, [P, P]),
+        "sphb_ensemble_stage_times": (C.c_int, [P, P]),
         "sphb_ensemble_get_field": (C.c_int, [P, C.c_int, C.c_char_p, P]),
         "sphb_ensemble_scalars": (C.c_int, [P, C.c_int, P]),
         "sphb_ensemble_stream": (C.c_void_p, [P]),
