@@ -129,7 +129,10 @@ struct sphb_ensemble
     cudaEvent_t ev[kStages + 1]{};
 
     int threads[kJLoops]{128, 128, 128, 128, 128};
-    cudaGraphExec_t graph{nullptr};
+    // two captured steps: they gather the particle state between the two buffer sets in opposite directions, so the
+    // state alternates between f and fAlt with no copy; graphs[parity] is the one whose input is the current set
+    cudaGraphExec_t graphs[2]{};
+    int parity{0};
     bool uploaded{false};
     bool synced{false};
     uint64_t steps{0};
@@ -407,7 +410,19 @@ int allocate(sphb_ensemble& e)
     return kOk;
 }
 
-//! keys, segmented sort, gather of 16 fields into fixed buffers (graph-replayable: no pointer swaps)
+//! the particle state (14 fields, ids, keys) now lives in the other buffer set
+void swapState(sphb_ensemble& e)
+{
+    for (int k = 0; k < kFields; ++k)
+    {
+        e.f[k].swap(e.fAlt[k]);
+    }
+    e.id.swap(e.idAlt);
+    e.keys.swap(e.keysAlt);
+}
+
+/*! keys, segmented sort, gather of 16 fields into the other buffer set, which then becomes the current one (a
+ *  captured step records the buffers of its set; the two captured steps alternate) */
 int syncBatched(sphb_ensemble& e, bool withLayout)
 {
     cudaStream_t st = e.stream;
@@ -426,18 +441,15 @@ int syncBatched(sphb_ensemble& e, bool withLayout)
     void* dst[16];
     for (int k = 0; k < kFields; ++k)
     {
-        SPHB_CUDA_TRY(
-            cudaMemcpyAsync(e.fAlt[k].data(), e.f[k].data(), n * sizeof(double), cudaMemcpyDeviceToDevice, st));
-        src[k] = e.fAlt[k].data();
-        dst[k] = e.f[k].data();
+        src[k] = e.f[k].data();
+        dst[k] = e.fAlt[k].data();
     }
-    SPHB_CUDA_TRY(cudaMemcpyAsync(e.idAlt.data(), e.id.data(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(e.keysAlt.data(), e.keys.data(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
-    src[14] = e.idAlt.data();
-    dst[14] = e.id.data();
-    src[15] = e.keysAlt.data();
-    dst[15] = e.keys.data();
+    src[14] = e.id.data();
+    dst[14] = e.idAlt.data();
+    src[15] = e.keys.data();
+    dst[15] = e.keysAlt.data();
     SPHB_TRY(gather8(e.order.data(), n, 16, src, dst, st));
+    swapState(e);
     countLaunch(6);
     if (e.skin)
     {
@@ -788,33 +800,45 @@ int stepBatched(sphb_ensemble& e)
 
 int dropGraph(sphb_ensemble& e)
 {
-    if (e.graph)
+    for (auto& g : e.graphs)
     {
-        SPHB_CUDA_TRY(cudaGraphExecDestroy(e.graph));
-        e.graph = nullptr;
+        if (g)
+        {
+            SPHB_CUDA_TRY(cudaGraphExecDestroy(g));
+            g = nullptr;
+        }
     }
+    e.parity = 0;
     return kOk;
 }
 
+/*! Capture two consecutive steps. Capturing runs nothing, but each captured step swaps the host's buffer sets, so
+ *  after both the host's sets are as before and graphs[0] starts from the current state. */
 int captureGraph(sphb_ensemble& e)
 {
     SPHB_TRY(dropGraph(e));
-    cudaGraph_t g = nullptr;
-    SPHB_CUDA_TRY(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
-    uint64_t l0        = launchCounter();
-    int rc             = stepBatched(e);
-    e.launchesPerStep  = launchCounter() - l0;
-    launchCounter()    = l0; // counted again on every replay
-    cudaError_t ce     = cudaStreamEndCapture(e.stream, &g);
-    if (rc != kOk)
+    const double* current = e.f[0].data(); // where the state is: capturing moves nothing
+    for (int q = 0; q < 2; ++q)
     {
-        if (g) { cudaGraphDestroy(g); }
-        return rc;
+        cudaGraph_t g = nullptr;
+        SPHB_CUDA_TRY(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+        uint64_t l0       = launchCounter();
+        int rc            = stepBatched(e);
+        e.launchesPerStep = launchCounter() - l0;
+        launchCounter()   = l0; // counted again on every replay
+        cudaError_t ce    = cudaStreamEndCapture(e.stream, &g);
+        if (rc != kOk)
+        {
+            if (g) { cudaGraphDestroy(g); }
+            if (e.f[0].data() != current) { swapState(e); }
+            dropGraph(e);
+            return rc;
+        }
+        SPHB_CUDA_TRY(ce);
+        cudaError_t ie = cudaGraphInstantiate(&e.graphs[q], g, 0);
+        cudaGraphDestroy(g);
+        SPHB_CUDA_TRY(ie);
     }
-    SPHB_CUDA_TRY(ce);
-    cudaError_t ie = cudaGraphInstantiate(&e.graph, g, 0);
-    cudaGraphDestroy(g);
-    SPHB_CUDA_TRY(ie);
     return kOk;
 }
 
@@ -1019,13 +1043,17 @@ extern "C" int sphb_ensemble_step(sphb_ensemble* e, int steps, int use_graph)
 {
     if (!e || steps < 0) { return SPHB_ERR_ARG; }
     if (!e->synced) { return SPHB_ERR_STATE; }
-    if (use_graph && !e->graph) { SPHB_TRY(captureGraph(*e)); }
+    if (use_graph && !e->graphs[0]) { SPHB_TRY(captureGraph(*e)); }
+    // an eager step moves the state to the other buffer set on its own, which the captured pair cannot follow
+    if (!use_graph && steps > 0) { SPHB_TRY(dropGraph(*e)); }
     for (int s = 0; s < steps; ++s)
     {
         if (use_graph)
         {
-            SPHB_CUDA_TRY(cudaGraphLaunch(e->graph, e->stream));
+            SPHB_CUDA_TRY(cudaGraphLaunch(e->graphs[e->parity], e->stream));
             countLaunch(e->launchesPerStep);
+            swapState(*e);
+            e->parity ^= 1;
         }
         else { SPHB_TRY(stepBatched(*e)); }
     }
