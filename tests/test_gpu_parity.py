@@ -365,6 +365,30 @@ def test_stage_calls_match_compute_forces(lib, precision):
         b.integrate()  # the next force computation has not run
 
 
+def test_noh_strong_shock_mixed_vs_fp64(lib):
+    """Noh 40^3 run to t = 0.2, when the centre holds the strong-shock density (~64x the initial one): the mixed step
+    against the FP64 one after the same ~157 steps. Total energy to 1e-6, density per particle to 1e-4 in the median
+    and 1e-3 in RMS (the shock front dominates the largest differences); both reach a density above 50."""
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    res = {}
+    for prec in ("fp64", "mixed"):
+        s = Simulation(icm.noh(40), prec)
+        steps = 0
+        while s.scalars()["ttot"] < 0.2 and steps < 1000:
+            s.step()
+            steps += 1
+        order = np.argsort(s.get("id"))
+        res[prec] = (steps, s.scalars(), (s.get("kx") * s.get("m") / s.get("xm"))[order])
+        s.close()
+    (na, sa, ra), (nb, sb, rb) = res["mixed"], res["fp64"]
+    assert na == nb
+    assert abs(sa["etot"] - sb["etot"]) <= 1e-6 * abs(sb["etot"])
+    d = np.abs(ra - rb) / rb
+    assert np.median(d) < 1e-4 and np.sqrt(np.mean(d * d)) < 1e-3, (np.median(d), np.sqrt(np.mean(d * d)))
+    assert ra.max() > 50 and rb.max() > 50
+
+
 def test_zero_length_calls(lib):
     import torch
     from sphexa_b200 import lib as L
