@@ -163,6 +163,35 @@ int sphb_sim_integrate(sphb_sim* sim);
 /*! compute_forces + integrate. */
 int sphb_sim_step(sphb_sim* sim);
 
+/*! Block time steps: switch this simulation to the propagator of main/src/propagator/ve_hydro_bdt.hpp
+ *  (HydroVeBdtProp<avClean = false>). Groups are the fixed groups of 32 SFC-consecutive particles. Each group gets
+ *  the time step min(Courant, Krho / |max divv|, eta_acc (h^2/|a|^2)^(1/4)) over its particles (ts_groups.cu), the
+ *  groups are sorted by it into up to 4 power-of-two rungs (ts_rungs.hpp:116-166), and a block step of
+ *  2^(numRungs - 1) substeps computes forces only on the groups of the active rungs while the others drift.
+ *  eta_acc: the acceleration criterion (ParticlesData::etaAcc, 0.2). After this call sphb_sim_compute_forces,
+ *  sphb_sim_step and the stage calls return SPHB_ERR_STATE; sphb_sim_upload resets the block-step state.
+ *  SPHB_ERR_ARG with AV cleaning. */
+int sphb_sim_bdt_enable(sphb_sim* sim, double eta_acc);
+
+/*! One substep of the block time-step propagator: computeForces (domain sync at the first substep of a block,
+ *  neighbour search of every particle, the SPH-VE chain on the active groups, EOS of every particle, group time
+ *  steps) then integrate (rungs, kick-drift of the rungs that complete their step, drift of the others, h update of
+ *  the active groups) (ve_hydro_bdt.hpp:224-380). SPHB_ERR_NOT_CONVERGED as sphb_sim_integrate. */
+int sphb_sim_bdt_step(sphb_sim* sim);
+
+/*! sph::Timestep of the block time-step propagator (sph/include/sph/timestep.h:17-31) after the last substep. */
+typedef struct
+{
+    float next_dt, elapsed_dt, total_dt;
+    int num_rungs, substep;
+    uint32_t rung_ranges[5]; /* groups [rung_ranges[r], rung_ranges[r+1]) of the dt-sorted order are rung r */
+    float dt_m1[4];          /* last full step per rung                                             */
+    float dt_drift[4];       /* time each rung has drifted since its last full step                 */
+    uint32_t num_active;     /* groups whose forces the last substep computed                        */
+} sphb_bdt_timestep;
+
+int sphb_sim_bdt_timestep(const sphb_sim* sim, sphb_bdt_timestep* out);
+
 /* The force computation one stage at a time, for a caller that runs its own code between the stages as the
  * reference's propagator does (HydroVeProp::computeForces, ve_hydro.hpp:126-203, exchanges halos between them).
  * sphb_sim_compute_forces runs exactly these eight calls. Each stage must follow the previous one of the same force

@@ -914,8 +914,9 @@ void orc_sim_destroy(orc_sim* s)
     free(s);
 }
 
-/* box of open axes (cstone/sfc/box_mpi.hpp:69-107, box.hpp:398-414), keys, stable sort, reorder every field */
-void orc_sim_sync(orc_sim* s)
+/* box of open axes (cstone/sfc/box_mpi.hpp:69-107, box.hpp:398-414), keys, stable sort, reorder every field;
+ * permOut (optional, n entries) receives the applied permutation (new index i held old index permOut[i]) */
+void orc_sim_sync_perm(orc_sim* s, uint32_t* permOut)
 {
     size_t n = s->n;
     for (int k = 0; k < 3; ++k)
@@ -961,17 +962,23 @@ void orc_sim_sync(orc_sim* s)
         tid[i] = s->id[perm[i]];
     }
     memcpy(s->id, tid, n * sizeof(uint64_t));
+    if (permOut) { memcpy(permOut, perm, n * sizeof(uint32_t)); }
     free(tid);
     free(tmp);
     free(perm);
 }
 
+void orc_sim_sync(orc_sim* s) { orc_sim_sync_perm(s, NULL); }
+
 static double idealCv(double mui, double gamma) { return 8.317e7 / mui / (gamma - 1.0); }
 
-int orc_sim_compute_forces(orc_sim* s)
+/* the force computation of HydroVeProp (ve_hydro.hpp:126-203); with an active mask, that of HydroVeBdtProp
+ * (main/src/propagator/ve_hydro_bdt.hpp:224-296): the search for every particle, the J-loops for the active ones,
+ * the EOS for every particle; avDt is the time step of the AV-switch update; dtOut (optional) receives the Courant
+ * step of every active particle (INFINITY for the others) */
+static int computeForcesImpl(orc_sim* s, const uint8_t* active, double avDt, double* dtOut)
 {
     size_t n = s->n;
-    orc_sim_sync(s);
     double* x = s->f[F_X];
     double* y = s->f[F_Y];
     double* z = s->f[F_Z];
@@ -991,11 +998,13 @@ int orc_sim_compute_forces(orc_sim* s)
 #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; ++i)
     {
+        if (active && !active[i]) { continue; }
         s->d[D_XM][i] = orc_xmass((unsigned)i, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, h, m, s->wh);
     }
 #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; ++i)
     {
+        if (active && !active[i]) { continue; }
         orc_ve_def_gradh((unsigned)i, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, h, m, s->wh, s->whd,
                          s->d[D_XM], &s->d[D_KX][i], &s->d[D_GRADH][i]);
     }
@@ -1012,6 +1021,7 @@ int orc_sim_compute_forces(orc_sim* s)
 #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; ++i)
     {
+        if (active && !active[i]) { continue; }
         double c6[6];
         orc_iad((unsigned)i, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, h, s->wh, s->d[D_XM], s->d[D_KX], c6);
         for (int k = 0; k < 6; ++k)
@@ -1023,6 +1033,7 @@ int orc_sim_compute_forces(orc_sim* s)
 #pragma omp parallel for schedule(static) reduction(max : maxDivv)
     for (size_t i = 0; i < n; ++i)
     {
+        if (active && !active[i]) { continue; }
         double dvv[6];
         orc_divv_curlv((unsigned)i, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, s->f[F_VX], s->f[F_VY],
                        s->f[F_VZ], h, cij, s->wh, s->d[D_KX], s->d[D_XM], &s->d[D_DIVV][i], &s->d[D_CURLV][i], dvv);
@@ -1034,9 +1045,14 @@ int orc_sim_compute_forces(orc_sim* s)
 #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < n; ++i)
     {
+        if (active && !active[i])
+        {
+            alphaN[i] = s->f[F_ALPHA][i];
+            continue;
+        }
         alphaN[i] = orc_av_switches((unsigned)i, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, s->f[F_VX],
                                     s->f[F_VY], s->f[F_VZ], h, s->d[D_C], cij, s->wh, s->d[D_KX], s->d[D_XM],
-                                    s->d[D_DIVV], s->minDt, s->alphamin, s->alphamax, s->decay, s->f[F_ALPHA][i]);
+                                    s->d[D_DIVV], avDt, s->alphamin, s->alphamax, s->decay, s->f[F_ALPHA][i]);
     }
     memcpy(s->f[F_ALPHA], alphaN, n * sizeof(double));
     free(alphaN);
@@ -1045,6 +1061,11 @@ int orc_sim_compute_forces(orc_sim* s)
 #pragma omp parallel for schedule(static) reduction(min : minDt)
     for (size_t i = 0; i < n; ++i)
     {
+        if (active && !active[i])
+        {
+            if (dtOut) { dtOut[i] = INFINITY; }
+            continue;
+        }
         double o[5];
         orc_momentum_energy((unsigned)i, 0, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, s->f[F_VX], s->f[F_VY],
                             s->f[F_VZ], h, m, s->d[D_PRHO], s->d[D_C], cij, 0.1, 0.2, 1.0 / (0.2 - 0.1), s->wh,
@@ -1057,6 +1078,7 @@ int orc_sim_compute_forces(orc_sim* s)
         double v  = o[4] > 0.0 ? o[4] : s->d[D_C][i];
         double dt = h[i] > 0.0 ? (double)kc * h[i] / v : INFINITY;
         minDt     = dt < minDt ? dt : minDt;
+        if (dtOut) { dtOut[i] = dt; }
     }
     s->minDtCourant = minDt;
 #undef CNT
@@ -1084,6 +1106,111 @@ int orc_sim_compute_forces(orc_sim* s)
     s->totalNeighbors = ncs;
     free(nc);
     return 0;
+}
+
+int orc_sim_compute_forces(orc_sim* s)
+{
+    orc_sim_sync(s);
+    return computeForcesImpl(s, NULL, s->minDt, NULL);
+}
+
+int orc_sim_forces_active(orc_sim* s, const uint8_t* active, double avDt, double* dtCourant)
+{
+    return computeForcesImpl(s, active, avDt, dtCourant);
+}
+
+/* positionUpdate of one axis (sph/include/sph/positions.hpp:100-111) */
+static double pressAxis(double X, double A, double dX, double dt, double dtm1, double* V, double* dXn1)
+{
+    double vh = dX * (1.0 / dtm1);
+    double vn = vh + 0.5 * dtm1 * A;
+    *V        = vn + A * dt;
+    *dXn1     = (vn + 0.5 * A * fabs(dt)) * dt;
+    return X + *dXn1;
+}
+
+/* energyUpdate (positions.hpp:77-84) */
+static double energyUpdate(double uOld, double dt, double dtm1, double du, double duM1)
+{
+    double uNew = uOld + du * dt + 0.5 * (du - duM1) / dtm1 * fabs(dt) * dt;
+    if (uNew < 0.0) { uNew = uOld * exp(uNew * dt / uOld); }
+    return uNew;
+}
+
+/* driftKernel (sph/include/sph/positions_gpu.cu:45-90) over the listed particles: back by dtBack, forward by dt from
+ * there, no periodic folding */
+void orc_drift(orc_sim* s, const uint32_t* idx, size_t cnt, float dt, float dtBack, const float* dtm1,
+               const uint8_t* rung)
+{
+    double cv = idealCv(s->mui, s->gamma);
+    for (size_t q = 0; q < cnt; ++q)
+    {
+        size_t i    = idx[q];
+        double m1   = (double)dtm1[rung[i]];
+        double back = -(double)dtBack, fwd = (double)dt;
+        double A[3] = {s->d[D_AX][i], s->d[D_AY][i], s->d[D_AZ][i]};
+        for (int k = 0; k < 3; ++k)
+        {
+            double v, d;
+            double Xn          = pressAxis(s->f[F_X + k][i], A[k], s->f[F_XM1 + k][i], back, m1, &v, &d);
+            s->f[F_X + k][i]   = pressAxis(Xn, A[k], s->f[F_XM1 + k][i], fwd, m1, &v, &d);
+            s->f[F_VX + k][i]  = v;
+        }
+        double du = s->d[D_DU][i], duM1 = s->f[F_DUM1][i];
+        double u  = energyUpdate(s->f[F_TEMP][i] * cv, back, m1, du, duM1);
+        s->f[F_TEMP][i] = energyUpdate(u, fwd, m1, du, duM1) / cv;
+    }
+}
+
+/* computePositionsKernel (positions_gpu.cu:117-166) over the listed particles; fold != 0: putInBox on the periodic
+ * axes */
+void orc_rung_positions(orc_sim* s, const uint32_t* idx, size_t cnt, float dt, const float* dtm1, const uint8_t* rung,
+                        int fold)
+{
+    double cv = idealCv(s->mui, s->gamma);
+    for (size_t q = 0; q < cnt; ++q)
+    {
+        size_t i    = idx[q];
+        double m1   = (double)dtm1[rung[i]];
+        double dtD  = (double)dt;
+        double A[3] = {s->d[D_AX][i], s->d[D_AY][i], s->d[D_AZ][i]};
+        for (int k = 0; k < 3; ++k)
+        {
+            double v, d;
+            double X = pressAxis(s->f[F_X + k][i], A[k], s->f[F_XM1 + k][i], dtD, m1, &v, &d);
+            if (fold && s->box.periodic[k])
+            {
+                double L = s->box.hi[k] - s->box.lo[k];
+                if (X > s->box.hi[k]) { X -= L; }
+                else if (X < s->box.lo[k]) { X += L; }
+            }
+            s->f[F_X + k][i]   = X;
+            s->f[F_XM1 + k][i] = d;
+            s->f[F_VX + k][i]  = v;
+        }
+        double du       = s->d[D_DU][i];
+        s->f[F_TEMP][i] = energyUpdate(cv * s->f[F_TEMP][i], dtD, m1, du, s->f[F_DUM1][i]) / cv;
+        s->f[F_DUM1][i] = du;
+    }
+}
+
+/* updateSmoothingLength over the listed particles (sph/include/sph/update_h.hpp:12-47); returns 1 if any has
+ * nc <= 1 */
+int orc_update_h_subset(orc_sim* s, const uint32_t* idx, size_t cnt)
+{
+    int removed = 0;
+    for (size_t q = 0; q < cnt; ++q)
+    {
+        size_t i     = idx[q];
+        unsigned nci = (unsigned)s->d[D_NC][i];
+        if (nci <= 1)
+        {
+            s->keys[i] = REMOVE_KEY;
+            removed    = 1;
+        }
+        s->f[F_H][i] = updateH(s->ng0, nci, s->f[F_H][i]);
+    }
+    return removed;
 }
 
 /* computeTimestep (sph/include/sph/ts_global.hpp:100-128), positions + energy (sph/include/sph/positions.hpp:77-160),

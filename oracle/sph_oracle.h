@@ -66,6 +66,13 @@ orc_sim* orc_sim_create(size_t n, const double* const* fields, const uint64_t* i
                         int periodic, const double* params);
 void orc_sim_destroy(orc_sim* s);
 void orc_sim_sync(orc_sim* s);
+void orc_sim_sync_perm(orc_sim* s, uint32_t* permOut);
+int orc_sim_forces_active(orc_sim* s, const uint8_t* active, double avDt, double* dtCourant);
+void orc_drift(orc_sim* s, const uint32_t* idx, size_t cnt, float dt, float dtBack, const float* dtm1,
+               const uint8_t* rung);
+void orc_rung_positions(orc_sim* s, const uint32_t* idx, size_t cnt, float dt, const float* dtm1, const uint8_t* rung,
+                        int fold);
+int orc_update_h_subset(orc_sim* s, const uint32_t* idx, size_t cnt);
 int orc_sim_compute_forces(orc_sim* s);
 int orc_sim_integrate(orc_sim* s);
 size_t orc_sim_size(const orc_sim* s);

@@ -16,6 +16,7 @@ constexpr int kChainThreads = 128;
 constexpr int kModeTape    = 1;
 constexpr int kModeBatch   = 2;
 constexpr int kModeAvClean = 4;
+constexpr int kModeList    = 8; // block time steps: only the groups of a device-side list
 
 /*! Neighbour-sum accumulator. FP64: every term is added as it comes, in list order (the reference's order).
  *  FP32: terms are summed plainly within one list chunk of 8 neighbours and each chunk sum is added to a
@@ -265,6 +266,27 @@ __device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned 
     t.count = min(nc[t.i] - 1u, ngmax);
     t.ngPad = paddedNgmax(ngmax);
     return true;
+}
+
+/*! The target of this thread: thread i of the launch, or in list mode lane i % 32 of group groupList[i / 32]
+ *  (GroupView slices of sph/include/sph/groups.hpp:96-103; a warp is one group). *w receives the list slot. */
+template<int kMode, class T>
+__device__ __forceinline__ bool chainTarget(const ChainArrays<T>& a, unsigned ngmax, Target& t, unsigned* w = nullptr)
+{
+    if constexpr (kMode & kModeList)
+    {
+        size_t slot = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5;
+        if (w) { *w = unsigned(slot); }
+        if (slot >= a.numListed) { return false; }
+        t.i = size_t(__ldg(a.groupList + slot)) * 32 + (threadIdx.x & 31);
+        if (t.i >= a.n) { return false; }
+        t.group = t.i >> 5;
+        t.lane  = unsigned(t.i & 31);
+        t.count = min(a.nc[t.i] - 1u, ngmax);
+        t.ngPad = paddedNgmax(ngmax);
+        return true;
+    }
+    else { return targetOf(a.n, a.nc, ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr); }
 }
 
 template<class T>

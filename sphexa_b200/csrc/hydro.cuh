@@ -126,6 +126,11 @@ struct ChainArrays
     DVRec<T>* dvrec{nullptr}; // set: AV cleaning (HydroVeProp<avClean = true>)
     T* dv[6]{};              // the same six fields as arrays (dV11 .. dV33)
     int threads{128}; // block size of the J-loop launches
+    // block time steps: the launch covers only the groups groupList[0, numListed) (one warp each); MomentumEnergy
+    // then lowers groupDt[w] of listed group w to the Courant step of its particles
+    const uint32_t* groupList{nullptr};
+    unsigned numListed{0};
+    float* groupDt{nullptr};
 };
 
 template<class T>

@@ -30,7 +30,7 @@ template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr)) { return; }
+    if (!chainTarget<kMode>(a, k.ngmax, t)) { return; }
     Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
@@ -67,7 +67,7 @@ template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr)) { return; }
+    if (!chainTarget<kMode>(a, k.ngmax, t)) { return; }
     Pos<T> pi  = posOf(a, t.i);
     double hiD = a.h[t.i];
     T hi       = T(hiD);
@@ -153,7 +153,7 @@ template<class T, int kMode>
 __global__ void __launch_bounds__(kChainMaxThreads) iadDivvCurlvKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid     = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
+    bool valid     = chainTarget<kMode>(a, k.ngmax, t);
     double divvOut = -INFINITY;
     if (valid)
     {
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kChainMaxThreads, 3) iadDivvCurlvFusedKernel(C
 {
     using T = float;
     Target t;
-    bool valid     = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
+    bool valid     = chainTarget<kMode>(a, k.ngmax, t);
     double divvOut = -INFINITY;
     if (valid)
     {
@@ -450,7 +450,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) avSwitchesKernel(ChainArrays
                                                                   double dt)
 {
     Target t;
-    if (!targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr)) { return; }
+    if (!chainTarget<kMode>(a, k.ngmax, t)) { return; }
     Pos<T> pi      = posOf(a, t.i);
     double hiD     = a.h[t.i];
     HydroRec<T> hr = a.hrec[t.i];
@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode &
     momentumEnergyKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
-    bool valid   = targetOf(a.n, a.nc, k.ngmax, t, (kMode & kModeBatch) ? a.batch.inst : nullptr);
+    bool valid   = chainTarget<kMode>(a, k.ngmax, t);
     double dtMin = INFINITY;
     if (valid)
     {
@@ -694,12 +694,26 @@ __global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode &
         double v = maxvsignalI > T(0) ? double(maxvsignalI) : double(ci);
         dtMin    = hiD > 0.0 ? k.Kcour * hiD / v : INFINITY;
     }
+    if constexpr (kMode & kModeList)
+    {
+        // the group's Courant step lowers its block time step (momentum_energy_gpu.cu:96-103); rounding to float is
+        // monotonic, so min(float, double) stored as float equals the min of the float values
+        unsigned w  = unsigned((blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5);
+        double gmin = dtMin;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            gmin = fmin(gmin, __shfl_xor_sync(0xffffffffu, gmin, off));
+        }
+        if ((threadIdx.x & 31) == 0 && w < a.numListed) { a.groupDt[w] = fminf(a.groupDt[w], float(gmin)); }
+    }
     reduceOrdered<false, (kMode & kModeBatch) != 0>(dtMin, a.n, a.reduce + 1, a.batch, 1);
 }
 
 template<class T>
 unsigned chainBlocks(const ChainArrays<T>& a)
 {
+    if (a.groupList) { return ceilDiv(size_t(a.numListed) * 32, unsigned(a.threads)); }
     return ceilDiv(a.n, size_t(a.threads));
 }
 
@@ -710,6 +724,7 @@ template<class T>
 int chainMode(const ChainArrays<T>& a)
 {
     int mode = (a.tape.energy ? kModeTape : 0) | (a.batch.inst ? kModeBatch : 0);
+    if (a.groupList) { return mode == 0 ? kModeList : -1; } // block time steps: no tape, no ensemble
     return mode == (kModeTape | kModeBatch) ? -1 : mode;
 }
 
@@ -719,6 +734,7 @@ int chainModeAv(const ChainArrays<T>& a)
 {
     int mode = chainMode(a);
     if (mode < 0 || !a.dvrec) { return mode; }
+    if (mode & kModeList) { return -1; } // no AV-cleaning variant under block time steps
     return (mode & kModeTape) ? -1 : (mode | kModeAvClean); // the adjoint has no AV-cleaning variant
 }
 
@@ -729,6 +745,7 @@ int chainModeAv(const ChainArrays<T>& a)
     case kModeTape: KERNEL<T, kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
     case kModeBatch: KERNEL<T, kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                  \
     case kModeAvClean: KERNEL<T, kModeAvClean><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;              \
+    case kModeList: KERNEL<T, kModeList><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
     case kModeAvClean | kModeBatch:                                                                                     \
         KERNEL<T, kModeAvClean | kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__);                         \
         break;                                                                                                          \
@@ -741,13 +758,14 @@ int chainModeAv(const ChainArrays<T>& a)
     case 0: KERNEL<T, 0><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                                    \
     case kModeTape: KERNEL<T, kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
     case kModeBatch: KERNEL<T, kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                  \
+    case kModeList: KERNEL<T, kModeList><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
     default: return kErrArg;                                                                                            \
     }
 
 template<class T>
 int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
-    if (a.n == 0) { return kOk; }
+    if (a.n == 0 || (a.groupList && a.numListed == 0)) { return kOk; }
     SPHB_DISPATCH(xmassKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
@@ -757,7 +775,7 @@ int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& 
 template<class T>
 int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
-    if (a.n == 0) { return kOk; }
+    if (a.n == 0 || (a.groupList && a.numListed == 0)) { return kOk; }
     SPHB_DISPATCH(veDefGradhEosKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
@@ -767,7 +785,7 @@ int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const 
 template<class T>
 int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
-    if (a.n == 0) { return kOk; }
+    if (a.n == 0 || (a.groupList && a.numListed == 0)) { return kOk; }
     if constexpr (sizeof(T) == 4)
     {
         switch (chainModeAv(a))
@@ -775,6 +793,7 @@ int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const D
         case 0: iadDivvCurlvFusedKernel<0><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
         case kModeTape: iadDivvCurlvFusedKernel<kModeTape><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
         case kModeBatch: iadDivvCurlvFusedKernel<kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
+        case kModeList: iadDivvCurlvFusedKernel<kModeList><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box); break;
         case kModeAvClean:
             iadDivvCurlvFusedKernel<kModeAvClean><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
             break;
@@ -793,7 +812,7 @@ int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const D
 template<class T>
 int launchAVswitches(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, double dt, cudaStream_t s)
 {
-    if (a.n == 0) { return kOk; }
+    if (a.n == 0 || (a.groupList && a.numListed == 0)) { return kOk; }
     SPHB_DISPATCH(avSwitchesKernel, a, k, box, dt)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
@@ -803,7 +822,7 @@ int launchAVswitches(const ChainArrays<T>& a, const HydroConsts<T>& k, const Dev
 template<class T>
 int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
-    if (a.n == 0) { return kOk; }
+    if (a.n == 0 || (a.groupList && a.numListed == 0)) { return kOk; }
     SPHB_DISPATCH_AV(momentumEnergyKernel, a, k, box)
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());

@@ -13,11 +13,12 @@ namespace
 
 //! one coordinate as 32-bit fixed point over [lo, lo + 2^32 unit), unit = span / 2^32 (periodic: span = L, the value
 //! L wraps to 0; open: span = 2 L so that differences of up to L stay below half the range and never wrap)
+//! Coordinates below lo (drifted out of the box between two domain syncs under block time steps) wrap modulo 2^32:
+//! on a periodic axis that is the periodic image, on an open axis differences below L still come out right.
 __device__ inline int quantiseFixed(double v, double lo, double invUnit)
 {
     double q = (v - lo) * invUnit;
-    q        = q < 0.0 ? 0.0 : q;
-    unsigned long long u = (unsigned long long)(q + 0.5);
+    unsigned long long u = q >= 0.0 ? (unsigned long long)(q + 0.5) : 0ull - (unsigned long long)(0.5 - q);
     return int(unsigned(u & 0xffffffffull));
 }
 

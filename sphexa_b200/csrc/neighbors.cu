@@ -463,7 +463,7 @@ __global__ void __launch_bounds__(kNbThreads, 8) findNeighborsKernel(const doubl
                 {
                     double d = tv.centers[3 * c + k] - gc[k];
                     if (box.periodic[k]) { d -= box.len[k] * rint(d * box.ilen[k]); }
-                    ov = ov && fabs(d) <= gs[k] + tv.sizes[3 * c + k] * (1.0 + 1e-12);
+                    ov = ov && fabs(d) <= gs[k] + tv.sizes[3 * c + k] * (1.0 + 1e-12) + tv.ext;
                 }
             }
             unsigned m = __ballot_sync(0xffffffffu, ov) & 0xffu;

@@ -17,6 +17,9 @@ struct TreeView
     const float4* blockLo; // per run of kBlockSize consecutive particles: bounding box relative to the box corner
     const float4* blockHi;
     int numNodes;
+    // bound on how far any particle has moved since the tree was built (block time steps drift particles between
+    // tree builds): node boxes are widened by it, so a particle outside its cell is still found
+    double ext{0.0};
 };
 
 //! particles per bounding-box block used to prune the candidates of the search below leaf resolution

@@ -3,10 +3,12 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
 #include "adjoint.cuh"
+#include "bdt.cuh"
 #include "hydro.cuh"
 #include "integrate.cuh"
 #include "neighbors.cuh"
@@ -126,6 +128,31 @@ struct sphb_sim
     unsigned skinDeferredLast{0};
     // tree searches of every group, row builds, refiltered steps, deferred groups, syncs that remapped the rows
     uint64_t searchStats[5]{};
+
+    // block time steps (main/src/propagator/ve_hydro_bdt.hpp), after sphb_sim_bdt_enable
+    struct BdtTimestep // sph::Timestep (sph/include/sph/timestep.h:17-31)
+    {
+        float nextDt{0}, elapsedDt{0}, totDt{0};
+        int numRungs{1};
+        int substep{0};
+        uint32_t rungRanges[kMaxRungs + 1]{};
+        float dtm1[kMaxRungs]{};
+        float dtDrift[kMaxRungs]{};
+    };
+    bool bdt{false};
+    float etaAcc{0.2f};
+    BdtTimestep bts, bprevTs;
+    DeviceBuffer<uint64_t> rung, rungAlt;   // rung each particle was last advanced on (a conserved field)
+    DeviceBuffer<float> groupDt;            // per group of the current group order
+    DeviceBuffer<uint32_t> groupIdx;        // sort permutation of groupDt
+    DeviceBuffer<uint32_t> grpSfc, grpTs;   // groups_ (SFC order after a full sync) and tsGroups_ (by time step)
+    DeviceBuffer<uint64_t> dtKeys;
+    DeviceBuffer<uint32_t> rungInfo;
+    DeviceBuffer<double> xs, ys, zs;        // positions at the last full sync (drift bound of the tree search)
+    DeviceBuffer<unsigned long long> dispMax;
+    const uint32_t* activeList{nullptr};    // activeRungs_: groups whose forces this substep computes
+    unsigned numActive{0};
+    double treeExt{0.0};                    // widening of the tree's node boxes (TreeView::ext)
 
     cudaEvent_t ev[kNumStages + 1]{};
     float stageMs[kNumStages]{};
@@ -276,8 +303,8 @@ int syncDomain(sphb_sim& s)
     if (!identity)
     {
         // reorder every conserved field and the ids into SFC order
-        const void* src[kNumConserved + 1];
-        void* dst[kNumConserved + 1];
+        const void* src[kNumConserved + 2];
+        void* dst[kNumConserved + 2];
         for (int k = 0; k < kNumConserved; ++k)
         {
             src[k] = s.f[k].data();
@@ -285,12 +312,20 @@ int syncDomain(sphb_sim& s)
         }
         src[kNumConserved] = s.id.data();
         dst[kNumConserved] = s.idAlt.data();
-        SPHB_TRY(gather8(s.order.data(), s.n, kNumConserved + 1, src, dst, st));
+        int numFields      = kNumConserved + 1;
+        if (s.bdt)
+        {
+            src[numFields] = s.rung.data();
+            dst[numFields] = s.rungAlt.data();
+            ++numFields;
+        }
+        SPHB_TRY(gather8(s.order.data(), s.n, numFields, src, dst, st));
         for (int k = 0; k < kNumConserved; ++k)
         {
             s.f[k].swap(s.fAlt[k]);
         }
         s.id.swap(s.idAlt);
+        if (s.bdt) { s.rung.swap(s.rungAlt); }
     }
 
     bool converged = false;
@@ -450,6 +485,7 @@ TreeView treeView(sphb_sim& s)
     tv.blockLo      = s.blockLo.data();
     tv.blockHi      = s.blockHi.data();
     tv.numNodes     = s.ftree.tree.numNodes;
+    tv.ext          = s.treeExt;
     return tv;
 }
 
@@ -498,7 +534,8 @@ int searchNeighbors(sphb_sim& s)
                              s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), st);
     };
 
-    bool useSkin = s.p.nb_skin > 0.0 && !s.taping;
+    // block time steps drift particles without a resort, which the displacement bounds of the rows do not track
+    bool useSkin = s.p.nb_skin > 0.0 && !s.taping && !s.bdt;
     if (!useSkin || s.skinHoldoff > 0)
     {
         if (s.skinHoldoff > 0) { --s.skinHoldoff; }
@@ -726,6 +763,306 @@ int integrateStep(sphb_sim& s)
     return flag ? kErrNotConverged : kOk;
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Block time steps: HydroVeBdtProp (main/src/propagator/ve_hydro_bdt.hpp:165-380) over fixed groups of 32
+// SFC-consecutive particles, with the rung logic of sph/include/sph/ts_rungs.hpp.
+// ---------------------------------------------------------------------------------------------------------------
+
+//! cstone::butterfly (cstone/primitives/math.hpp:35-40): 0, then 1 + trailing zeros
+int butterflyOf(uint32_t i) { return i == 0 ? 0 : 1 + __builtin_ctz(i); }
+
+//! HydroVeBdtProp::activeRung (ve_hydro_bdt.hpp:109-113): the rungs below it are active at this substep
+int activeRungOf(int substep, int numRungs)
+{
+    if (substep == 0 || substep >= (1 << (numRungs - 1))) { return 0; }
+    return butterflyOf(uint32_t(substep));
+}
+
+int allocateBdt(sphb_sim& s)
+{
+    size_t G = s.numGroups();
+    SPHB_TRY(s.rung.reserve(s.n));
+    SPHB_TRY(s.rungAlt.reserve(s.n));
+    SPHB_TRY(s.groupDt.reserve(G));
+    SPHB_TRY(s.groupIdx.reserve(G));
+    SPHB_TRY(s.grpSfc.reserve(G));
+    SPHB_TRY(s.grpTs.reserve(G));
+    SPHB_TRY(s.dtKeys.reserve(G));
+    SPHB_TRY(s.rungInfo.reserve(8));
+    SPHB_TRY(s.xs.reserve(s.n));
+    SPHB_TRY(s.ys.reserve(s.n));
+    SPHB_TRY(s.zs.reserve(s.n));
+    SPHB_TRY(s.dispMax.reserve(1));
+    return kOk;
+}
+
+//! the propagator's state after construction: one rung, dt_m1[0] = minDt (ve_hydro_bdt.hpp:116-130), rungs 0
+int resetBdt(sphb_sim& s)
+{
+    s.bts       = sphb_sim::BdtTimestep{};
+    s.bts.dtm1[0] = float(s.minDt);
+    s.bprevTs   = s.bts;
+    s.treeExt   = 0.0;
+    s.activeList = nullptr;
+    s.numActive  = 0;
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.rung.data(), 0, s.n * sizeof(uint64_t), s.stream));
+    return kOk;
+}
+
+//! fullSync / partialSync (ve_hydro_bdt.hpp:165-215)
+int bdtSync(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    unsigned G      = unsigned(s.numGroups());
+    if (activeRungOf(s.bts.substep, s.bts.numRungs) == 0)
+    {
+        SPHB_TRY(syncDomain(s));
+        SPHB_TRY(launchSequence(s.grpSfc.data(), G, 0, st)); // computeGroups: fixed groups in SFC order
+        s.activeList = s.grpSfc.data();
+        s.numActive  = G;
+        std::vector<float> big(G, std::numeric_limits<float>::max());
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.groupDt.data(), big.data(), G * sizeof(float), cudaMemcpyHostToDevice, st));
+        size_t bytes = s.n * sizeof(double);
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.xs.data(), s.f[fX].data(), bytes, cudaMemcpyDeviceToDevice, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.ys.data(), s.f[fY].data(), bytes, cudaMemcpyDeviceToDevice, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.zs.data(), s.f[fZ].data(), bytes, cudaMemcpyDeviceToDevice, st));
+        SPHB_CUDA_TRY(cudaStreamSynchronize(st)); // the host vector above
+        s.treeExt = 0.0;
+        return kOk;
+    }
+    // partial sync: no resort, so the groups keep their particles; the packed positions and the block boxes follow
+    // the drifted particles, and the tree's node boxes are widened by the largest drift since the full sync (the
+    // reference widens its search by 1.2 % per substep instead, ve_hydro_bdt.hpp:201-203)
+    SPHB_TRY(packPositionsAndBoxes(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n,
+                                   s.pos.data(), s.mixed ? s.posq.data() : nullptr, s.box, s.blockLo.data(),
+                                   s.blockHi.data(), st));
+    unsigned long long zero = orderedBits(0.0), dmax = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s.dispMax.data(), &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+    SPHB_TRY(launchMaxDisplacement(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.xs.data(), s.ys.data(),
+                                   s.zs.data(), s.n, s.box, s.dispMax.data(), st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&dmax, s.dispMax.data(), sizeof(dmax), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    double lenMax = std::max({s.box.len[0], s.box.len[1], s.box.len[2]});
+    s.treeExt     = fromOrderedBits(dmax) * (1.0 + 1e-9) + 1e-14 * lenMax;
+    int highest   = butterflyOf(uint32_t(s.bts.substep));
+    s.activeList  = s.grpTs.data() + s.bts.rungRanges[0];
+    s.numActive   = s.bts.rungRanges[highest] - s.bts.rungRanges[0];
+    return kOk;
+}
+
+//! computeForces of the block time-step propagator on the active groups (ve_hydro_bdt.hpp:224-296)
+template<class T>
+int bdtChain(sphb_sim& s)
+{
+    cudaStream_t st  = s.stream;
+    ChainArrays<T> a = chainArrays<T>(s);
+    HydroConsts<T> k = hydroConsts<T>(s);
+    ChainArrays<T> l = a;
+    l.groupList      = s.activeList;
+    l.numListed      = s.numActive;
+    l.groupDt        = s.groupDt.data();
+    SPHB_TRY(launchXMass(l, k, s.box, st));
+    SPHB_TRY(launchVeDefGradhEos(l, k, s.box, st));
+    SPHB_TRY(launchEosRefresh(a, k, st));
+    SPHB_TRY(launchIadDivvCurlv(l, k, s.box, st));
+    SPHB_TRY(launchGroupDivv(s.activeList, s.numActive, s.n, a.divv, float(s.p.Krho), s.groupDt.data(), st));
+    SPHB_TRY(launchAVswitches(l, k, s.box, s.minDt, st));
+    SPHB_TRY(launchMomentumEnergy(l, k, s.box, st));
+    return launchGroupAcc(s.activeList, s.numActive, s.n, a.ax, a.ay, a.az, s.f[fH].data(), s.etaAcc,
+                          s.groupDt.data(), st);
+}
+
+int bdtComputeForces(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    SPHB_TRY(bdtSync(s));
+    unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
+    SPHB_TRY(searchNeighbors(s));
+    SPHB_TRY(s.mixed ? bdtChain<float>(s) : bdtChain<double>(s));
+    double cv = idealGasCv(s.p.mui, s.p.gamma);
+    SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
+                           s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
+                           s.cons.data(), st));
+    double cons[9];
+    unsigned status = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (status) { return kErrCapacity; }
+    s.ecin           = 0.5 * cons[0];
+    s.eint           = cons[1];
+    s.etot           = s.ecin + s.eint;
+    s.linmom         = std::sqrt(cons[2] * cons[2] + cons[3] * cons[3] + cons[4] * cons[4]);
+    s.angmom         = std::sqrt(cons[5] * cons[5] + cons[6] * cons[6] + cons[7] * cons[7]);
+    s.totalNeighbors = cons[8];
+    return kOk;
+}
+
+/*! computeMinTimestep + findRungRanges (ts_rungs.hpp:84-146) on groupDt[0, num): sorts it (and groupIdx[0, num),
+ *  the permutation) and returns the smallest dt, the dt at index 0.4 num, and the lower bounds of 2^r min dt */
+int sortGroupDt(sphb_sim& s, unsigned num, float* minDt, float* fastDt, uint32_t lb[kMaxRungs])
+{
+    cudaStream_t st = s.stream;
+    SPHB_TRY(launchDtKeys(s.groupDt.data(), num, s.dtKeys.data(), s.groupIdx.data(), st));
+    SPHB_TRY(sortByKeyAsync(s.dtKeys.data(), s.groupIdx.data(), num, false, s.sortScratch.data(),
+                            s.sortScratch.capacity(), 0x0fu, s.status.data() + 2, st));
+    unsigned fastIdx = unsigned(0.4f * float(num)); // LocalIndex(fastFraction * numGroups), ts_rungs.hpp:86,102
+    SPHB_TRY(launchSortedDt(s.dtKeys.data(), num, fastIdx, s.groupDt.data(), s.rungInfo.data(), st));
+    uint32_t info[1 + kMaxRungs];
+    unsigned err = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(info, s.rungInfo.data(), sizeof(info), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.status.data() + 2, sizeof(err), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (err) { return kErrCuda; }
+    std::memcpy(minDt, &info[0], sizeof(float));
+    std::memcpy(fastDt, &info[1], sizeof(float));
+    lb[0] = 0;
+    for (int r = 1; r < kMaxRungs; ++r)
+    {
+        lb[r] = info[1 + r];
+    }
+    return kOk;
+}
+
+//! computeRungs (ve_hydro_bdt.hpp:299-334) with rungTimestep / minimumGroupDt (ts_rungs.hpp:148-166)
+int bdtComputeRungs(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    unsigned G      = unsigned(s.numGroups());
+    int highRung    = activeRungOf(s.bts.substep, s.bts.numRungs);
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 2, 0, sizeof(unsigned), st));
+    if (highRung == 0)
+    {
+        s.bprevTs   = s.bts;
+        float maxDt = float(double(s.bts.dtm1[0]) * 1.1); // maxDtIncrease (particles_data.hpp:138)
+        float minDt, fastDt;
+        uint32_t lb[kMaxRungs];
+        SPHB_TRY(sortGroupDt(s, G, &minDt, &fastDt, lb));
+        int numRungs = std::min(int(std::log2(fastDt / minDt)) + 1, kMaxRungs);
+        sphb_sim::BdtTimestep t{};
+        t.rungRanges[0] = 0;
+        for (int r = 1; r <= kMaxRungs; ++r)
+        {
+            t.rungRanges[r] = r < numRungs ? lb[r] : G;
+        }
+        minDt      = std::min(maxDt, minDt);
+        t.nextDt   = minDt;
+        t.totDt    = minDt * float(1 << numRungs);
+        t.numRungs = numRungs;
+        s.bts      = t;
+    }
+    else
+    {
+        unsigned numActive = s.bts.rungRanges[highRung];
+        unsigned numTot    = s.bts.rungRanges[kMaxRungs];
+        float minDt, fastDt;
+        uint32_t lb[kMaxRungs];
+        SPHB_TRY(sortGroupDt(s, numActive, &minDt, &fastDt, lb));
+        SPHB_TRY(launchSequence(s.groupIdx.data() + numActive, numTot - numActive, numActive, st));
+        float timeLeft   = s.bts.totDt - s.bts.elapsedDt;
+        int substepsLeft = (1 << s.bts.numRungs) - s.bts.substep;
+        s.bts.nextDt      = std::min(minDt, timeLeft / float(substepsLeft));
+        for (int r = 1; r < highRung; ++r)
+        {
+            s.bts.rungRanges[r] = lb[r];
+        }
+        s.bts.rungRanges[0] = 0;
+    }
+    if (highRung == 0 || highRung > 1)
+    {
+        if (highRung > 1) { s.grpSfc.swap(s.grpTs); }
+        SPHB_TRY(launchGatherGroups(s.grpSfc.data(), s.groupIdx.data(), s.bts.rungRanges[kMaxRungs], s.grpTs.data(),
+                                    st));
+    }
+    return kOk;
+}
+
+template<class T>
+IntegrateArrays<T> integrateArrays(sphb_sim& s)
+{
+    IntegrateArrays<T> a;
+    a.x    = s.f[fX].data();
+    a.y    = s.f[fY].data();
+    a.z    = s.f[fZ].data();
+    a.vx   = s.f[fVx].data();
+    a.vy   = s.f[fVy].data();
+    a.vz   = s.f[fVz].data();
+    a.xm1  = s.f[fXm1].data();
+    a.ym1  = s.f[fYm1].data();
+    a.zm1  = s.f[fZm1].data();
+    a.temp = s.f[fTemp].data();
+    a.duM1 = s.f[fDuM1].data();
+    a.du   = s.du.data();
+    a.ax   = s.dptr<T>(dAx);
+    a.ay   = s.dptr<T>(dAy);
+    a.az   = s.dptr<T>(dAz);
+    return a;
+}
+
+//! integrate of the block time-step propagator (ve_hydro_bdt.hpp:336-380)
+template<class T>
+int bdtIntegrateRungs(sphb_sim& s)
+{
+    cudaStream_t st          = s.stream;
+    IntegrateArrays<T> a     = integrateArrays<T>(s);
+    double cv                = idealGasCv(s.p.mui, s.p.gamma);
+    int lowestDriftRung      = butterflyOf(uint32_t(s.bts.substep + 1));
+    bool isLastSubstep       = activeRungOf(s.bts.substep + 1, s.bts.numRungs) == 0;
+    DevBox box               = s.box;
+    if (!isLastSubstep) { box.periodic[0] = box.periodic[1] = box.periodic[2] = 0; }
+    for (int i = 0; i < s.bts.numRungs; ++i)
+    {
+        bool useRung = s.bts.substep == s.bts.substep % (1 << i); // drift back to the start of the hierarchy
+        bool advance = i < lowestDriftRung;
+        float dt     = s.bts.nextDt;
+        RungSteps steps;
+        std::memcpy(steps.dtm1, useRung ? s.bprevTs.dtm1 : s.bts.dtm1, sizeof(steps.dtm1));
+        const uint32_t* list = s.grpTs.data() + s.bts.rungRanges[i];
+        unsigned num         = s.bts.rungRanges[i + 1] - s.bts.rungRanges[i];
+        if (advance)
+        {
+            if (s.bts.dtDrift[i] > 0)
+            {
+                SPHB_TRY(launchDrift(list, num, s.n, 0.f, s.bts.dtDrift[i], steps, s.rung.data(), a, cv, st));
+            }
+            SPHB_TRY(launchRungPositions(list, num, s.n, s.bts.dtDrift[i] + dt, steps, s.rung.data(), a, box, cv,
+                                         st));
+            s.bts.dtm1[i]    = s.bts.dtDrift[i] + dt;
+            s.bts.dtDrift[i] = 0;
+            SPHB_TRY(launchStoreRung(list, num, s.n, uint64_t(i), s.rung.data(), st));
+        }
+        else
+        {
+            SPHB_TRY(launchDrift(list, num, s.n, s.bts.dtDrift[i] + dt, s.bts.dtDrift[i], steps, s.rung.data(), a, cv,
+                                 st));
+            s.bts.dtDrift[i] += dt;
+        }
+    }
+    return kOk;
+}
+
+int bdtIntegrate(sphb_sim& s)
+{
+    cudaStream_t st = s.stream;
+    SPHB_TRY(bdtComputeRungs(s));
+    SPHB_TRY(s.mixed ? bdtIntegrateRungs<float>(s) : bdtIntegrateRungs<double>(s));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 1, 0, sizeof(unsigned), st));
+    SPHB_TRY(launchListUpdateH(s.activeList, s.numActive, s.n, s.p.ng0, s.nc.data(), s.f[fH].data(), s.keys.data(),
+                               s.status.data() + 1, st));
+    unsigned flag = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&flag, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    s.bts.substep++;
+    s.bts.elapsedDt += s.bts.nextDt;
+    s.ttot += double(s.bts.nextDt);
+    s.minDt_m1 = s.minDt;
+    s.minDt    = double(s.bts.nextDt);
+    s.iteration++;
+    return flag ? kErrNotConverged : kOk;
+}
+
 int allocateAdjoint(sphb_sim& s)
 {
     size_t n = s.n;
@@ -938,6 +1275,7 @@ extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const u
     s->iteration    = 1;
     s->uploaded     = true;
     s->forcesDone   = false;
+    if (s->bdt) { SPHB_TRY(resetBdt(*s)); }
     return SPHB_OK;
 }
 
@@ -954,7 +1292,7 @@ extern "C" int sphb_sim_initial_sync(sphb_sim* s)
 extern "C" int sphb_sim_compute_forces(sphb_sim* s)
 {
     if (!s) { return SPHB_ERR_ARG; }
-    if (!s->uploaded) { return SPHB_ERR_STATE; }
+    if (!s->uploaded || s->bdt) { return SPHB_ERR_STATE; }
     return computeForces(*s);
 }
 
@@ -972,12 +1310,56 @@ extern "C" int sphb_sim_step(sphb_sim* s)
     return sphb_sim_integrate(s);
 }
 
+extern "C" int sphb_sim_bdt_enable(sphb_sim* s, double eta_acc)
+{
+    if (!s || !(eta_acc > 0.0)) { return SPHB_ERR_ARG; }
+    if (s->p.av_clean || s->taping) { return SPHB_ERR_ARG; } // no AV-cleaning or adjoint variant of this propagator
+    SPHB_TRY(allocateBdt(*s));
+    s->bdt    = true;
+    s->etaAcc = float(eta_acc);
+    s->skinValid = false;
+    SPHB_TRY(resetBdt(*s));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SPHB_OK;
+}
+
+extern "C" int sphb_sim_bdt_step(sphb_sim* s)
+{
+    if (!s) { return SPHB_ERR_ARG; }
+    if (!s->uploaded || !s->bdt) { return SPHB_ERR_STATE; }
+    SPHB_TRY(bdtComputeForces(*s));
+    return bdtIntegrate(*s);
+}
+
+extern "C" int sphb_sim_bdt_timestep(const sphb_sim* s, sphb_bdt_timestep* out)
+{
+    if (!s || !out) { return SPHB_ERR_ARG; }
+    if (!s->bdt) { return SPHB_ERR_STATE; }
+    out->next_dt    = s->bts.nextDt;
+    out->elapsed_dt = s->bts.elapsedDt;
+    out->total_dt   = s->bts.totDt;
+    out->num_rungs  = s->bts.numRungs;
+    out->substep    = s->bts.substep;
+    for (int r = 0; r <= kMaxRungs; ++r)
+    {
+        out->rung_ranges[r] = s->bts.rungRanges[r];
+    }
+    for (int r = 0; r < kMaxRungs; ++r)
+    {
+        out->dt_m1[r]    = s->bts.dtm1[r];
+        out->dt_drift[r] = s->bts.dtDrift[r];
+    }
+    out->num_active = s->numActive;
+    return SPHB_OK;
+}
+
 namespace
 {
 
 int stageEntry(sphb_sim* s, int stage)
 {
     if (!s) { return SPHB_ERR_ARG; }
+    if (s->bdt) { return SPHB_ERR_STATE; }
     if (!s->uploaded) { return SPHB_ERR_STATE; }
     return runStageChecked(*s, stage);
 }
@@ -1068,6 +1450,12 @@ bool findField(sphb_sim* s, const char* name, void** ptr, int* kind)
     if (std::strcmp(name, "id") == 0)
     {
         *ptr  = s->id.data();
+        *kind = 3;
+        return true;
+    }
+    if (s->bdt && std::strcmp(name, "rung") == 0)
+    {
+        *ptr  = s->rung.data();
         *kind = 3;
         return true;
     }

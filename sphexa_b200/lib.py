@@ -31,6 +31,13 @@ class Box(C.Structure):
     _fields_ = [("lo", C.c_double * 3), ("hi", C.c_double * 3), ("periodic", C.c_int * 3)]
 
 
+class BdtTimestep(C.Structure):
+    """sphb_bdt_timestep: sph::Timestep of the block time-step propagator"""
+    _fields_ = [("next_dt", C.c_float), ("elapsed_dt", C.c_float), ("total_dt", C.c_float), ("num_rungs", C.c_int),
+                ("substep", C.c_int), ("rung_ranges", C.c_uint32 * 5), ("dt_m1", C.c_float * 4),
+                ("dt_drift", C.c_float * 4), ("num_active", C.c_uint32)]
+
+
 class Params(C.Structure):
     _fields_ = [("ng0", C.c_uint32), ("ngmax", C.c_uint32), ("gamma", C.c_double), ("mui", C.c_double),
                 ("Kcour", C.c_double), ("Krho", C.c_double), ("alphamin", C.c_double), ("alphamax", C.c_double),
@@ -43,7 +50,7 @@ class Params(C.Structure):
 EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sphb_sort_by_key_scratch_bytes",
             "sphb_sort_by_key", "sphb_gather8", "sphb_compute_octree", "sphb_sim_create", "sphb_sim_destroy",
             "sphb_sim_upload", "sphb_sim_initial_sync", "sphb_sim_compute_forces", "sphb_sim_integrate",
-            "sphb_sim_step", "sphb_sim_sync", "sphb_sim_find_neighbors", "sphb_sim_xmass",
+            "sphb_sim_step", "sphb_sim_bdt_enable", "sphb_sim_bdt_step", "sphb_sim_bdt_timestep", "sphb_sim_sync", "sphb_sim_find_neighbors", "sphb_sim_xmass",
             "sphb_sim_ve_def_gradh_eos", "sphb_sim_iad_divv_curlv", "sphb_sim_av_switches", "sphb_sim_momentum_energy",
             "sphb_sim_conserved", "sphb_sim_size", "sphb_sim_get_field", "sphb_sim_set_field", "sphb_sim_scalars",
             "sphb_sim_tree", "sphb_sim_neighbors", "sphb_sim_stage_times", "sphb_sim_kernel_launches",
@@ -83,6 +90,9 @@ def load() -> C.CDLL:
         "sphb_sim_compute_forces": (C.c_int, [P]),
         "sphb_sim_integrate": (C.c_int, [P]),
         "sphb_sim_step": (C.c_int, [P]),
+        "sphb_sim_bdt_enable": (C.c_int, [P, C.c_double]),
+        "sphb_sim_bdt_step": (C.c_int, [P]),
+        "sphb_sim_bdt_timestep": (C.c_int, [P, C.POINTER(BdtTimestep)]),
         "sphb_sim_sync": (C.c_int, [P]),
         "sphb_sim_find_neighbors": (C.c_int, [P]),
         "sphb_sim_xmass": (C.c_int, [P]),

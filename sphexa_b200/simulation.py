@@ -97,10 +97,28 @@ class Simulation:
         self.compute_forces()
         return self.integrate()
 
+    def enable_block_timesteps(self, eta_acc: float = 0.2):
+        """Switch to the block time-step propagator (HydroVeBdtProp, main/src/propagator/ve_hydro_bdt.hpp)."""
+        L.check(self.lib.sphb_sim_bdt_enable(self.h, float(eta_acc)), "bdt_enable")
+
+    def bdt_step(self) -> int:
+        """One substep of the block time-step propagator; returns 0 or 4 (particles with nc <= 1)."""
+        rc = self.lib.sphb_sim_bdt_step(self.h)
+        if rc not in (L.SPHB_OK, 4):
+            L.check(rc, "bdt_step")
+        return rc
+
+    def bdt_timestep(self) -> dict:
+        t = L.BdtTimestep()
+        L.check(self.lib.sphb_sim_bdt_timestep(self.h, C.byref(t)), "bdt_timestep")
+        return {"next_dt": t.next_dt, "elapsed_dt": t.elapsed_dt, "total_dt": t.total_dt, "num_rungs": t.num_rungs,
+                "substep": t.substep, "rung_ranges": list(t.rung_ranges), "dt_m1": list(t.dt_m1),
+                "dt_drift": list(t.dt_drift), "num_active": t.num_active}
+
     def get(self, name: str) -> np.ndarray:
         out = np.empty(self.n, dtype=np.float64)
         L.check(self.lib.sphb_sim_get_field(self.h, name.encode(), L.ptr(out), 0), f"get_field({name})")
-        if name in ("keys", "id"):
+        if name in ("keys", "id", "rung"):
             return out.view(np.uint64)
         return out
 

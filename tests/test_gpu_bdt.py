@@ -1,0 +1,155 @@
+"""GPU tests of the block time-step propagator (sphb_sim_bdt_*, main/src/propagator/ve_hydro_bdt.hpp) against its
+restatement over the C oracle (oracle/bdt.py), substep by substep. The reference runs this propagator only on
+GPUs, so the restatement is pinned through the oracle's J-loops (themselves pinned to the reference's CPU code) and
+by reading the cited sources. Integer state (rungs, rung ranges, particle order) must be equal; time steps are
+float32 values that must agree to a few ulp; fields are compared by relative error with the tolerance in each test."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib(cuda_device):
+    from sphexa_b200 import lib as L
+    return L.load()
+
+
+def _max_rel(a, b, floor=0.0):
+    d = np.abs(a - b)
+    s = np.maximum(np.abs(b), floor)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(s > 0, d / s, d)
+    return float(np.max(r)) if r.size else 0.0
+
+
+def _check_timestep(tg, to, where):
+    assert tg["num_rungs"] == to["num_rungs"], where
+    assert tg["substep"] == to["substep"], where
+    assert tg["rung_ranges"] == to["rung_ranges"], (where, tg["rung_ranges"], to["rung_ranges"])
+    for k in ("next_dt", "elapsed_dt", "total_dt"):
+        assert abs(tg[k] - to[k]) <= 4e-7 * abs(to[k]), (where, k, tg[k], to[k])
+    for k in ("dt_m1", "dt_drift"):
+        assert np.allclose(tg[k], to[k], rtol=4e-7, atol=0), (where, k)
+
+
+def test_bdt_fp64_vs_oracle(lib):
+    """Twelve substeps of Sedov 20^3 (one block of 8 substeps over 4 rungs and the start of the next)."""
+    from oracle.bdt import BdtOracle
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(20, seed=3)
+    o = BdtOracle(ic)
+    g = Simulation(ic, "fp64")
+    g.enable_block_timesteps(0.2)
+    rungs_seen = set()
+    for k in range(12):
+        assert o.step() == 0
+        assert g.bdt_step() == 0
+        tg, to = g.bdt_timestep(), o.ts.as_dict()
+        _check_timestep(tg, to, k)
+        rungs_seen.add(tg["num_rungs"])
+        assert tg["num_active"] == len(o.active), k
+        assert np.array_equal(g.get("id"), o.get("id")), k
+        assert np.array_equal(g.get("rung"), o.rung.astype(np.uint64)), k
+        assert np.array_equal(g.get("nc"), o.get("nc")), k
+        for f in ("x", "y", "z", "temp"):
+            assert _max_rel(g.get(f), o.get(f), floor=1e-3) < 1e-9, (k, f)
+        assert _max_rel(g.get("h"), o.get("h")) < 1e-12, k
+        for f in ("vx", "vy", "vz", "ax", "du", "alpha"):
+            b = o.get(f)
+            assert _max_rel(g.get(f), b, floor=1e-6 * np.max(np.abs(b))) < 1e-8, (k, f)
+    assert max(rungs_seen) > 1
+
+
+def test_bdt_first_substep_equals_global_forces(lib):
+    """The first substep has every group active after a full sync: its forces are those of the global step."""
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(24, seed=5)
+    a = Simulation(ic, "fp64")
+    a.compute_forces()
+    b = Simulation(ic, "fp64")
+    b.enable_block_timesteps(0.2)
+    b.bdt_step()
+    for f in ("xm", "kx", "gradh", "prho", "c", "c11", "divv", "alpha", "ax", "ay", "az", "du", "nc"):
+        assert np.array_equal(a.get(f), b.get(f)), f
+    t = b.bdt_timestep()
+    assert t["num_active"] == (b.n + 31) // 32
+
+
+def test_bdt_mixed_vs_oracle(lib):
+    """Mixed precision through one block: the rung structure follows the FP64 restatement and the fields stay within
+    the mixed form's tolerance."""
+    from oracle.bdt import BdtOracle
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(20, seed=3)
+    o = BdtOracle(ic)
+    g = Simulation(ic, "mixed")
+    g.enable_block_timesteps(0.2)
+    for k in range(8):
+        assert o.step() == 0
+        assert g.bdt_step() == 0
+        tg, to = g.bdt_timestep(), o.ts.as_dict()
+        assert tg["num_rungs"] == to["num_rungs"] and tg["rung_ranges"] == to["rung_ranges"], k
+        assert abs(tg["next_dt"] - to["next_dt"]) <= 1e-5 * to["next_dt"], k
+    for f in ("x", "y", "z"):
+        assert _max_rel(g.get(f), o.get(f), floor=1e-3) < 1e-7, f
+    for f in ("temp", "h"):
+        assert _max_rel(g.get(f), o.get(f)) < 1e-5, f
+    b = o.get("vx")
+    assert _max_rel(g.get("vx"), b, floor=1e-3 * np.max(np.abs(b))) < 1e-4
+
+
+def test_bdt_periodic_drift_out_of_box(lib):
+    """A uniform flow across the periodic boundary: between full syncs particles drift past the box faces without
+    folding and without a resort; the lists (and so nc and the forces) must still match the oracle's exact search."""
+    from oracle.bdt import BdtOracle
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(16, seed=9)
+    # a bulk flow of about one lattice spacing per block of substeps; Sedov's hot centre keeps several rungs
+    ic["vx"] = ic["vx"] + 1.0e4
+    ic["x_m1"] = ic["vx"] * ic["params"]["minDt"]
+    o = BdtOracle(ic)
+    g = Simulation(ic, "fp64")
+    g.enable_block_timesteps(0.2)
+    outside = 0
+    for k in range(10):
+        assert o.step() == 0
+        assert g.bdt_step() == 0
+        _check_timestep(g.bdt_timestep(), o.ts.as_dict(), k)
+        assert np.array_equal(g.get("nc"), o.get("nc")), k
+        x = g.get("x")
+        outside += int(np.sum((x > 0.5) | (x < -0.5)))
+        assert _max_rel(x, o.get("x"), floor=1e-3) < 1e-9, k
+        b = o.get("ax")
+        assert _max_rel(g.get("ax"), b, floor=1e-6 * np.max(np.abs(b))) < 1e-8, k
+    assert outside > 0  # the case this test is for happened
+
+
+def test_bdt_state_errors(lib):
+    from sphexa_b200 import ic as icm
+    from sphexa_b200 import lib as L
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(12)
+    g = Simulation(ic, "fp64")
+    with pytest.raises(L.SphbError) as e:
+        g.bdt_timestep()
+    assert e.value.code == L.SPHB_ERR_STATE
+    with pytest.raises(L.SphbError):
+        g.enable_block_timesteps(0.0)
+    g.enable_block_timesteps(0.2)
+    with pytest.raises(L.SphbError) as e:
+        g.compute_forces()
+    assert e.value.code == L.SPHB_ERR_STATE
+    with pytest.raises(L.SphbError) as e:
+        g.sync()
+    assert e.value.code == L.SPHB_ERR_STATE
+    av = dict(ic)
+    av["params"] = dict(ic["params"], avClean=True)
+    h = Simulation(av, "fp64")
+    with pytest.raises(L.SphbError) as e:
+        h.enable_block_timesteps(0.2)
+    assert e.value.code == L.SPHB_ERR_ARG
