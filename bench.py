@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg (48^3, 20 steps)")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-instance ensemble leg")
     ap.add_argument("--no-noh", action="store_true", help="skip the Noh 160^3 leg")
+    ap.add_argument("--no-bdt", action="store_true", help="skip the block time-step leg (Sedov 128^3)")
     return ap.parse_args()
 
 
@@ -449,6 +450,8 @@ def run_ours(args, ws, rank, local):
         line["ensemble"] = ensemble_leg()
     if rank == 0 and not args.no_noh:
         line["noh"] = noh_leg()
+    if rank == 0 and not args.no_bdt:
+        line["block_timesteps"] = bdt_leg()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ic, n)
     if dist is not None:
@@ -555,6 +558,79 @@ def noh_leg(side=160, steps=150, warmup=3) -> dict:
            "particles": n, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
            "particle_steps_per_s": n * steps / (ms * 1e-3), "max_density": float(rho.max()),
            "time": s["ttot"], "energy_drift": abs(s["etot"] - e0) / abs(e0)}
+    sim.close()
+    return out
+
+
+def bdt_leg(side=128, blocks=2, steps=16, warmup=3, min_dt=1e-4) -> dict:
+    """Block time steps (main/src/propagator/ve_hydro_bdt.hpp) against the global step on Sedov side^3, mixed
+    precision, each from its own fresh start after warm-up (the global propagator: `warmup` steps; the block one: its
+    first block). The previous time step starts at min_dt, above the Courant limit of the blast centre, so that both
+    propagators step at that limit from the start instead of growing their step by 1.1x per step (global) or per
+    block (block time steps). CUDA events on each simulation's stream around `steps` global steps and around `blocks`
+    complete blocks of substeps. Reported: time per step / substep, the simulated time each advances per second, the
+    share of groups whose forces the substeps computed and the groups per rung of the last block."""
+    import torch
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(side)
+    ic["params"] = dict(ic["params"], minDt=min_dt, minDt_m1=min_dt)
+    n = ic["x"].size
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+
+    glob = Simulation(ic, "mixed")
+    stream = torch.cuda.ExternalStream(glob.lib.sphb_sim_stream(glob.h))
+    for _ in range(warmup):
+        glob.step()
+    t0 = glob.scalars()["ttot"]
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(steps):
+        glob.step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_glob = a.elapsed_time(b)
+    dt_glob = glob.scalars()["ttot"] - t0
+    glob.close()
+
+    sim = Simulation(ic, "mixed")
+    sim.enable_block_timesteps(0.2)
+    stream = torch.cuda.ExternalStream(sim.lib.sphb_sim_stream(sim.h))
+
+    def one_block():
+        count, active = 0, 0
+        while True:
+            sim.bdt_step()
+            t = sim.bdt_timestep()
+            count += 1
+            active += t["num_active"]
+            if t["substep"] >= (1 << (t["num_rungs"] - 1)):
+                return count, active, t
+
+    one_block()
+    t0 = sim.scalars()["ttot"]
+    torch.cuda.synchronize()
+    a.record(stream)
+    substeps, active, last = 0, 0, None
+    for _ in range(blocks):
+        c, act, last = one_block()
+        substeps += c
+        active += act
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_bdt = a.elapsed_time(b)
+    dt_bdt = sim.scalars()["ttot"] - t0
+    groups = (n + 31) // 32
+    r = last["rung_ranges"]
+    out = {"workload": f"sedov-{side}^3 ({n:,} particles), mixed precision, eta_acc 0.2, first dt_m1 {min_dt:g}",
+           "global": {"steps": steps, "ms_per_step": ms_glob / steps, "simulated_time": dt_glob,
+                      "simulated_time_per_s": dt_glob / (ms_glob * 1e-3)},
+           "block": {"blocks": blocks, "substeps": substeps, "ms_per_substep": ms_bdt / substeps,
+                     "simulated_time": dt_bdt, "simulated_time_per_s": dt_bdt / (ms_bdt * 1e-3),
+                     "active_group_share": active / (substeps * groups), "base_dt_last": last["next_dt"],
+                     "groups_per_rung_last_block": [r[k + 1] - r[k] for k in range(last["num_rungs"])]}}
+    out["simulated_time_ratio"] = out["block"]["simulated_time_per_s"] / out["global"]["simulated_time_per_s"]
     sim.close()
     return out
 

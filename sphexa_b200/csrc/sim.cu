@@ -534,8 +534,7 @@ int searchNeighbors(sphb_sim& s)
                              s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), st);
     };
 
-    // block time steps drift particles without a resort, which the displacement bounds of the rows do not track
-    bool useSkin = s.p.nb_skin > 0.0 && !s.taping && !s.bdt;
+    bool useSkin = s.p.nb_skin > 0.0 && !s.taping;
     if (!useSkin || s.skinHoldoff > 0)
     {
         if (s.skinHoldoff > 0) { --s.skinHoldoff; }

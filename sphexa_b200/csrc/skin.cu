@@ -87,11 +87,25 @@ __device__ inline double displacement(double x, double y, double z, double bx, d
     return sqrt(dx * dx + dy * dy + dz * dz);
 }
 
-//! grid cell of a coordinate on one axis, clamped to the grid (positions lie in the box; rounding may touch the edge)
-__device__ inline int cellOf(double v, double lo, double ilen)
+/*! grid cell of a coordinate on one axis: wrapped on a periodic axis, clamped on an open one, as checkGroup maps
+ *  the search ranges (positions outside the box occur between domain syncs under block time steps) */
+__device__ inline int cellOf(double v, double lo, double ilen, int periodic)
 {
-    int c = int(floor((v - lo) * ilen * kSkinGrid));
-    return min(max(c, 0), kSkinGrid - 1);
+    double f = floor((v - lo) * ilen * kSkinGrid);
+    if (periodic)
+    {
+        int c = int(f - double(kSkinGrid) * floor(f * (1.0 / kSkinGrid)));
+        return min(max(c, 0), kSkinGrid - 1);
+    }
+    return int(fmin(fmax(f, 0.0), double(kSkinGrid - 1)));
+}
+
+__device__ inline int gridCell(double x, double y, double z, const DevBox& box)
+{
+    return (cellOf(x, box.lo[0], box.ilen[0], box.periodic[0]) * kSkinGrid +
+            cellOf(y, box.lo[1], box.ilen[1], box.periodic[1])) *
+               kSkinGrid +
+           cellOf(z, box.lo[2], box.ilen[2], box.periodic[2]);
 }
 
 __global__ void skinDisplacementKernel(const double4* __restrict__ pos, const double* __restrict__ xb,
@@ -113,16 +127,11 @@ __global__ void skinDisplacementKernel(const double4* __restrict__ pos, const do
         // rounded up, so that the grid bounds the FP64 value
         bits = __float_as_uint(__double2float_ru(d));
         const int gridBase = inst ? int(inst[i]) * kSkinCells : 0;
-        cell = gridBase + (cellOf(p.x, box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(p.y, box.lo[1], box.ilen[1])) *
-                              kSkinGrid +
-               cellOf(p.z, box.lo[2], box.ilen[2]);
+        cell = gridBase + gridCell(p.x, p.y, p.z, box);
         // The displacement also goes to the cell of the build position, which every group whose rows list this
         // particle checks: the refilter decides most entries from their build distance and these bounds. A particle
         // at another index than at the build makes those rows stale: infinite there.
-        int cb = gridBase +
-                 (cellOf(xb[b], box.lo[0], box.ilen[0]) * kSkinGrid + cellOf(yb[b], box.lo[1], box.ilen[1])) *
-                     kSkinGrid +
-                 cellOf(zb[b], box.lo[2], box.ilen[2]);
+        int cb = gridBase + gridCell(xb[b], yb[b], zb[b], box);
         unsigned atBuild = b != i ? __float_as_uint(INFINITY) : bits;
         if (cb != cell && atBuild != 0u) { atomicMax(grid + cb, atBuild); }
         else if (cb == cell) { bits = max(bits, atBuild); }

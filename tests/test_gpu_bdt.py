@@ -33,12 +33,15 @@ def _check_timestep(tg, to, where):
         assert np.allclose(tg[k], to[k], rtol=4e-7, atol=0), (where, k)
 
 
-def test_bdt_fp64_vs_oracle(lib):
-    """Twelve substeps of Sedov 20^3 (one block of 8 substeps over 4 rungs and the start of the next)."""
+@pytest.mark.parametrize("skin", [0.0, 0.05])
+def test_bdt_fp64_vs_oracle(lib, skin):
+    """Twelve substeps of Sedov 20^3 (one block of 8 substeps over 4 rungs and the start of the next), with the tree
+    searched every substep or skin rows refiltered."""
     from oracle.bdt import BdtOracle
     from sphexa_b200 import ic as icm
     from sphexa_b200.simulation import Simulation
     ic = icm.sedov(20, seed=3)
+    ic["params"] = dict(ic["params"], nbSkin=skin)
     o = BdtOracle(ic)
     g = Simulation(ic, "fp64")
     g.enable_block_timesteps(0.2)
@@ -60,6 +63,8 @@ def test_bdt_fp64_vs_oracle(lib):
             b = o.get(f)
             assert _max_rel(g.get(f), b, floor=1e-6 * np.max(np.abs(b))) < 1e-8, (k, f)
     assert max(rungs_seen) > 1
+    if skin > 0:
+        assert g.search_stats()["skin_steps"] >= 6
 
 
 def test_bdt_first_substep_equals_global_forces(lib):
@@ -102,13 +107,16 @@ def test_bdt_mixed_vs_oracle(lib):
     assert _max_rel(g.get("vx"), b, floor=1e-3 * np.max(np.abs(b))) < 1e-4
 
 
-def test_bdt_periodic_drift_out_of_box(lib):
+@pytest.mark.parametrize("skin", [0.0, 0.05])
+def test_bdt_periodic_drift_out_of_box(lib, skin):
     """A uniform flow across the periodic boundary: between full syncs particles drift past the box faces without
-    folding and without a resort; the lists (and so nc and the forces) must still match the oracle's exact search."""
+    folding and without a resort; the lists (and so nc and the forces) must still match the oracle's exact search,
+    through the widened tree search and through the skin rows' wrapped displacement grid."""
     from oracle.bdt import BdtOracle
     from sphexa_b200 import ic as icm
     from sphexa_b200.simulation import Simulation
     ic = icm.sedov(16, seed=9)
+    ic["params"] = dict(ic["params"], nbSkin=skin)
     # a bulk flow of about one lattice spacing per block of substeps; Sedov's hot centre keeps several rungs
     ic["vx"] = ic["vx"] + 1.0e4
     ic["x_m1"] = ic["vx"] * ic["params"]["minDt"]
