@@ -598,23 +598,28 @@ def bdt_leg(side=128, blocks=2, steps=16, warmup=3, min_dt=1e-4) -> dict:
     sim.enable_block_timesteps(0.2)
     stream = torch.cuda.ExternalStream(sim.lib.sphb_sim_stream(sim.h))
 
-    def one_block():
+    stage_sum = {}
+
+    def one_block(timed):
         count, active = 0, 0
         while True:
             sim.bdt_step()
             t = sim.bdt_timestep()
             count += 1
             active += t["num_active"]
+            if timed:
+                for key, v in sim.stage_times().items():
+                    stage_sum[key] = stage_sum.get(key, 0.0) + v
             if t["substep"] >= (1 << (t["num_rungs"] - 1)):
                 return count, active, t
 
-    one_block()
+    one_block(False)
     t0 = sim.scalars()["ttot"]
     torch.cuda.synchronize()
     a.record(stream)
     substeps, active, last = 0, 0, None
     for _ in range(blocks):
-        c, act, last = one_block()
+        c, act, last = one_block(True)
         substeps += c
         active += act
     b.record(stream)
@@ -629,7 +634,8 @@ def bdt_leg(side=128, blocks=2, steps=16, warmup=3, min_dt=1e-4) -> dict:
            "block": {"blocks": blocks, "substeps": substeps, "ms_per_substep": ms_bdt / substeps,
                      "simulated_time": dt_bdt, "simulated_time_per_s": dt_bdt / (ms_bdt * 1e-3),
                      "active_group_share": active / (substeps * groups), "base_dt_last": last["next_dt"],
-                     "groups_per_rung_last_block": [r[k + 1] - r[k] for k in range(last["num_rungs"])]}}
+                     "groups_per_rung_last_block": [r[k + 1] - r[k] for k in range(last["num_rungs"])],
+                     "stage_ms_per_substep": {k: round(v / substeps, 4) for k, v in stage_sum.items()}}}
     out["simulated_time_ratio"] = out["block"]["simulated_time_per_s"] / out["global"]["simulated_time_per_s"]
     sim.close()
     return out

@@ -860,26 +860,37 @@ int bdtChain(sphb_sim& s)
     l.groupList      = s.activeList;
     l.numListed      = s.numActive;
     l.groupDt        = s.groupDt.data();
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
     SPHB_TRY(launchXMass(l, k, s.box, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sVeDefGradh], st));
     SPHB_TRY(launchVeDefGradhEos(l, k, s.box, st));
     SPHB_TRY(launchEosRefresh(a, k, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIad], st));
     SPHB_TRY(launchIadDivvCurlv(l, k, s.box, st));
     SPHB_TRY(launchGroupDivv(s.activeList, s.numActive, s.n, a.divv, float(s.p.Krho), s.groupDt.data(), st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sAV], st));
     SPHB_TRY(launchAVswitches(l, k, s.box, s.minDt, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sMomentum], st));
     SPHB_TRY(launchMomentumEnergy(l, k, s.box, st));
     return launchGroupAcc(s.activeList, s.numActive, s.n, a.ax, a.ay, a.az, s.f[fH].data(), s.etaAcc,
                           s.groupDt.data(), st);
 }
 
+/*! Stage events as the global step records them (sphb_sim_stage_times): sync, neighbours, the five J-loops (with
+ *  the EOS of every particle in VeDefGradh and the group time steps in IAD and MomentumEnergy), conserved sums, and
+ *  the integration with the rung sort. */
 int bdtComputeForces(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sSync], st));
     SPHB_TRY(bdtSync(s));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sNeighbors], st));
     unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
     SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
     SPHB_TRY(searchNeighbors(s));
     SPHB_TRY(s.mixed ? bdtChain<float>(s) : bdtChain<double>(s));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sConserved], st));
     double cv = idealGasCv(s.p.mui, s.p.gamma);
     SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
                            s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
@@ -888,6 +899,7 @@ int bdtComputeForces(sphb_sim& s)
     unsigned status = 0;
     SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIntegrate], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
     if (status) { return kErrCapacity; }
     s.ecin           = 0.5 * cons[0];
@@ -1052,7 +1064,12 @@ int bdtIntegrate(sphb_sim& s)
                                s.status.data() + 1, st));
     unsigned flag = 0;
     SPHB_CUDA_TRY(cudaMemcpyAsync(&flag, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaEventRecord(s.ev[kNumStages], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int k = 0; k < kNumStages; ++k)
+    {
+        cudaEventElapsedTime(&s.stageMs[k], s.ev[k], s.ev[k + 1]);
+    }
     s.bts.substep++;
     s.bts.elapsedDt += s.bts.nextDt;
     s.ttot += double(s.bts.nextDt);
