@@ -451,12 +451,23 @@ HydroConsts<T> hydroConsts(const sphb_sim& s)
     return k;
 }
 
+/*! Block size of a J-loop launch. 256 threads (8 consecutive groups per block share their neighbours in L1) except
+ *  the FP64 AV switches and MomentumEnergy, whose register counts leave more warps resident at 128. Measured at 128^3:
+ *  FP32 step 6.09 -> 6.04 ms; FP64 XMass, VeDefGradh, IAD 7.07 -> 6.86 ms, while FP64 MomentumEnergy went 5.33 ->
+ *  6.61 ms at 256. */
+int chainThreads(bool mixed, int stage)
+{
+    if (mixed) { return 256; }
+    return stage == sAV || stage == sMomentum ? 128 : 256;
+}
+
 template<class T>
 int runChainStage(sphb_sim& s, int stage)
 {
     cudaStream_t st  = s.stream;
     ChainArrays<T> a = chainArrays<T>(s);
     HydroConsts<T> k = hydroConsts<T>(s);
+    a.threads        = chainThreads(s.mixed, stage);
     switch (stage)
     {
     case sXMass: return launchXMass(a, k, s.box, st);
@@ -861,16 +872,21 @@ int bdtChain(sphb_sim& s)
     l.numListed      = s.numActive;
     l.groupDt        = s.groupDt.data();
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
+    l.threads = chainThreads(s.mixed, sXMass);
     SPHB_TRY(launchXMass(l, k, s.box, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sVeDefGradh], st));
+    l.threads = chainThreads(s.mixed, sVeDefGradh);
     SPHB_TRY(launchVeDefGradhEos(l, k, s.box, st));
     SPHB_TRY(launchEosRefresh(a, k, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIad], st));
+    l.threads = chainThreads(s.mixed, sIad);
     SPHB_TRY(launchIadDivvCurlv(l, k, s.box, st));
     SPHB_TRY(launchGroupDivv(s.activeList, s.numActive, s.n, a.divv, float(s.p.Krho), s.groupDt.data(), st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sAV], st));
+    l.threads = chainThreads(s.mixed, sAV);
     SPHB_TRY(launchAVswitches(l, k, s.box, s.minDt, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sMomentum], st));
+    l.threads = chainThreads(s.mixed, sMomentum);
     SPHB_TRY(launchMomentumEnergy(l, k, s.box, st));
     return launchGroupAcc(s.activeList, s.numActive, s.n, a.ax, a.ay, a.az, s.f[fH].data(), s.etaAcc,
                           s.groupDt.data(), st);
