@@ -196,16 +196,24 @@ __global__ void __launch_bounds__(kRedThreads) conservedPartialKernel(size_t n, 
     }
 }
 
+//! the 9 block partials reduced in a fixed order (deterministic): warp q sums quantity q, lane l the blocks
+//! l, l + 32, ... in turn, then a fixed shuffle tree over the lanes
 __global__ void conservedFinalKernel(const double* partial, int numBlocks, double* out)
 {
-    int q = threadIdx.x;
+    int q    = threadIdx.x >> 5;
+    int lane = threadIdx.x & 31;
     if (q >= 9) { return; }
     double s = 0;
-    for (int b = 0; b < numBlocks; ++b)
+    for (int b = lane; b < numBlocks; b += 32)
     {
         s += partial[b * 9 + q];
     }
-    out[q] = s;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        s += __shfl_xor_sync(0xffffffffu, s, off);
+    }
+    if (lane == 0) { out[q] = s; }
 }
 
 __global__ void minMaxKernel(const double* v, size_t n, unsigned long long* out)
@@ -292,7 +300,7 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
 {
     int blocks = int(std::min<size_t>(std::max<size_t>(ceilDiv(n, kRedThreads), 1), size_t(maxBlocks)));
     conservedPartialKernel<<<blocks, kRedThreads, 0, s>>>(n, x, y, z, vx, vy, vz, m, temp, nc, cv, partial);
-    conservedFinalKernel<<<1, 32, 0, s>>>(partial, blocks, out9);
+    conservedFinalKernel<<<1, 9 * 32, 0, s>>>(partial, blocks, out9);
     countLaunch(2);
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;

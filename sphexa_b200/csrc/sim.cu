@@ -156,6 +156,9 @@ struct sphb_sim
 
     cudaEvent_t ev[kNumStages + 1]{};
     float stageMs[kNumStages]{};
+    // pinned landing place of the small per-step reads (sums, reductions, status), so that they queue behind the
+    // kernels and the host waits once
+    unsigned long long* hostMsg{nullptr};
 
     size_t elemBytes() const { return mixed ? sizeof(float) : sizeof(double); }
     size_t numGroups() const { return (n + kWarp - 1) / kWarp; }
@@ -204,6 +207,7 @@ int allocateSim(sphb_sim& s)
     }
     SPHB_TRY(s.reduce.reserve(4));
     SPHB_TRY(s.status.reserve(4));
+    SPHB_CUDA_TRY(cudaMallocHost(reinterpret_cast<void**>(&s.hostMsg), 32 * sizeof(unsigned long long)));
     SPHB_TRY(s.partial.reserve(9 * 1024));
     SPHB_TRY(s.cons.reserve(16));
 
@@ -672,19 +676,26 @@ int runStage(sphb_sim& s, int stage)
     SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
                            s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
                            s.cons.data(), st));
-    double cons[9];
-    unsigned long long red[2];
-    unsigned status = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(red, s.reduce.data(), sizeof(red), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    unsigned deferred[2] = {0, 0};
+    // hostMsg: [0, 9) the sums, [9, 11) the two reductions, [11] status, [12] the two deferred counts
+    unsigned long long* msg = s.hostMsg;
+    std::memset(msg + 11, 0, 2 * sizeof(unsigned long long));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg, s.cons.data(), 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 9, s.reduce.data(), 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                  st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 11, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     if (s.skinFiltered)
     {
-        SPHB_CUDA_TRY(cudaMemcpyAsync(deferred, s.skinWork.data(), sizeof(deferred), cudaMemcpyDeviceToHost, st));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 12, s.skinWork.data(), 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     }
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIntegrate], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    double cons[9];
+    unsigned long long red[2];
+    unsigned status, deferred[2];
+    std::memcpy(cons, msg, sizeof(cons));
+    std::memcpy(red, msg + 9, sizeof(red));
+    std::memcpy(&status, msg + 11, sizeof(status));
+    std::memcpy(deferred, msg + 12, sizeof(deferred));
     s.skinDeferredLast = deferred[0] + deferred[1];
     s.searchStats[3] += s.skinDeferredLast;
     if (status) { return kErrCapacity; }
@@ -1256,7 +1267,7 @@ extern "C" int sphb_sim_create(sphb_sim** out, size_t n, const sphb_box* box, co
     if (rc == kOk) { rc = allocateSim(*s); }
     if (rc != kOk)
     {
-        delete s;
+        sphb_sim_destroy(s);
         return rc;
     }
     *out = s;
@@ -1279,6 +1290,7 @@ extern "C" int sphb_sim_destroy(sphb_sim* s)
     }
     if (s->skinFork) { cudaEventDestroy(s->skinFork); }
     if (s->skinJoin) { cudaEventDestroy(s->skinJoin); }
+    if (s->hostMsg) { cudaFreeHost(s->hostMsg); }
     delete s;
     return SPHB_OK;
 }
