@@ -37,10 +37,10 @@ KERNEL_STAGES = ("sync", "neighbors", "xmass", "ve_def_gradh_eos", "iad_divv_cur
 #: (stage, precision); scaled by the particle count of the run. From the capture of one steady-state launch each at
 #: Sedov 96^3 (884,736 particles), mixed precision: dram__bytes_read.sum + dram__bytes_write.sum / particles. The
 #: neighbour stage's figure is its refilter of the skin rows (the kernel of every step but the row builds).
-NCU_TRAFFIC = {("neighbors", "mixed"): (718.18e6 + 320.99e6) / 884736,
-               ("iad_divv_curlv", "mixed"): (412.73e6 + 73.93e6) / 884736,
-               ("av_switches", "mixed"): (473.59e6 + 29.04e6) / 884736,
-               ("momentum_energy", "mixed"): (437.91e6 + 19.61e6) / 884736}
+NCU_TRAFFIC = {("neighbors", "mixed"): (718.09e6 + 318.53e6) / 884736,
+               ("iad_divv_curlv", "mixed"): (412.24e6 + 73.40e6) / 884736,
+               ("av_switches", "mixed"): (474.71e6 + 29.72e6) / 884736,
+               ("momentum_energy", "mixed"): (437.29e6 + 20.36e6) / 884736}
 
 
 def parse():
