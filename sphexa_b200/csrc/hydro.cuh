@@ -11,6 +11,7 @@ constexpr int kPolyTerms = 13;
 
 //! largest block size a J-loop launch may use (ChainArrays::threads; the ensemble autotuner picks 64, 128 or 256)
 constexpr int kChainMaxThreads = 256;
+constexpr int kAvMaxThreads    = 384; // the AV switches, which need no block reduction
 
 //! physics constants of one simulation, in the J-loop type T
 template<class T>

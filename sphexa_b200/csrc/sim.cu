@@ -455,13 +455,13 @@ HydroConsts<T> hydroConsts(const sphb_sim& s)
     return k;
 }
 
-/*! Block size of a J-loop launch. 256 threads (8 consecutive groups per block share their neighbours in L1) except
- *  the FP64 AV switches and MomentumEnergy, whose register counts leave more warps resident at 128. Measured at 128^3:
- *  FP32 step 6.09 -> 6.04 ms; FP64 XMass, VeDefGradh, IAD 7.07 -> 6.86 ms, while FP64 MomentumEnergy went 5.33 ->
- *  6.61 ms at 256. */
+/*! Block size of a J-loop launch. 256 threads (8 consecutive groups per block share their neighbours in L1), the FP32
+ *  AV switches 384, and 128 for the FP64 AV switches and MomentumEnergy, whose register counts leave more warps
+ *  resident that way. Measured at 128^3 against 128 everywhere: FP32 step 6.09 -> 6.04 ms; FP64 XMass, VeDefGradh, IAD
+ *  7.07 -> 6.86 ms, while FP64 MomentumEnergy went 5.33 -> 6.61 ms at 256. */
 int chainThreads(bool mixed, int stage)
 {
-    if (mixed) { return 256; }
+    if (mixed) { return stage == sAV ? 384 : 256; }
     return stage == sAV || stage == sMomentum ? 128 : 256;
 }
 
