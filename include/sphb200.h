@@ -164,13 +164,12 @@ int sphb_sim_integrate(sphb_sim* sim);
 int sphb_sim_step(sphb_sim* sim);
 
 /*! Block time steps: switch this simulation to the propagator of main/src/propagator/ve_hydro_bdt.hpp
- *  (HydroVeBdtProp<avClean = false>). Groups are the fixed groups of 32 SFC-consecutive particles. Each group gets
+ *  (HydroVeBdtProp<avClean>, avClean from sphb_params.av_clean). Groups are the fixed groups of 32 SFC-consecutive particles. Each group gets
  *  the time step min(Courant, Krho / |max divv|, eta_acc (h^2/|a|^2)^(1/4)) over its particles (ts_groups.cu), the
  *  groups are sorted by it into up to 4 power-of-two rungs (ts_rungs.hpp:116-166), and a block step of
  *  2^(numRungs - 1) substeps computes forces only on the groups of the active rungs while the others drift.
  *  eta_acc: the acceleration criterion (ParticlesData::etaAcc, 0.2). After this call sphb_sim_compute_forces,
- *  sphb_sim_step and the stage calls return SPHB_ERR_STATE; sphb_sim_upload resets the block-step state.
- *  SPHB_ERR_ARG with AV cleaning. */
+ *  sphb_sim_step and the stage calls return SPHB_ERR_STATE; sphb_sim_upload resets the block-step state. */
 int sphb_sim_bdt_enable(sphb_sim* sim, double eta_acc);
 
 /*! One substep of the block time-step propagator: computeForces (domain sync at the first substep of a block,

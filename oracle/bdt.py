@@ -1,4 +1,4 @@
-"""TEST ORACLE ONLY: restatement of the block time-step propagator HydroVeBdtProp<avClean = false>
+"""TEST ORACLE ONLY: restatement of the block time-step propagator HydroVeBdtProp<avClean>
 (main/src/propagator/ve_hydro_bdt.hpp:165-380) with the rung logic of sph/include/sph/ts_rungs.hpp:84-166 and the
 group time steps of sph/include/sph/ts_groups.cu, over the plain-C oracle (oracle/sph_oracle.c) for the J-loops,
 drifts and kick-drifts. Imported only by tests/.

@@ -51,6 +51,7 @@ def load():
         "orc_sim_sync": (None, [P]),
         "orc_sim_compute_forces": (C.c_int, [P]),
         "orc_sim_integrate": (C.c_int, [P]),
+        "orc_sim_set_av_clean": (None, [P, C.c_int]),
         "orc_sim_size": (S, [P]),
         "orc_sim_get": (C.c_int, [P, C.c_char_p, P]),
         "orc_sim_keys": (None, [P, P]),
@@ -146,6 +147,8 @@ class OracleSim:
         self.ngmax = int(p["ngmax"])
         self.h = self.lib.orc_sim_create(ids.size, tbl, ptr(ids), ptr(lim), int(bool(ic["periodic"])), ptr(prm))
         self.n = ids.size
+        # HydroVeProp<avClean = true>: IAD keeps the velocity gradients, MomentumEnergy corrects r.v with them
+        self.lib.orc_sim_set_av_clean(self.h, int(bool(p.get("avClean", False))))
         self.lib.orc_sim_sync(self.h)
 
     def __del__(self):

@@ -832,10 +832,11 @@ static const char* const consNames[NUM_CONS] = {"x",  "y",  "z",    "h",    "m",
 enum
 {
     D_XM, D_KX, D_GRADH, D_PRHO, D_C, D_C11, D_C12, D_C13, D_C22, D_C23, D_C33, D_DIVV, D_CURLV, D_AX, D_AY, D_AZ,
-    D_DU, D_NC, NUM_DEP
+    D_DU, D_NC, D_DV11, D_DV12, D_DV13, D_DV22, D_DV23, D_DV33, NUM_DEP
 };
-static const char* const depNames[NUM_DEP] = {"xm",  "kx",  "gradh", "prho", "c",     "c11", "c12", "c13", "c22",
-                                              "c23", "c33", "divv",  "curlv", "ax",   "ay",  "az",  "du",  "nc"};
+static const char* const depNames[NUM_DEP] = {"xm",   "kx",   "gradh", "prho", "c",    "c11",   "c12", "c13",
+                                              "c22",  "c23",  "c33",   "divv", "curlv", "ax",   "ay",  "az",
+                                              "du",   "nc",   "dV11",  "dV12", "dV13",  "dV22", "dV23", "dV33"};
 
 struct orc_sim
 {
@@ -852,6 +853,7 @@ struct orc_sim
     double minDt, minDt_m1, minDtCourant, minDtRho, ttot;
     double etot, ecin, eint, linmom, angmom, totalNeighbors;
     double iteration;
+    int avClean; /* HydroVeProp<avClean = true>: IAD keeps the velocity gradients, MomentumEnergy corrects r.v */
     double K;
     double wh[ORC_TABLE], whd[ORC_TABLE];
 };
@@ -991,7 +993,7 @@ static int computeForcesImpl(orc_sim* s, const uint8_t* active, double avDt, dou
     }
     const double* m = s->f[F_M];
     const double* cij[6] = {s->d[D_C11], s->d[D_C12], s->d[D_C13], s->d[D_C22], s->d[D_C23], s->d[D_C33]};
-    const double* dv[6]  = {0, 0, 0, 0, 0, 0};
+    const double* dv[6]  = {s->d[D_DV11], s->d[D_DV12], s->d[D_DV13], s->d[D_DV22], s->d[D_DV23], s->d[D_DV33]};
     double cv            = idealCv(s->mui, s->gamma);
     unsigned ng          = s->ngmax;
 #define CNT(i) (nc[i] - 1 < ng ? nc[i] - 1 : ng)
@@ -1037,6 +1039,10 @@ static int computeForcesImpl(orc_sim* s, const uint8_t* active, double avDt, dou
         double dvv[6];
         orc_divv_curlv((unsigned)i, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, s->f[F_VX], s->f[F_VY],
                        s->f[F_VZ], h, cij, s->wh, s->d[D_KX], s->d[D_XM], &s->d[D_DIVV][i], &s->d[D_CURLV][i], dvv);
+        for (int k = 0; k < 6; ++k)
+        {
+            s->d[D_DV11 + k][i] = dvv[k];
+        }
         maxDivv = s->d[D_DIVV][i] > maxDivv ? s->d[D_DIVV][i] : maxDivv;
     }
     /* rhoTimestep, sph/include/sph/ts_global.hpp:75-98 */
@@ -1067,9 +1073,9 @@ static int computeForcesImpl(orc_sim* s, const uint8_t* active, double avDt, dou
             continue;
         }
         double o[5];
-        orc_momentum_energy((unsigned)i, 0, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, s->f[F_VX], s->f[F_VY],
-                            s->f[F_VZ], h, m, s->d[D_PRHO], s->d[D_C], cij, 0.1, 0.2, 1.0 / (0.2 - 0.1), s->wh,
-                            s->d[D_KX], s->d[D_XM], s->f[F_ALPHA], dv, o);
+        orc_momentum_energy((unsigned)i, s->avClean, s->K, &s->box, s->nbr + i * ng, CNT(i), x, y, z, s->f[F_VX],
+                            s->f[F_VY], s->f[F_VZ], h, m, s->d[D_PRHO], s->d[D_C], cij, 0.1, 0.2, 1.0 / (0.2 - 0.1),
+                            s->wh, s->d[D_KX], s->d[D_XM], s->f[F_ALPHA], dv, o);
         s->d[D_AX][i] = o[0];
         s->d[D_AY][i] = o[1];
         s->d[D_AZ][i] = o[2];
@@ -1113,6 +1119,8 @@ int orc_sim_compute_forces(orc_sim* s)
     orc_sim_sync(s);
     return computeForcesImpl(s, NULL, s->minDt, NULL);
 }
+
+void orc_sim_set_av_clean(orc_sim* s, int on) { s->avClean = on != 0; }
 
 int orc_sim_forces_active(orc_sim* s, const uint8_t* active, double avDt, double* dtCourant)
 {

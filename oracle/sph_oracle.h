@@ -68,6 +68,7 @@ void orc_sim_destroy(orc_sim* s);
 void orc_sim_sync(orc_sim* s);
 void orc_sim_sync_perm(orc_sim* s, uint32_t* permOut);
 int orc_sim_forces_active(orc_sim* s, const uint8_t* active, double avDt, double* dtCourant);
+void orc_sim_set_av_clean(orc_sim* s, int on);
 void orc_drift(orc_sim* s, const uint32_t* idx, size_t cnt, float dt, float dtBack, const float* dtm1,
                const uint8_t* rung);
 void orc_rung_positions(orc_sim* s, const uint32_t* idx, size_t cnt, float dt, const float* dtm1, const uint8_t* rung,

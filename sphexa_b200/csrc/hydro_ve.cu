@@ -738,7 +738,6 @@ int chainModeAv(const ChainArrays<T>& a)
 {
     int mode = chainMode(a);
     if (mode < 0 || !a.dvrec) { return mode; }
-    if (mode & kModeList) { return -1; } // no AV-cleaning variant under block time steps
     return (mode & kModeTape) ? -1 : (mode | kModeAvClean); // the adjoint has no AV-cleaning variant
 }
 
@@ -750,6 +749,9 @@ int chainModeAv(const ChainArrays<T>& a)
     case kModeBatch: KERNEL<T, kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                  \
     case kModeAvClean: KERNEL<T, kModeAvClean><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;              \
     case kModeList: KERNEL<T, kModeList><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__); break;                    \
+    case kModeAvClean | kModeList:                                                                                      \
+        KERNEL<T, kModeAvClean | kModeList><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__);                          \
+        break;                                                                                                          \
     case kModeAvClean | kModeBatch:                                                                                     \
         KERNEL<T, kModeAvClean | kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(__VA_ARGS__);                         \
         break;                                                                                                          \
@@ -803,6 +805,9 @@ int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const D
             break;
         case kModeAvClean | kModeBatch:
             iadDivvCurlvFusedKernel<kModeAvClean | kModeBatch><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
+            break;
+        case kModeAvClean | kModeList:
+            iadDivvCurlvFusedKernel<kModeAvClean | kModeList><<<chainBlocks(a), a.threads, 0, s>>>(a, k, box);
             break;
         default: return kErrArg;
         }

@@ -1357,7 +1357,7 @@ extern "C" int sphb_sim_step(sphb_sim* s)
 extern "C" int sphb_sim_bdt_enable(sphb_sim* s, double eta_acc)
 {
     if (!s || !(eta_acc > 0.0)) { return SPHB_ERR_ARG; }
-    if (s->p.av_clean || s->taping) { return SPHB_ERR_ARG; } // no AV-cleaning or adjoint variant of this propagator
+    if (s->taping) { return SPHB_ERR_ARG; } // the adjoint has no block time-step variant
     SPHB_TRY(allocateBdt(*s));
     s->bdt    = true;
     s->etaAcc = float(eta_acc);

@@ -270,3 +270,24 @@ def test_oracle_multi_step_vs_reference(orc):
     sr, so = r.scalars(), s.scalars()
     for k in ("minDt", "ttot", "etot"):
         assert abs(so[k] - sr[k]) <= 1e-12 * abs(sr[k]), k
+
+
+def test_oracle_av_clean_vs_reference(orc):
+    """The restated step with AV cleaning (HydroVeProp<avClean = true>) against the reference's own compiled
+    avClean step: the velocity gradients of IAD and the corrected MomentumEnergy over three steps."""
+    ref = _ref()
+    from sphexa_b200 import ic as icm
+    ic = icm.sedov(14)
+    ic["params"] = dict(ic["params"], avClean=True)
+    r = ref.RefSim(ic)
+    s = orc.OracleSim(ic)
+    plain = orc.OracleSim(icm.sedov(14))
+    for _ in range(3):
+        r.step()
+        s.step()
+        plain.step()
+    for f in ("dV11", "dV12", "dV23", "ax", "ay", "du", "x", "vx", "temp"):
+        a, b = s.get(f), r.get(f)
+        assert np.max(np.abs(a - b)) <= 1e-11 * max(np.max(np.abs(b)), 1e-300), f
+    # the correction changes the accelerations where the viscosity acts (early in the blast by a few 1e-7)
+    assert np.max(np.abs(s.get("ax") - plain.get("ax"))) > 1e-7 * np.max(np.abs(plain.get("ax")))
