@@ -340,12 +340,13 @@ int sphb_ensemble_initial_sync(sphb_ensemble* ens);
 /*! Rebuild the per-instance focus trees from the current particle order (outside the captured step). */
 int sphb_ensemble_rebuild_trees(sphb_ensemble* ens);
 
-/*! Block sizes (multiples of 32, at most 256) of the five J-loop launches: XMass, VeDefGradh+EOS, IAD+divv/curlv,
- *  AV switches, MomentumEnergy. */
+/*! Block sizes (multiples of 32, at most 256; the AV switches of a mixed-precision ensemble at most 384) of the five
+ *  J-loop launches: XMass, VeDefGradh+EOS, IAD+divv/curlv, AV switches, MomentumEnergy. */
 int sphb_ensemble_set_threads(sphb_ensemble* ens, const int* threads5);
 
-/*! Time every J-loop at 64, 128 and 256 threads per block on the current state, keep the fastest, and write the
- *  choice to threads5_out (5 ints, may be null). The particle state is unchanged. */
+/*! Time every J-loop at 64, 128 and 256 threads per block (the AV switches of a mixed-precision ensemble also at
+ *  384) on the current state, keep the fastest, and write the choice to threads5_out (5 ints, may be null). The
+ *  particle state is unchanged. */
 int sphb_ensemble_autotune(sphb_ensemble* ens, int* threads5_out);
 
 /*! Advance every instance by steps steps; use_graph != 0 replays one captured step (captured on first use). */

@@ -36,6 +36,7 @@ namespace
 constexpr int kFields    = 14; // conserved fields, order x y z h m temp vx vy vz x_m1 y_m1 z_m1 du_m1 alpha
 constexpr int kNumCons   = 9;  // per-instance conserved sums
 constexpr int kJLoops    = 5;  // tunable J-loop launches
+constexpr int kAvLoop    = 3;  // their index of the AV switches
 constexpr int kMaxInst   = 254;
 const char* const kFieldNames[kFields] = {"x",  "y",  "z",    "h",    "m",    "temp",  "vx",
                                           "vy", "vz", "x_m1", "y_m1", "z_m1", "du_m1", "alpha"};
@@ -1032,8 +1033,9 @@ extern "C" int sphb_ensemble_set_threads(sphb_ensemble* e, const int* threads)
     if (!e || !threads) { return SPHB_ERR_ARG; }
     for (int q = 0; q < kJLoops; ++q)
     {
-        int t = threads[q];
-        if (t < 32 || t > kChainMaxThreads || t % 32) { return SPHB_ERR_ARG; }
+        int t   = threads[q];
+        int tmx = (q == kAvLoop && e->mixed) ? kAvMaxThreads : kChainMaxThreads;
+        if (t < 32 || t > tmx || t % 32) { return SPHB_ERR_ARG; }
     }
     std::copy(threads, threads + kJLoops, e->threads);
     return dropGraph(*e);
@@ -1084,7 +1086,8 @@ extern "C" int sphb_ensemble_autotune(sphb_ensemble* e, int* threads_out)
     cudaEvent_t a, b;
     SPHB_CUDA_TRY(cudaEventCreate(&a));
     SPHB_CUDA_TRY(cudaEventCreate(&b));
-    const int cand[3] = {64, 128, 256};
+    // 384 only for the FP32 AV switches, the one J-loop whose bound allows it
+    const int cand[4] = {64, 128, 256, 384};
     int rc            = kOk;
     for (int q = 0; q < kJLoops && rc == kOk; ++q)
     {
@@ -1092,11 +1095,12 @@ extern "C" int sphb_ensemble_autotune(sphb_ensemble* e, int* threads_out)
         int bestT  = e->threads[q];
         for (int c : cand)
         {
+            if (c > kChainMaxThreads && !(q == kAvLoop && e->mixed)) { continue; }
             e->threads[q] = c;
             float times[3];
             for (int r = 0; r < 3 && rc == kOk; ++r)
             {
-                if (q == 3)
+                if (q == kAvLoop)
                 {
                     cudaMemcpyAsync(e->f[13].data(), e->alphaBackup.data(), n * sizeof(double),
                                     cudaMemcpyDeviceToDevice, st);
