@@ -1,5 +1,7 @@
 // Kernels of the block time-step propagator (main/src/propagator/ve_hydro_bdt.hpp). Each listed group is one warp
 // of 32 consecutive particles; the lists are the dt-sorted group ids of one rung or of the active rungs.
+#include <algorithm>
+
 #include "bdt.cuh"
 #include "neighbors.cuh"
 #include "primitives.cuh"
@@ -193,24 +195,35 @@ __global__ void listUpdateHKernel(const uint32_t* groups, unsigned num, size_t n
     h[i]         = __dmul_rn(__dmul_rn(h[i], 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
 }
 
-__global__ void maxDisplacementKernel(const double* x, const double* y, const double* z, const double* xs,
-                                      const double* ys, const double* zs, size_t n, DevBox box,
-                                      unsigned long long* out)
+//! grid-stride maximum with one atomic per block: one per warp on the single word serialised ~65 k atomics at 128^3
+__global__ void __launch_bounds__(kBdtThreads) maxDisplacementKernel(const double* x, const double* y,
+                                                                     const double* z, const double* xs,
+                                                                     const double* ys, const double* zs, size_t n,
+                                                                     DevBox box, unsigned long long* out)
 {
-    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
     double d = 0.0;
-    if (i < n)
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
     {
-        d = fmax(fabs(minImage(x[i] - xs[i], box.len[0], box.ilen[0], box.periodic[0])),
-                 fabs(minImage(y[i] - ys[i], box.len[1], box.ilen[1], box.periodic[1])));
-        d = fmax(d, fabs(minImage(z[i] - zs[i], box.len[2], box.ilen[2], box.periodic[2])));
+        double di = fmax(fabs(minImage(x[i] - xs[i], box.len[0], box.ilen[0], box.periodic[0])),
+                         fabs(minImage(y[i] - ys[i], box.len[1], box.ilen[1], box.periodic[1])));
+        d         = fmax(d, fmax(di, fabs(minImage(z[i] - zs[i], box.len[2], box.ilen[2], box.periodic[2]))));
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1)
     {
         d = fmax(d, __shfl_xor_sync(0xffffffffu, d, off));
     }
-    if ((threadIdx.x & 31) == 0) { atomicMax(out, orderedBits(d)); }
+    __shared__ double warpMax[kBdtThreads / 32];
+    if ((threadIdx.x & 31) == 0) { warpMax[threadIdx.x >> 5] = d; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        for (int w = 1; w < int(blockDim.x >> 5); ++w)
+        {
+            d = fmax(d, warpMax[w]);
+        }
+        atomicMax(out, orderedBits(d));
+    }
 }
 
 __global__ void dtKeysKernel(const float* groupDt, unsigned num, uint64_t* keys, uint32_t* values)
@@ -347,7 +360,8 @@ int launchMaxDisplacement(const double* x, const double* y, const double* z, con
                           const double* zs, size_t n, const DevBox& box, unsigned long long* out, cudaStream_t s)
 {
     if (n == 0) { return kOk; }
-    maxDisplacementKernel<<<ceilDiv(n, kBdtThreads), kBdtThreads, 0, s>>>(x, y, z, xs, ys, zs, n, box, out);
+    unsigned blocks = unsigned(std::min<size_t>(ceilDiv(n, kBdtThreads), size_t(smCount()) * 8));
+    maxDisplacementKernel<<<blocks, kBdtThreads, 0, s>>>(x, y, z, xs, ys, zs, n, box, out);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
