@@ -922,12 +922,17 @@ int bdtComputeForces(sphb_sim& s)
     SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
                            s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
                            s.cons.data(), st));
-    double cons[9];
-    unsigned status = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(cons, s.cons.data(), sizeof(cons), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&status, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    // the sums and the status word through the pinned block, one wait
+    unsigned long long* msg = s.hostMsg;
+    msg[11]                 = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg, s.cons.data(), 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 11, s.status.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIntegrate], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    double cons[9];
+    unsigned status;
+    std::memcpy(cons, msg, sizeof(cons));
+    std::memcpy(&status, msg + 11, sizeof(status));
     if (status) { return kErrCapacity; }
     s.ecin           = 0.5 * cons[0];
     s.eint           = cons[1];
