@@ -676,7 +676,8 @@ int runStage(sphb_sim& s, int stage)
     SPHB_TRY(conservedSums(s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fVx].data(), s.f[fVy].data(),
                            s.f[fVz].data(), s.f[fM].data(), s.f[fTemp].data(), s.nc.data(), cv, s.partial.data(), 1024,
                            s.cons.data(), st));
-    // hostMsg: [0, 9) the sums, [9, 11) the two reductions, [11] status, [12] the two deferred counts
+    // hostMsg: [0, 9) the sums, [9, 11) the two reductions, [11] status, [12] the two deferred counts, [13] the h
+    // update's flag under block time steps
     unsigned long long* msg = s.hostMsg;
     std::memset(msg + 11, 0, 2 * sizeof(unsigned long long));
     SPHB_CUDA_TRY(cudaMemcpyAsync(msg, s.cons.data(), 9 * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -1094,10 +1095,12 @@ int bdtIntegrate(sphb_sim& s)
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 1, 0, sizeof(unsigned), st));
     SPHB_TRY(launchListUpdateH(s.activeList, s.numActive, s.n, s.p.ng0, s.nc.data(), s.f[fH].data(), s.keys.data(),
                                s.status.data() + 1, st));
-    unsigned flag = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&flag, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    s.hostMsg[13] = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(s.hostMsg + 13, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[kNumStages], st));
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    unsigned flag;
+    std::memcpy(&flag, s.hostMsg + 13, sizeof(flag));
     for (int k = 0; k < kNumStages; ++k)
     {
         cudaEventElapsedTime(&s.stageMs[k], s.ev[k], s.ev[k + 1]);
