@@ -4,8 +4,8 @@ VE chain, integration) on a Sedov blast of 128^3 = 2,097,152 particles.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--side S]
 
-Prints one JSON line (rank 0). For N > 1 (torchrun) every rank runs an independent replica of the workload (the
-path does not shard at one GPU), times are max-reduced over ranks and `value` is the whole-job
+Prints one JSON line (rank 0). For N > 1 (torchrun) every rank runs an independent replica of the workload (one
+simulation per GPU, no data-path collective), times are max-reduced over ranks and `value` is the whole-job
 throughput. `--impl reference` times the reference's own OpenMP CPU implementation (oracle/_ref, compiled from the
 reference sources) on this host's cores instead.
 """
@@ -453,7 +453,8 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and not args.no_bdt:
         line["block_timesteps"] = bdt_leg()
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(ic, n)
+        line["cpu_baseline"] = cpu_baseline(ic, n, steps=min(args.steps, REF_STEPS),
+                                            warmup=min(args.warmup, REF_WARMUP))
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -708,13 +709,22 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-def cpu_baseline(ic, n, steps=2, warmup=1, mixed=True):
-    """Reference OpenMP CPU step (oracle/_ref, reference default types unless mixed=False) on this host."""
+#: the CPU sample both CPU legs time: at most this many steps after at most REF_WARMUP warm-up steps
+REF_STEPS, REF_WARMUP = 10, 3
+
+
+def cpu_baseline(ic, n, steps=REF_STEPS, warmup=REF_WARMUP):
+    """The reference's own OpenMP CPU step on this host's cores, all threads: the reference-default-types build with
+    the compiler's default FP contraction for the widest x86-64 level the host supports (oracle/_ref/
+    libsphref_timed_*.so). Wall clock over `steps` steps after `warmup` (the first-call tree convergence of the
+    initial sync is outside)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(host_threads()))
     from oracle import refsim
-    if not refsim.available(mixed):
+    if not refsim.available("timed"):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": "oracle/_ref not built"}
-    r = refsim.RefSim(ic, mixed=mixed)
+    model, _ = refsim.host_cpu()
+    isa = refsim.timed_isa()
+    r = refsim.RefSim(ic, mixed="timed")
     for _ in range(warmup):
         r.step()
     t0 = time.perf_counter()
@@ -722,7 +732,8 @@ def cpu_baseline(ic, n, steps=2, warmup=1, mixed=True):
         r.step()
     dt = time.perf_counter() - t0
     return {"value": n * steps / dt, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]),
-            "kind": "reference",
+            "kind": "reference", "cpu_model": model,
+            "build": f"g++ -O3 -march=x86-64-{isa or 'v3 (parity build)'} -fopenmp, default FP contraction",
             "sample": f"{steps} steps after {warmup} warm-up of the same Sedov workload ({n:,} particles), reference "
                       f"CPU code with its default types (f64 coordinates, f32 hydro fields), wall clock"}
 
@@ -734,9 +745,9 @@ def run_reference(args, ws, rank):
     from sphexa_b200 import ic as icm
     ic = icm.sedov(args.side)
     n = ic["x"].size
-    # a bounded sample of the workload: at most 10 timed steps (~15 s on 16 cores) after up to 3 warm-up steps
-    steps = min(args.steps, 10)
-    warmup = min(args.warmup, 3)
+    # a bounded sample of the workload: at most 10 timed steps (~20 s on 16 cores) after up to 3 warm-up steps
+    steps = min(args.steps, REF_STEPS)
+    warmup = min(args.warmup, REF_WARMUP)
     base = cpu_baseline(ic, n, steps=steps, warmup=warmup)
     v = base["value"]
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": ws, "steps": steps,

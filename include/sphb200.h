@@ -30,6 +30,7 @@ extern "C" {
 #define SPHB_ERR_CAPACITY 3      /* a bounded device buffer or wait was exhausted (scratch, traversal, lookback)    */
 #define SPHB_ERR_NOT_CONVERGED 4 /* smoothing-length iteration left particles with nc <= 1 (update_h_gpu.cu:51-55) */
 #define SPHB_ERR_STATE 5         /* call out of order (e.g. step before upload)                                    */
+#define SPHB_ERR_TIMEOUT 6       /* a bounded device-side wait gave up (the sort's look-back); outputs are undefined */
 
 /* precision of the neighbour sums (the SPH-VE J-loops) */
 #define SPHB_FP64 0  /* every field and sum in double: the plain drop-in                                           */
@@ -90,22 +91,11 @@ size_t sphb_sort_by_key_scratch_bytes(size_t n);
 
 /*! Stable ascending sort of n (uint64 key, uint32 value) pairs in place, using caller scratch of at least
  *  sphb_sort_by_key_scratch_bytes(n) bytes. If init_values != 0, values are first set to 0..n-1 (the sequence +
- *  sort of GlobalAssignment::assign, domain/include/cstone/domain/assignment.hpp:110-112).
+ *  sort of GlobalAssignment::assign, domain/include/cstone/domain/assignment.hpp:110-112). Host-blocking: it reads
+ *  the digit histogram and the error word back. A look-back wait that gives up returns SPHB_ERR_TIMEOUT.
  *  Replaces cstone::sortByKeyGpu (domain/include/cstone/primitives/primitives_gpu.cu:308-339). */
 int sphb_sort_by_key(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* scratch, size_t scratch_bytes,
                      void* stream);
-
-/*! Same sort as sphb_sort_by_key, for callers that cannot allocate device memory: for example code whose device
- *  memory all belongs to another allocator (a framework's caching pool), or code running where cudaMalloc is not
- *  allowed or would synchronise the device. It calls no cudaMalloc, cudaFree or other allocating routine; its
- *  scratch is a fixed array of about 12.6 MB inside this library, which every GPU that loads the library keeps until
- *  the process exits. n may be at most sphb_sort_by_key_static_max() (1,048,576); larger n returns
- *  SPHB_ERR_CAPACITY and sorts nothing. The first call on a device looks up the array's device address (once per
- *  device); make that first call before any stream capture. All calls share the one array: calls that overlap on
- *  the GPU (on different streams or from different threads) race with each other, so run them one after another.
- *  The array keeps the previous call's contents; every call clears what it needs before use.
- *  No counterpart in the reference. */
-int sphb_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* stream);
 
 /*! Same result as sphb_sort_by_key with init_values = 1, for keys that are nearly in order (the particles of the
  *  previous step, which moved a fraction of a smoothing length). If no adjacent pair is out of order nothing moves
@@ -114,6 +104,21 @@ int sphb_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, int init
  *  No counterpart in the reference (it sorts from scratch every step, assignment.hpp:112). */
 int sphb_sort_by_key_nearly_sorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, size_t scratch_bytes,
                                    int* identity, void* stream);
+
+/*! Same sort as sphb_sort_by_key, for callers that cannot allocate device memory: for example code whose device
+ *  memory all belongs to another allocator (a framework's caching pool), or code running where cudaMalloc is not
+ *  allowed. It calls no cudaMalloc, cudaFree or other allocating routine; its scratch is a fixed array of about
+ *  12.6 MB inside this library. The array is reserved on a device when the library's device code is loaded there
+ *  (with lazy module loading, at the first call on that device at the latest) and kept until the process exits.
+ *  n may be at most sphb_sort_by_key_static_max() (1,048,576); larger n returns SPHB_ERR_CAPACITY and sorts
+ *  nothing. The first call in a CUDA context looks up the array's device address (once per context); make that
+ *  first call before any stream capture. Like sphb_sort_by_key, every call blocks the calling host thread: it
+ *  waits for the stream twice (the digit histogram and the error word are read back). All calls share the one
+ *  array: calls that overlap on the GPU (on different streams or from different threads) race with each other, so
+ *  run them one after another. The array keeps the previous call's contents; every call clears what it needs
+ *  before use. A look-back wait that gives up returns SPHB_ERR_TIMEOUT.
+ *  No counterpart in the reference. */
+int sphb_sort_by_key_static(uint64_t* keys, uint32_t* values, size_t n, int init_values, void* stream);
 
 /*! Largest n accepted by sphb_sort_by_key_static. */
 size_t sphb_sort_by_key_static_max(void);

@@ -14,15 +14,50 @@ KTABLE = 20000
 _LIBS = {}
 
 
-def ref_lib_path(mixed: bool = False) -> str:
+#: x86-64 feature levels of the timed builds, widest first, with the CPU flags each needs
+TIMED_ISAS = (("v4", ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl", "avx2", "fma", "bmi2")),
+              ("v3", ("avx2", "fma", "bmi2", "movbe")))
+
+
+def host_cpu() -> tuple[str, set]:
+    """Model name and feature flags of this host's CPU (from /proc/cpuinfo)."""
+    model, flags = "unknown", set()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model == "unknown":
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return model, flags
+
+
+def timed_isa() -> str | None:
+    """The widest x86-64 level whose timed build exists and that this host's CPU supports."""
+    _, flags = host_cpu()
+    for isa, need in TIMED_ISAS:
+        if all(f in flags for f in need) and os.path.exists(os.path.join(HERE, "_ref", f"libsphref_timed_{isa}.so")):
+            return isa
+    return None
+
+
+def ref_lib_path(mixed: bool | str = False) -> str:
+    """mixed=False: the FP64 parity build; True: the reference-default-types parity build; "timed": the
+    reference-default-types build with the compiler's default FP contraction for this host's widest ISA level (the
+    build the CPU baselines time), else the parity build of the same types."""
+    if mixed == "timed":
+        isa = timed_isa()
+        return os.path.join(HERE, "_ref", f"libsphref_timed_{isa}.so" if isa else "libsphref_mixed.so")
     return os.path.join(HERE, "_ref", "libsphref_mixed.so" if mixed else "libsphref.so")
 
 
-def available(mixed: bool = False) -> bool:
+def available(mixed: bool | str = False) -> bool:
     return os.path.exists(ref_lib_path(mixed))
 
 
-def load(mixed: bool = False):
+def load(mixed: bool | str = False):
     if mixed in _LIBS:
         return _LIBS[mixed]
     path = ref_lib_path(mixed)
@@ -73,8 +108,8 @@ SCALAR_NAMES = ("minDt", "minDt_m1", "minDtCourant", "minDtRho", "ttot", "etot",
 class RefSim:
     """One simulation of the reference CPU hydro step (1 rank, OpenMP)."""
 
-    def __init__(self, ic: dict, mixed: bool = False):
-        """ic["params"].get("avClean") selects HydroVeProp<avClean = true>."""
+    def __init__(self, ic: dict, mixed: bool | str = False):
+        """ic["params"].get("avClean") selects HydroVeProp<avClean = true>; mixed as in ref_lib_path."""
         from sphexa_b200.ic import CONSERVED_FIELDS
         self.lib = load(mixed)
         p = ic["params"]

@@ -44,6 +44,7 @@ enum Status : int
     kErrCapacity   = SPHB_ERR_CAPACITY,
     kErrNotConverged = SPHB_ERR_NOT_CONVERGED,
     kErrState        = SPHB_ERR_STATE,
+    kErrTimeout      = SPHB_ERR_TIMEOUT,
 };
 
 #define SPHB_CUDA_TRY(expr)                                                                                            \

@@ -9,6 +9,9 @@
 // Every spin on a predecessor's status is bounded; on timeout the pass records an error word that the host reads.
 #include <mutex>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "common.cuh"
 #include "sort.cuh"
 
@@ -390,7 +393,8 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
     uint32_t err = 0;
     SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
-    return err ? kErrCapacity : kOk;
+    // 1: a look-back wait gave up; 2: offsets left inconsistent by such a wait (nothing else produces them)
+    return err ? kErrTimeout : kOk;
 }
 
 int sortNearlySorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, size_t scratchBytes, bool* identity,
@@ -518,24 +522,55 @@ static __device__ __align__(256) unsigned char gStaticSortScratch[kStaticSortByt
 namespace
 {
 
-constexpr int kMaxDevices = 64;
+//! one looked-up address per CUDA context: a context created after cudaDeviceReset gets its own entry
+struct StaticScratchEntry
+{
+    CUcontext ctx;
+    void* addr;
+};
+constexpr int kMaxContexts = 64;
 std::mutex gStaticScratchMutex;
-void* gStaticScratchAddr[kMaxDevices] = {};
+StaticScratchEntry gStaticScratch[kMaxContexts] = {};
+int gStaticScratchNext                          = 0;
+PFN_cuCtxGetCurrent_v4000 gCtxGetCurrent        = nullptr;
 
-//! device address of gStaticSortScratch on the current device, looked up on the first call per device
+/*! Device address of gStaticSortScratch in the current context, looked up with the context's device current on the
+ *  first call in that context. The driver's cuCtxGetCurrent is reached through the runtime's entry-point query, so
+ *  this library does not link libcuda. */
 int staticSortScratch(void** ptr)
 {
-    int dev = 0;
-    SPHB_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) { return kErrArg; }
     std::lock_guard<std::mutex> lock(gStaticScratchMutex);
-    if (!gStaticScratchAddr[dev])
+    if (!gCtxGetCurrent)
     {
-        void* p = nullptr;
-        SPHB_CUDA_TRY(cudaGetSymbolAddress(&p, gStaticSortScratch));
-        gStaticScratchAddr[dev] = p;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SPHB_CUDA_TRY(cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !fn) { return kErrCuda; }
+        gCtxGetCurrent = reinterpret_cast<PFN_cuCtxGetCurrent_v4000>(fn);
     }
-    *ptr = gStaticScratchAddr[dev];
+    CUcontext ctx = nullptr;
+    if (gCtxGetCurrent(&ctx) != CUDA_SUCCESS) { return kErrCuda; }
+    if (!ctx)
+    {
+        // no context is current on this thread yet: make the current device's primary context current
+        int dev = 0;
+        SPHB_CUDA_TRY(cudaGetDevice(&dev));
+        SPHB_CUDA_TRY(cudaSetDevice(dev));
+        if (gCtxGetCurrent(&ctx) != CUDA_SUCCESS || !ctx) { return kErrCuda; }
+    }
+    for (const StaticScratchEntry& e : gStaticScratch)
+    {
+        if (e.ctx == ctx && e.addr)
+        {
+            *ptr = e.addr;
+            return kOk;
+        }
+    }
+    void* p = nullptr;
+    SPHB_CUDA_TRY(cudaGetSymbolAddress(&p, gStaticSortScratch));
+    gStaticScratch[gStaticScratchNext] = {ctx, p};
+    gStaticScratchNext                 = (gStaticScratchNext + 1) % kMaxContexts;
+    *ptr                               = p;
     return kOk;
 }
 

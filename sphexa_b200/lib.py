@@ -15,8 +15,9 @@ LIB_PATH = os.path.join(HERE, "libsphb200.so")
 
 SPHB_OK = 0
 SPHB_ERR_ARG, SPHB_ERR_CUDA, SPHB_ERR_CAPACITY, SPHB_ERR_NOT_CONVERGED, SPHB_ERR_STATE = 1, 2, 3, 4, 5
+SPHB_ERR_TIMEOUT = 6
 ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "capacity exhausted", 4: "smoothing length not converged",
-          5: "call out of order"}
+          5: "call out of order", 6: "bounded device wait gave up"}
 SPHB_FP64 = 0
 SPHB_MIXED = 1
 

@@ -1,6 +1,6 @@
 """Regenerate the golden fixtures of tests/golden/ from the reference (run where the reference sources are present):
 
-  python tests/golden/make_golden.py [/root/reference]
+  python tests/golden/make_golden.py [<reference source tree>]
 
 * ve_example_data.npy — the 99-particle x 31-column fixture of the reference's SPH kernel tests
   (sph/test/example_data.txt, read by sph/test/ve.cpp:69-77), as float64.
@@ -77,8 +77,13 @@ def reference_run(ic, path):
     np.savez_compressed(path, **out)
 
 
+def reference_root() -> str:
+    """$SPHEXA_REFERENCE, else the directory "reference" beside this repository."""
+    return os.environ.get("SPHEXA_REFERENCE", os.path.abspath(os.path.join(ROOT, "..", "reference")))
+
+
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else reference_root()
     ve_fixture(ref_root)
     from sphexa_b200 import ic as icm
     reference_run(icm.sedov(12), os.path.join(HERE, "sedov12_ref.npz"))
