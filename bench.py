@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-instance ensemble leg")
     ap.add_argument("--no-noh", action="store_true", help="skip the Noh 160^3 leg")
     ap.add_argument("--no-bdt", action="store_true", help="skip the block time-step leg (Sedov 128^3)")
+    ap.add_argument("--no-ref-parity", action="store_true",
+                    help="skip the per-field comparison of the GPU states with the reference CPU step (128^3)")
     return ap.parse_args()
 
 
@@ -248,6 +250,10 @@ def evaluation_errors(mixed_sim, fp64_sim, n) -> dict:
     tbl = (C.c_void_p * len(host))(*[h.data_ptr() for h in host])
     L.check(fp64_sim.lib.sphb_sim_store_state(fp64_sim.h, tbl, C.c_void_p(hid.data_ptr()), 0), "store_state")
     L.check(mixed_sim.lib.sphb_sim_load_state(mixed_sim.h, tbl, C.c_void_p(hid.data_ptr()), 0), "load_state")
+    # the AV switches integrate alpha over the previous time step: both take the FP64 run's
+    dt = fp64_sim.scalars()["minDt"]
+    fp64_sim.set_fixed_dt(dt)
+    mixed_sim.set_fixed_dt(dt)
     fp64_sim.compute_forces()
     mixed_sim.compute_forces()
     a = {f: mixed_sim.get(f) for f in EVAL_FIELDS}
@@ -452,6 +458,8 @@ def run_ours(args, ws, rank, local):
         line["noh"] = noh_leg()
     if rank == 0 and not args.no_bdt:
         line["block_timesteps"] = bdt_leg()
+    if rank == 0 and not args.no_ref_parity:
+        line["mixed_vs_reference"] = reference_parity_leg(args.side)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(ic, n, steps=min(args.steps, REF_STEPS),
                                             warmup=min(args.warmup, REF_WARMUP))
@@ -460,6 +468,62 @@ def run_ours(args, ws, rank, local):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def reference_parity_leg(side=128, steps=3) -> dict:
+    """Per-field error of the GPU states, mixed precision and plain FP64, against the reference's own CPU step
+    (oracle/_ref/libsphref.so, every field FP64, OpenMP on the host's cores) after `steps` steps from the same initial
+    state: density, internal energy and h per particle (relative), positions relative to the box, velocities and
+    accelerations and du relative to the field's largest magnitude, alpha relative; total energy; whether the FP64
+    path reproduced the neighbour counts and the SFC order exactly."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(host_threads()))
+    from oracle import refsim
+    from sphexa_b200 import ic as icm
+    from sphexa_b200.simulation import Simulation
+    if not refsim.available():
+        return {"unavailable": "oracle/_ref not built"}
+    ic = icm.sedov(side)
+    n = ic["x"].size
+    t0 = time.perf_counter()
+    r = refsim.RefSim(ic)
+    for _ in range(steps):
+        r.step()
+    t_ref = time.perf_counter() - t0
+    fields = ("id", "x", "y", "z", "h", "m", "temp", "vx", "vy", "vz", "kx", "xm", "ax", "ay", "az", "du", "alpha",
+              "nc")
+    snap_r = {f: r.get(f) for f in fields}
+    e_r = r.scalars()["etot"]
+    del r
+    out = {"workload": f"sedov-{side}^3 ({n:,} particles), {steps} steps from the initial state; reference: the "
+                       f"reference's CPU step with every field FP64 (parity build)",
+           "steps": steps, "reference_seconds": t_ref}
+    for prec in ("fp64", "mixed"):
+        g = Simulation(ic, prec)
+        for _ in range(steps):
+            g.step()
+        snap_g = {f: g.get(f) for f in fields}
+        e_g = g.scalars()["etot"]
+        g.close()
+        entry = {"same_sfc_order": bool(np.array_equal(snap_g["id"].astype(np.uint64),
+                                                       snap_r["id"].astype(np.uint64))),
+                 "same_neighbor_counts": bool(np.array_equal(snap_g["nc"], snap_r["nc"])),
+                 "total_energy": abs(e_g - e_r) / abs(e_r)}
+        a, b = align_by_id(snap_g), align_by_id(snap_r)
+
+        def put(name, d, sc):
+            q = np.abs(d) / sc
+            entry[name] = {"max": float(np.max(q)), "rms": float(np.sqrt(np.mean(q * q)))}
+
+        put("rho", a["kx"] * a["m"] / a["xm"] - b["kx"] * b["m"] / b["xm"], np.abs(b["kx"] * b["m"] / b["xm"]))
+        put("u", a["temp"] - b["temp"], np.abs(b["temp"]))
+        put("h", a["h"] - b["h"], np.abs(b["h"]))
+        put("alpha", a["alpha"] - b["alpha"], np.abs(b["alpha"]))
+        for f in ("x", "y", "z"):
+            put(f, a[f] - b[f], 1.0)
+        for f in ("vx", "vy", "vz", "ax", "ay", "az", "du"):
+            put(f, a[f] - b[f], max(float(np.max(np.abs(b[f]))), 1e-300))
+        out[prec] = entry
+    return out
 
 
 def adjoint_leg(side=48, steps=20, dt=1e-5, every=5, directions=64, eps=1e-6) -> dict:
