@@ -69,7 +69,25 @@ typedef struct
                                step keeps exactly the j with |x_i - x_j| < 2 h_i.           */
 } sphb_params;
 
+/* element types of caller arrays in sphb_field */
+#define SPHB_F32 1 /* float          */
+#define SPHB_F64 2 /* double         */
+#define SPHB_U32 3 /* uint32 (nc)    */
+#define SPHB_U64 4 /* uint64 (id, keys) */
+
+/*! One caller array of a particle field: the field's name in the reference's ParticlesData
+ *  (sph/include/sph/particles_data.hpp:262-266), the array's first element, and its element type (SPHB_F32 ...).
+ *  With the reference's default SphTypes (sph/types.hpp:39-46) x, y, z, temp, u and du are double, and h, m, vx,
+ *  vy, vz, x_m1, y_m1, z_m1, du_m1, alpha and the derived hydro fields are float. */
+typedef struct
+{
+    const char* name;
+    void* data;
+    int dtype;
+} sphb_field;
+
 /*! Fill p with the reference defaults listed above (precision = SPHB_FP64). */
+
 void sphb_default_params(sphb_params* p);
 
 /*! Library version string. */
@@ -128,6 +146,15 @@ size_t sphb_sort_by_key_static_max(void);
  *  Domain::updateLayout (domain/include/cstone/domain/domain.hpp:491-537). */
 int sphb_gather8(const uint32_t* order, size_t n, int num_fields, const void* const* src, void* const* dst,
                  void* stream);
+
+/*! The ideal-gas EOS on caller arrays, per particle i in [first, last), in FP64 and stored in each array's type:
+ *  rho = kx m / xm, p = rho u (gamma - 1) with u = cv(mui, gamma) temp (or u itself if given),
+ *  c = sqrt(gamma u (gamma - 1)), prho = p / (kx m^2 gradh). fields names temp or u, m, kx, xm, gradh (read) and
+ *  prho, c, and optionally rho and p (written), each SPHB_F32 or SPHB_F64, device memory. Asynchronous on stream.
+ *  Replaces sph::gpu::computeIdealGasEOS (sph/include/sph/sph_gpu.hpp:42-45; hydro_ve/eos_gpu.cu:44-61;
+ *  sph/include/sph/eos.hpp:19-50). */
+int sphb_ideal_gas_eos(size_t first, size_t last, double mui, double gamma, const sphb_field* fields, int num_fields,
+                       void* stream);
 
 /*! Fully converged cornerstone leaf array for sorted keys (host-blocking: loops until no node splits or merges).
  *  Writes num_leaves + 1 keys to leaves and num_leaves counts, if num_leaves + 1 <= capacity.
@@ -276,6 +303,73 @@ int sphb_sim_load_state(sphb_sim* sim, const double* const* fields, const uint64
 
 /*! Copy the 14 conserved fields and the ids out (current SFC order), host memory if on_device == 0. */
 int sphb_sim_store_state(sphb_sim* sim, double* const* fields, uint64_t* id, int on_device);
+
+/*! sphb_sim_upload with the caller's own element types: fields must name the 14 conserved fields (SPHB_F32 or
+ *  SPHB_F64 each) and "id" (SPHB_U64), in any order. Host arrays cross the bus at their own width and are converted
+ *  on the device, so a Dataset with the reference's default types (a mix of float and double) passes as it is. */
+int sphb_sim_upload_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
+
+/*! sphb_sim_load_state with the caller's own element types (the fields of sphb_sim_upload_fields). */
+int sphb_sim_load_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
+
+/*! Copy fields out by name, each converted to the element type of its descriptor: any name of
+ *  sphb_sim_get_field (conserved, derived, du, nc, keys, id; keys and id only as SPHB_U64). Host memory if
+ *  on_device == 0. */
+int sphb_sim_store_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
+
+/* ---------------------------------------------------------------------------------------------------------------- */
+/* 2b. The force stages on a caller's dataset, in place                                                             */
+/* ---------------------------------------------------------------------------------------------------------------- */
+
+/* These replace the reference's per-stage GPU dispatch of HydroVeProp (main/src/propagator/ve_hydro.hpp:126-220):
+ * sph::gpu::computeXMass, computeVeDefGradh, computeIdealGasEOS, computeIadDivvCurlv, computeAVswitches,
+ * computeMomentumEnergy<avClean = false> (sph/include/sph/sph_gpu.hpp:24-45), computePositionsGpu and
+ * updateSmoothingLengthGpu (sph_gpu.hpp:79-87). Each reads and writes the arrays of a caller's Dataset on the device,
+ * bound once by field name, in the caller's element types; the simulation object only holds this library's own
+ * state (octree, neighbour lists, records). first/last are the GroupView's particle range (firstBody, lastBody;
+ * cstone/traversal/groups.hpp:28-34); at one rank without halos it must be [0, sphb_sim_size(sim)). box is the
+ * Domain's box of this force computation; the later stages must pass the box of its sphb_dataset_xmass
+ * (SPHB_ERR_STATE otherwise). The stages keep the reference's order (the stage ABI's SPHB_ERR_STATE rule). Positions
+ * and h must not change between sphb_dataset_xmass and the later stages of the same force computation, as within
+ * computeForces. Not available with block time steps or AV cleaning (SPHB_ERR_STATE). */
+
+/*! Bind the caller's device arrays (each of sphb_sim_size(sim) elements) by field name: any field of
+ *  sphb_sim_get_field plus rho, p and u (the EOS's optional fields), reals as SPHB_F32 or SPHB_F64, nc as SPHB_U32,
+ *  id and keys as SPHB_U64. Replaces any previous binding and restarts the step state (as an upload). */
+int sphb_sim_bind_fields(sphb_sim* sim, const sphb_field* fields, int num_fields);
+
+/*! sph::gpu::computeXMass (sph_gpu.hpp:24-25; xmass_gpu.cu:103-124): builds this library's octree from the bound
+ *  particles, which must already be in the SFC order of box (as after the reference's Domain::sync; otherwise
+ *  SPHB_ERR_STATE), then runs the neighbour search with the smoothing-length iteration and XMass.
+ *  Reads id, x, y, z, h, m; writes h, nc, xm. */
+int sphb_dataset_xmass(sphb_sim* sim, size_t first, size_t last, const sphb_box* box);
+
+/*! sph::gpu::computeVeDefGradh (sph_gpu.hpp:30-31; ve_def_gradh_kern.hpp:43-90). Reads xm (and x, y, z, h, m of the
+ *  preceding sphb_dataset_xmass); writes kx, gradh. */
+int sphb_dataset_ve_def_gradh(sphb_sim* sim, size_t first, size_t last, const sphb_box* box);
+
+/*! sph::gpu::computeIadDivvCurlv (sph_gpu.hpp:33-34; iad_kern.hpp:43-110, divv_curlv_kern.hpp:43-123). Reads vx,
+ *  vy, vz, xm, kx, c, prho; writes c11, c12, c13, c22, c23, c33, divv, curlv. */
+int sphb_dataset_iad_divv_curlv(sphb_sim* sim, size_t first, size_t last, const sphb_box* box);
+
+/*! sph::gpu::computeAVswitches (sph_gpu.hpp:36-37; av_switches_kern.hpp:43-137) with the previous time step min_dt.
+ *  Reads vx, vy, vz, xm, kx, c, prho, c11 ... c33, divv, alpha; writes alpha. */
+int sphb_dataset_av_switches(sphb_sim* sim, size_t first, size_t last, const sphb_box* box, double min_dt);
+
+/*! sph::gpu::computeMomentumEnergy<avClean = false> (sph_gpu.hpp:39-40; momentum_energy_kern.hpp:65-222). Reads vx,
+ *  vy, vz, xm, kx, c, prho, c11 ... c33, divv, alpha; writes ax, ay, az, du and, if not NULL, *min_dt_courant (the
+ *  float the reference's kernel reduces, momentum_energy_gpu.cu:109-116). */
+int sphb_dataset_momentum_energy(sphb_sim* sim, size_t first, size_t last, const sphb_box* box,
+                                 float* min_dt_courant);
+
+/*! computePositionsGpu of the global step (sph_gpu.hpp:79-83; positions_gpu.cu:118-183) with time steps dt and
+ *  dt_m1. Reads x, y, z, vx, vy, vz, x_m1, y_m1, z_m1, temp, du, du_m1, ax, ay, az; writes x, y, z, vx, vy, vz,
+ *  x_m1, y_m1, z_m1, temp, du_m1. */
+int sphb_dataset_positions(sphb_sim* sim, size_t first, size_t last, double dt, double dt_m1, const sphb_box* box);
+
+/*! updateSmoothingLengthGpu (sph_gpu.hpp:86-87; update_h_gpu.cu:41-71). Reads nc, h; writes h, and keys (if bound)
+ *  with the removal key for particles left with nc <= 1, in which case it returns SPHB_ERR_NOT_CONVERGED. */
+int sphb_dataset_update_h(sphb_sim* sim, size_t first, size_t last, unsigned ng0);
 
 /* ---------------------------------------------------------------------------------------------------------------- */
 /* 3. Differentiation of the step                                                                                   */

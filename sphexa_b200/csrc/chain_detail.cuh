@@ -360,6 +360,20 @@ __device__ __forceinline__ void loadChunk(const uint32_t* nidx, const Target& t,
         : "l"(p));
 }
 
+/*! The next neighbour index of a list chunk: returns js[0] and shifts the rest down. Every index stays static, so
+ *  the chunk stays in registers while a pair loop runs one pair per iteration instead of fully unrolled (the largest
+ *  FP32 J-loop's unrolled 8-pair body overflowed the instruction cache). */
+__device__ __forceinline__ uint32_t popChunk(uint32_t (&js)[kNbChunk])
+{
+    uint32_t j = js[0];
+#pragma unroll
+    for (unsigned r = 0; r + 1 < kNbChunk; ++r)
+    {
+        js[r] = js[r + 1];
+    }
+    return j;
+}
+
 /*! Maximum (kMax) or minimum of one double per thread, published as ordered bits with one atomic per block on
  *  *single (one simulation), or one atomic per warp on the warp's instance slot batch.reduce[2 q + slot] (an ensemble:
  *  a warp never spans two instances). Every thread of the block must call it. */

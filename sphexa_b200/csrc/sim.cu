@@ -7,168 +7,8 @@
 #include <string>
 #include <vector>
 
-#include "adjoint.cuh"
-#include "bdt.cuh"
-#include "hydro.cuh"
-#include "integrate.cuh"
-#include "neighbors.cuh"
-#include "octree.cuh"
-#include "primitives.cuh"
-#include "sfc.cuh"
-#include "sort.cuh"
+#include "sim.cuh"
 #include "tables.hpp"
-
-namespace sphb
-{
-
-//! conserved fields, in the order of the upload ABI
-enum Field : int
-{
-    fX, fY, fZ, fH, fM, fTemp, fVx, fVy, fVz, fXm1, fYm1, fZm1, fDuM1, fAlpha, kNumConserved
-};
-static const char* const kConservedNames[kNumConserved] = {"x",  "y",    "z",    "h",    "m",     "temp", "vx",
-                                                           "vy", "vz",   "x_m1", "y_m1", "z_m1", "du_m1", "alpha"};
-
-//! derived fields stored in the J-loop type
-enum Derived : int
-{
-    dXm, dKx, dGradh, dPrho, dC, dC11, dC12, dC13, dC22, dC23, dC33, dDivv, dCurlv, dAx, dAy, dAz, kNumDerived
-};
-static const char* const kDerivedNames[kNumDerived] = {"xm",  "kx",  "gradh", "prho", "c",     "c11", "c12", "c13",
-                                                       "c22", "c23", "c33",   "divv", "curlv", "ax",  "ay",  "az"};
-
-enum Stage : int
-{
-    sSync, sNeighbors, sXMass, sVeDefGradh, sIad, sAV, sMomentum, sConserved, sIntegrate, kNumStages
-};
-
-} // namespace sphb
-
-using namespace sphb;
-
-struct sphb_sim
-{
-    size_t n{0};
-    sphb_params p{};
-    sphb_box hbox{};
-    DevBox box{};
-    bool mixed{false};
-    cudaStream_t stream{nullptr};
-
-    DeviceBuffer<double> f[kNumConserved];
-    DeviceBuffer<double> fAlt[kNumConserved];
-    DeviceBuffer<uint64_t> id, idAlt, keys;
-    DeviceBuffer<uint32_t> order;
-    DeviceBuffer<char> sortScratch;
-    DeviceBuffer<double4> pos;
-    DeviceBuffer<int4> posq;
-    DeviceBuffer<float4> blockLo, blockHi;
-    DeviceBuffer<uint32_t> nidx;
-    DeviceBuffer<unsigned> nc;
-    DeviceBuffer<char> derived[kNumDerived];
-    DeviceBuffer<double> du;
-    DeviceBuffer<char> hrec, grec, avrec;
-    DeviceBuffer<char> dvrec, dv; // AV cleaning only: symmetrised velocity gradients (record + 6 arrays)
-    DeviceBuffer<double> whD, whdD;
-    DeviceBuffer<float> whF, whdF;
-    DeviceBuffer<unsigned long long> reduce;
-    DeviceBuffer<unsigned> status;
-    DeviceBuffer<double> partial, cons;
-    double K{0};
-    // FP32 polynomial kernel: fitted once per simulation (it depends only on the sinc index)
-    bool polyReady{false};
-    int polyOk{0};
-    float wpoly[kPolyTerms]{};
-    float dwpoly[kPolyTerms]{};
-
-    GlobalTree gtree;
-    FocusTree ftree;
-    TreeScratch ts;
-    bool boxFirstCall{true};
-
-    double minDt{0}, minDt_m1{0}, minDtCourant{INFINITY}, minDtRho{INFINITY}, ttot{0};
-    double etot{0}, ecin{0}, eint{0}, linmom{0}, angmom{0};
-    double totalNeighbors{0};
-    uint64_t iteration{1};
-    bool uploaded{false};
-    bool forcesDone{false};
-    int nextStage{0}; // the stage of the force computation that may run next (StageOrder), 0 = the domain sync
-
-    // fixed time step (> 0) instead of computeTimestep; required by the step adjoint
-    double fixedDt{0};
-    // adjoint support: when taping, the forward also records what its adjoint needs
-    bool taping{false};
-    DeviceBuffer<double> hPre, alphaPre;
-    DeviceBuffer<char> tapeT;
-    DeviceBuffer<int> tapeJ;
-    DeviceBuffer<char> adjT;
-    DeviceBuffer<double> adjWork, adjScalar;
-    // recorded steps: copies of everything the step adjoint reads, one slot per step of a checkpoint segment
-    DeviceBuffer<char> tapeSlots;
-    size_t tapeSlotBytes{0};
-    int numTapeSlots{0};
-
-    // skin lists (neighbors.cuh): candidate rows kept across steps and refiltered exactly every step
-    DeviceBuffer<uint32_t> skinRows;
-    DeviceBuffer<uint16_t> skinDist;
-    DeviceBuffer<unsigned> skinCount;
-    DeviceBuffer<double> skinRadius, skinXb, skinYb, skinZb;
-    DeviceBuffer<uint32_t> skinBuild, skinBuildAlt, skinMoved;
-    DeviceBuffer<unsigned> skinGrid;
-    DeviceBuffer<unsigned> skinWork; // [0], [1]: deferred by the check / by the iteration, then the two lists
-    DeviceBuffer<unsigned> skinGroupD;
-    cudaStream_t sideStream{nullptr}; // the tree search of deferred groups, beside the refilter
-    cudaEvent_t skinFork{nullptr}, skinJoin{nullptr};
-    unsigned skinCap{0};
-    bool skinValid{false};    // rows match the particles' current indices (up to the tracked permutation)
-    bool skinAnyMoved{false}; // some index holds another particle than at the build (skinBuild, skinMoved valid)
-    bool skinFiltered{false}; // this step's lists came from the rows
-    int skinAge{0};           // steps since the build
-    int skinHoldoff{0};       // steps left of plain tree searches after rows proved short-lived
-    unsigned skinDeferredLast{0};
-    // tree searches of every group, row builds, refiltered steps, deferred groups, syncs that remapped the rows
-    uint64_t searchStats[5]{};
-
-    // block time steps (main/src/propagator/ve_hydro_bdt.hpp), after sphb_sim_bdt_enable
-    struct BdtTimestep // sph::Timestep (sph/include/sph/timestep.h:17-31)
-    {
-        float nextDt{0}, elapsedDt{0}, totDt{0};
-        int numRungs{1};
-        int substep{0};
-        uint32_t rungRanges[kMaxRungs + 1]{};
-        float dtm1[kMaxRungs]{};
-        float dtDrift[kMaxRungs]{};
-    };
-    bool bdt{false};
-    float etaAcc{0.2f};
-    BdtTimestep bts, bprevTs;
-    DeviceBuffer<uint64_t> rung, rungAlt;   // rung each particle was last advanced on (a conserved field)
-    DeviceBuffer<float> groupDt;            // per group of the current group order
-    DeviceBuffer<uint32_t> groupIdx;        // sort permutation of groupDt
-    DeviceBuffer<uint32_t> grpSfc, grpTs;   // groups_ (SFC order after a full sync) and tsGroups_ (by time step)
-    DeviceBuffer<uint64_t> dtKeys;
-    DeviceBuffer<uint32_t> rungInfo;
-    DeviceBuffer<double> xs, ys, zs;        // positions at the last full sync (drift bound of the tree search)
-    DeviceBuffer<unsigned long long> dispMax;
-    const uint32_t* activeList{nullptr};    // activeRungs_: groups whose forces this substep computes
-    unsigned numActive{0};
-    double treeExt{0.0};                    // widening of the tree's node boxes (TreeView::ext)
-
-    cudaEvent_t ev[kNumStages + 1]{};
-    float stageMs[kNumStages]{};
-    // pinned landing place of the small per-step reads (sums, reductions, status), so that they queue behind the
-    // kernels and the host waits once
-    unsigned long long* hostMsg{nullptr};
-
-    size_t elemBytes() const { return mixed ? sizeof(float) : sizeof(double); }
-    size_t numGroups() const { return (n + kWarp - 1) / kWarp; }
-
-    template<class T>
-    T* dptr(int d) const
-    {
-        return reinterpret_cast<T*>(derived[d].data());
-    }
-};
 
 namespace
 {
@@ -247,7 +87,7 @@ double idealGasCv(double mui, double gamma) { return 8.317e7 / mui / (gamma - 1.
 int updateBox(sphb_sim& s)
 {
     bool anyOpen = !s.hbox.periodic[0] || !s.hbox.periodic[1] || !s.hbox.periodic[2];
-    if (!anyOpen) { return kOk; }
+    if (!anyOpen || s.boxFromCaller) { return kOk; }
     double fit[6];
     for (int k = 0; k < 3; ++k)
     {
@@ -293,6 +133,7 @@ int syncDomain(sphb_sim& s)
     bool identity = false;
     SPHB_TRY(sortNearlySorted(s.keys.data(), s.order.data(), s.n, s.sortScratch.data(), s.sortScratch.capacity(),
                               &identity, st));
+    s.lastSyncIdentity = identity;
     if (s.skinValid && !identity)
     {
         // the skin rows hold build indices: track which particle now sits at each index
@@ -1313,22 +1154,7 @@ extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const u
         SPHB_CUDA_TRY(cudaMemcpyAsync(s->f[k].data(), fields[k], s->n * sizeof(double), kind, s->stream));
     }
     SPHB_CUDA_TRY(cudaMemcpyAsync(s->id.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
-    SPHB_CUDA_TRY(cudaMemsetAsync(s->keys.data(), 0, s->n * sizeof(uint64_t), s->stream));
-    SPHB_CUDA_TRY(cudaMemsetAsync(s->du.data(), 0, s->n * sizeof(double), s->stream));
-    SPHB_TRY(initGlobalTree(s->gtree, std::max<unsigned>(s->p.bucket_focus, unsigned(s->n / 100)), s->stream));
-    SPHB_TRY(initFocusTree(s->ftree, s->p.bucket_focus, s->ts, s->stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
-    s->boxFirstCall = true;
-    s->skinValid    = false;
-    s->nextStage    = sSync;
-    s->minDt        = s->p.minDt;
-    s->minDt_m1     = s->p.minDt_m1;
-    s->ttot         = 0;
-    s->iteration    = 1;
-    s->uploaded     = true;
-    s->forcesDone   = false;
-    if (s->bdt) { SPHB_TRY(resetBdt(*s)); }
-    return SPHB_OK;
+    return simimpl::finishUpload(*s);
 }
 
 extern "C" int sphb_sim_initial_sync(sphb_sim* s)
@@ -1663,21 +1489,8 @@ extern "C" int sphb_sim_load_state(sphb_sim* s, const double* const* fields, con
         if (!fields[k]) { return SPHB_ERR_ARG; }
         SPHB_CUDA_TRY(cudaMemcpyAsync(s->f[k].data(), fields[k], s->n * sizeof(double), kind, s->stream));
     }
-    if (!s->skinValid)
-    {
-        SPHB_CUDA_TRY(cudaMemcpyAsync(s->id.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
-        return SPHB_OK;
-    }
-    // the skin rows stay usable when every index holds the same particle as before (positions and h may differ
-    // arbitrarily: the next refilter checks them against the build)
     SPHB_CUDA_TRY(cudaMemcpyAsync(s->idAlt.data(), id, s->n * sizeof(uint64_t), kind, s->stream));
-    SPHB_TRY(idsDiffer(s->id.data(), s->idAlt.data(), s->n, s->skinWork.data(), s->stream));
-    unsigned differ = 1;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&differ, s->skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, s->stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
-    s->id.swap(s->idAlt);
-    if (differ) { s->skinValid = false; }
-    return SPHB_OK;
+    return simimpl::finishLoad(*s);
 }
 
 extern "C" int sphb_sim_store_state(sphb_sim* s, double* const* fields, uint64_t* id, int on_device)
@@ -1792,3 +1605,59 @@ extern "C" int sphb_sim_step_vjp_recorded(sphb_sim* s, int slot, const double* c
     s->taping = false;
     return rc;
 }
+
+namespace sphb
+{
+namespace simimpl
+{
+int runStage(sphb_sim& s, int stage) { return runStageChecked(s, stage); }
+bool findField(sphb_sim& s, const char* name, void** ptr, int* kind) { return ::findField(&s, name, ptr, kind); }
+double cv(const sphb_sim& s) { return idealGasCv(s.p.mui, s.p.gamma); }
+
+int finishUpload(sphb_sim& s)
+{
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.keys.data(), 0, s.n * sizeof(uint64_t), s.stream));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.du.data(), 0, s.n * sizeof(double), s.stream));
+    SPHB_TRY(initGlobalTree(s.gtree, std::max<unsigned>(s.p.bucket_focus, unsigned(s.n / 100)), s.stream));
+    SPHB_TRY(initFocusTree(s.ftree, s.p.bucket_focus, s.ts, s.stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    s.boxFirstCall = true;
+    s.skinValid    = false;
+    s.nextStage    = sSync;
+    s.minDt        = s.p.minDt;
+    s.minDt_m1     = s.p.minDt_m1;
+    s.ttot         = 0;
+    s.iteration    = 1;
+    s.uploaded     = true;
+    s.forcesDone   = false;
+    if (s.bdt) { SPHB_TRY(resetBdt(s)); }
+    return kOk;
+}
+
+int finishLoad(sphb_sim& s)
+{
+    if (!s.skinValid)
+    {
+        s.id.swap(s.idAlt);
+        return kOk;
+    }
+    // the skin rows stay usable when every index holds the same particle as before (positions and h may differ
+    // arbitrarily: the next refilter checks them against the build)
+    SPHB_TRY(idsDiffer(s.id.data(), s.idAlt.data(), s.n, s.skinWork.data(), s.stream));
+    unsigned differ = 1;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&differ, s.skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, s.stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    s.id.swap(s.idAlt);
+    if (differ) { s.skinValid = false; }
+    return kOk;
+}
+
+int positions(sphb_sim& s, double dt, double dtM1)
+{
+    s.minDt    = dt;
+    s.minDt_m1 = dtM1;
+    double c   = idealGasCv(s.p.mui, s.p.gamma);
+    return s.mixed ? runPositions<float>(s, c) : runPositions<double>(s, c);
+}
+} // namespace simimpl
+} // namespace sphb

@@ -20,6 +20,7 @@ ERRORS = {1: "invalid argument", 2: "CUDA error", 3: "capacity exhausted", 4: "s
           5: "call out of order", 6: "bounded device wait gave up"}
 SPHB_FP64 = 0
 SPHB_MIXED = 1
+SPHB_F32, SPHB_F64, SPHB_U32, SPHB_U64 = 1, 2, 3, 4
 
 
 class SphbError(RuntimeError):
@@ -30,6 +31,31 @@ class SphbError(RuntimeError):
 
 class Box(C.Structure):
     _fields_ = [("lo", C.c_double * 3), ("hi", C.c_double * 3), ("periodic", C.c_int * 3)]
+
+
+class Field(C.Structure):
+    """sphb_field: one caller array of a particle field, by the reference's field name"""
+    _fields_ = [("name", C.c_char_p), ("data", C.c_void_p), ("dtype", C.c_int)]
+
+
+def dtype_code(a) -> int:
+    """SPHB_F32 ... of a numpy array or torch tensor"""
+    name = str(a.dtype).replace("torch.", "")
+    codes = {"float32": SPHB_F32, "float64": SPHB_F64, "uint32": SPHB_U32, "int32": SPHB_U32,
+             "uint64": SPHB_U64, "int64": SPHB_U64}
+    if name not in codes:
+        raise TypeError(f"no sphb element type for {a.dtype}")
+    return codes[name]
+
+
+def make_fields(arrays: dict):
+    """A ctypes array of sphb_field from {name: numpy array or torch tensor}; the arrays must stay alive."""
+    tbl = (Field * len(arrays))()
+    for q, (name, a) in enumerate(arrays.items()):
+        tbl[q].name = name.encode()
+        tbl[q].data = ptr(a).value
+        tbl[q].dtype = dtype_code(a)
+    return tbl
 
 
 class BdtTimestep(C.Structure):
@@ -63,7 +89,11 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_ensemble_upload", "sphb_ensemble_initial_sync", "sphb_ensemble_rebuild_trees",
             "sphb_ensemble_set_threads", "sphb_ensemble_autotune", "sphb_ensemble_step", "sphb_ensemble_size", "sphb_ensemble_search_stats",
             "sphb_ensemble_stage_times",
-            "sphb_ensemble_get_field", "sphb_ensemble_scalars", "sphb_ensemble_stream")
+            "sphb_ensemble_get_field", "sphb_ensemble_scalars", "sphb_ensemble_stream",
+            "sphb_sim_upload_fields", "sphb_sim_load_fields", "sphb_sim_store_fields", "sphb_sim_bind_fields",
+            "sphb_dataset_xmass", "sphb_dataset_ve_def_gradh", "sphb_ideal_gas_eos",
+            "sphb_dataset_iad_divv_curlv", "sphb_dataset_av_switches", "sphb_dataset_momentum_energy",
+            "sphb_dataset_positions", "sphb_dataset_update_h")
 
 _lib = None
 
@@ -138,6 +168,18 @@ def load() -> C.CDLL:
         "sphb_ensemble_get_field": (C.c_int, [P, C.c_int, C.c_char_p, P]),
         "sphb_ensemble_scalars": (C.c_int, [P, C.c_int, P]),
         "sphb_ensemble_stream": (C.c_void_p, [P]),
+        "sphb_sim_upload_fields": (C.c_int, [P, P, C.c_int, C.c_int]),
+        "sphb_sim_load_fields": (C.c_int, [P, P, C.c_int, C.c_int]),
+        "sphb_sim_store_fields": (C.c_int, [P, P, C.c_int, C.c_int]),
+        "sphb_sim_bind_fields": (C.c_int, [P, P, C.c_int]),
+        "sphb_dataset_xmass": (C.c_int, [P, S, S, C.POINTER(Box)]),
+        "sphb_dataset_ve_def_gradh": (C.c_int, [P, S, S, C.POINTER(Box)]),
+        "sphb_ideal_gas_eos": (C.c_int, [S, S, C.c_double, C.c_double, P, C.c_int, P]),
+        "sphb_dataset_iad_divv_curlv": (C.c_int, [P, S, S, C.POINTER(Box)]),
+        "sphb_dataset_av_switches": (C.c_int, [P, S, S, C.POINTER(Box), C.c_double]),
+        "sphb_dataset_momentum_energy": (C.c_int, [P, S, S, C.POINTER(Box), C.POINTER(C.c_float)]),
+        "sphb_dataset_positions": (C.c_int, [P, S, S, C.c_double, C.c_double, C.POINTER(Box)]),
+        "sphb_dataset_update_h": (C.c_int, [P, S, S, C.c_uint]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
