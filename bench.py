@@ -359,24 +359,27 @@ def run_ours(args, ws, rank, local):
                "pairs": pairs, "clocks": clk, "snap": snap, "energy": energy, "ttot": sim.scalars()["ttot"]}
         if with_e2e:
             # per step: host->device copy of the whole particle state from pinned memory, the step, and the
-            # device->host copy of the updated state (the C-ABI round trip of a caller holding host buffers)
-            host = [torch.empty(n, dtype=torch.float64, pin_memory=True) for _ in CONSERVED_FIELDS]
-            hid = torch.empty(n, dtype=torch.int64, pin_memory=True)
-            tbl_out = (C.c_void_p * len(host))(*[h.data_ptr() for h in host])
-            L.check(sim.lib.sphb_sim_store_state(sim.h, tbl_out, C.c_void_p(hid.data_ptr()), 0), "store_state")
-            tbl_in = (C.c_void_p * len(host))(*[h.data_ptr() for h in host])
+            # device->host copy of the updated state: the C-ABI round trip of a caller holding the reference's
+            # Dataset in host buffers of its default types (SphTypes: x, y, z, temp double; h, m, v, x_m1, du_m1,
+            # alpha float; id uint64), through the typed load and store
+            wide = ("x", "y", "z", "temp")
+            host = {f: torch.empty(n, dtype=torch.float64 if f in wide else torch.float32, pin_memory=True)
+                    for f in CONSERVED_FIELDS}
+            host["id"] = torch.empty(n, dtype=torch.int64, pin_memory=True)
+            tbl = L.make_fields(host)
+            L.check(sim.lib.sphb_sim_store_fields(sim.h, tbl, len(tbl), 0), "store_fields")
             barrier_sync()
             e0.record(stream)
             for _ in range(steps):
-                L.check(sim.lib.sphb_sim_load_state(sim.h, tbl_in, C.c_void_p(hid.data_ptr()), 0), "load_state")
+                L.check(sim.lib.sphb_sim_load_fields(sim.h, tbl, len(tbl), 0), "load_fields")
                 sim.step()
-                L.check(sim.lib.sphb_sim_store_state(sim.h, tbl_out, C.c_void_p(hid.data_ptr()), 0),
-                        "store_state")
+                L.check(sim.lib.sphb_sim_store_fields(sim.h, tbl, len(tbl), 0), "store_fields")
             e1.record(stream)
             barrier_sync()
             res["e2e_ms"] = max_over_ranks(e0.elapsed_time(e1))
-            res["h2d_bytes"] = (len(host) * 8 + 8) * n
-            res["d2h_bytes"] = (len(host) * 8 + 8) * n
+            nbytes = sum(t.numel() * t.element_size() for t in host.values())
+            res["h2d_bytes"] = nbytes
+            res["d2h_bytes"] = nbytes
         res["sim_obj"] = sim
         return res
 
@@ -421,7 +424,9 @@ def run_ours(args, ws, rank, local):
                       "keys, integration, h update and reductions") if args.precision == "mixed" else "fp64",
         "config": workload_config(args.side, n, args.precision),
         "e2e": {"value": n * ws * steps / (main_leg["e2e_ms"] * 1e-3), "unit": UNIT,
-                "h2d_bytes_per_step": main_leg["h2d_bytes"], "d2h_bytes_per_step": main_leg["d2h_bytes"]},
+                "h2d_bytes_per_step": main_leg["h2d_bytes"], "d2h_bytes_per_step": main_leg["d2h_bytes"],
+                "path": "sphb_sim_load_fields + sphb_sim_step + sphb_sim_store_fields, pinned host buffers in the "
+                        "reference's default field types (80 B per particle each way)"},
         "gpu_launches": main_leg["launches"],
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "neighbor_pairs_per_step": main_leg["pairs"],
@@ -666,12 +671,12 @@ def bdt_leg(side=128, blocks=2, steps=16, warmup=3, min_dt=1e-4) -> dict:
     stage_sum = {}
 
     def one_block(timed):
-        count, active = 0, 0
+        count, active = 0, 0.0
         while True:
             sim.bdt_step()
             t = sim.bdt_timestep()
             count += 1
-            active += t["num_active"]
+            active += t["num_active"] / t["rung_ranges"][4]  # share of the spatial groups of this block
             if timed:
                 for key, v in sim.stage_times().items():
                     stage_sum[key] = stage_sum.get(key, 0.0) + v
@@ -691,14 +696,14 @@ def bdt_leg(side=128, blocks=2, steps=16, warmup=3, min_dt=1e-4) -> dict:
     torch.cuda.synchronize()
     ms_bdt = a.elapsed_time(b)
     dt_bdt = sim.scalars()["ttot"] - t0
-    groups = (n + 31) // 32
     r = last["rung_ranges"]
     out = {"workload": f"sedov-{side}^3 ({n:,} particles), mixed precision, eta_acc 0.2, first dt_m1 {min_dt:g}",
            "global": {"steps": steps, "ms_per_step": ms_glob / steps, "simulated_time": dt_glob,
                       "simulated_time_per_s": dt_glob / (ms_glob * 1e-3)},
            "block": {"blocks": blocks, "substeps": substeps, "ms_per_substep": ms_bdt / substeps,
                      "simulated_time": dt_bdt, "simulated_time_per_s": dt_bdt / (ms_bdt * 1e-3),
-                     "active_group_share": active / (substeps * groups), "base_dt_last": last["next_dt"],
+                     "active_group_share": active / substeps, "spatial_groups_last_block": r[4],
+                     "base_dt_last": last["next_dt"],
                      "groups_per_rung_last_block": [r[k + 1] - r[k] for k in range(last["num_rungs"])],
                      "stage_ms_per_substep": {k: round(v / substeps, 4) for k, v in stage_sum.items()}}}
     out["simulated_time_ratio"] = out["block"]["simulated_time_per_s"] / out["global"]["simulated_time_per_s"]

@@ -163,6 +163,21 @@ int sphb_ideal_gas_eos(size_t first, size_t last, double mui, double gamma, cons
 int sphb_compute_octree(const uint64_t* sorted_keys, size_t n, unsigned bucket, uint64_t* leaves, uint32_t* counts,
                         size_t capacity, size_t* num_leaves, void* stream);
 
+/*! Spatial target groups of the particles [first, last), which are in SFC order: fixed runs of group_size (32 or 64)
+ *  consecutive particles, each split after every particle whose successor lies farther than
+ *  min(tol_factor * the run's smallest leaf edge, 2 h) (lengths relative to the box; the leaf edge from leaves
+ *  (num_leaves + 1 keys) and layout (first particle of each leaf) of the focus tree). groups receives
+ *  num_groups + 1 boundaries, group g being [groups[g], groups[g + 1]), if num_groups + 1 <= capacity (else
+ *  SPHB_ERR_CAPACITY; *num_groups is always written). h may be NULL (no smoothing-length criterion); h_dtype
+ *  (SPHB_F32 or SPHB_F64) is its type and the precision of the threshold, as in the reference. Device arrays;
+ *  host-blocking. Replaces cstone::computeGroupSplits (domain/include/cstone/traversal/groups_gpu.cu:108-137,
+ *  groups_gpu.cuh:37-216) as sph::computeSpatialGroups calls it (sph/include/sph/groups.hpp:41-55: tol_factor 2,
+ *  group_size 32). */
+int sphb_compute_group_splits(size_t first, size_t last, const double* x, const double* y, const double* z,
+                              const void* h, int h_dtype, const uint64_t* leaves, size_t num_leaves,
+                              const uint32_t* layout, const sphb_box* box, unsigned group_size, float tol_factor,
+                              uint32_t* groups, size_t capacity, size_t* num_groups, void* stream);
+
 /* ---------------------------------------------------------------------------------------------------------------- */
 /* 2. Simulation object: the whole hydro step of HydroVeProp                                                        */
 /* ---------------------------------------------------------------------------------------------------------------- */
@@ -196,7 +211,9 @@ int sphb_sim_integrate(sphb_sim* sim);
 int sphb_sim_step(sphb_sim* sim);
 
 /*! Block time steps: switch this simulation to the propagator of main/src/propagator/ve_hydro_bdt.hpp
- *  (HydroVeBdtProp<avClean>, avClean from sphb_params.av_clean). Groups are the fixed groups of 32 SFC-consecutive particles. Each group gets
+ *  (HydroVeBdtProp<avClean>, avClean from sphb_params.av_clean). The groups are the reference's spatial target
+ *  groups of at most 32 SFC-consecutive particles (sph::computeSpatialGroups, as sphb_compute_group_splits), formed
+ *  at every full sync (ve_hydro_bdt.hpp:185). Each group gets
  *  the time step min(Courant, Krho / |max divv|, eta_acc (h^2/|a|^2)^(1/4)) over its particles (ts_groups.cu), the
  *  groups are sorted by it into up to 4 power-of-two rungs (ts_rungs.hpp:116-166), and a block step of
  *  2^(numRungs - 1) substeps computes forces only on the groups of the active rungs while the others drift.

@@ -3,8 +3,11 @@
 group time steps of sph/include/sph/ts_groups.cu, over the plain-C oracle (oracle/sph_oracle.c) for the J-loops,
 drifts and kick-drifts. Imported only by tests/.
 
-Groups are fixed runs of 32 SFC-consecutive particles, as in the CUDA path. Time-step arithmetic is float32, as in
-the reference (sph::Timestep holds floats). The reference runs this propagator only on GPUs (its constructor refuses
+Groups are the reference's spatial target groups (sph::computeSpatialGroups at every full sync,
+ve_hydro_bdt.hpp:185), from the restated group splits of oracle/groups.py over a cornerstone focus tree: the tree
+comes from a caller-supplied provider (the tests pass the CUDA path's focus tree, which other tests pin bit for bit
+to the reference's), by default the converged tree of the current keys. Time-step arithmetic is float32, as in the
+reference (sph::Timestep holds floats). The reference runs this propagator only on GPUs (its constructor refuses
 CPUs, ve_hydro_bdt.hpp:119), so nothing of the reference itself can pin this restatement here: it is checked only
 against the reading of the sources cited on each step.
 """
@@ -14,7 +17,8 @@ import ctypes as C
 
 import numpy as np
 
-from .restated import OracleSim, load, ptr
+from .groups import group_splits
+from .restated import OracleSim, compute_octree, load, ptr
 
 F32 = np.float32
 MAX_RUNGS = 4   # Timestep::maxNumRungs (sph/include/sph/timestep.h:19)
@@ -68,8 +72,11 @@ class Timestep:
 class BdtOracle(OracleSim):
     """One substep per step(): computeForces then integrate of HydroVeBdtProp, one rank."""
 
-    def __init__(self, ic: dict, eta_acc: float = 0.2):
+    def __init__(self, ic: dict, eta_acc: float = 0.2, tree=None):
+        """tree: callable returning (leaves, layout) of the focus tree for the particles in their current SFC order,
+        called at every full sync; None: the converged cornerstone tree (bucket 64) of the current keys."""
         super().__init__(ic)
+        self.tree = tree
         lib = load()
         lib.orc_sim_sync_perm.restype = None
         lib.orc_sim_sync_perm.argtypes = [C.c_void_p, C.c_void_p]
@@ -85,7 +92,8 @@ class BdtOracle(OracleSim):
         p = ic["params"]
         self.eta_acc = F32(eta_acc)
         self.krho = F32(p["Krho"])
-        self.num_groups = (self.n + GROUP - 1) // GROUP
+        self.bounds = np.array([0, self.n], dtype=np.uint32)  # set at every full sync
+        self.num_groups = 1
         self.ts = Timestep()
         self.ts.dt_m1[0] = F32(p["minDt"])          # the constructor, ve_hydro_bdt.hpp:122
         self.prev = self.ts.copy()
@@ -101,8 +109,23 @@ class BdtOracle(OracleSim):
     def particles(self, groups: np.ndarray) -> np.ndarray:
         if len(groups) == 0:
             return np.zeros(0, dtype=np.uint32)
-        idx = (groups.astype(np.int64)[:, None] * GROUP + np.arange(GROUP)[None, :]).ravel()
-        return np.ascontiguousarray(idx[idx < self.n], dtype=np.uint32)
+        g = groups.astype(np.int64)
+        return np.ascontiguousarray(np.concatenate([np.arange(self.bounds[k], self.bounds[k + 1]) for k in g]),
+                                    dtype=np.uint32)
+
+    def spatial_groups(self):
+        """computeGroups -> computeSpatialGroups (sph/include/sph/groups.hpp:41-74): group boundaries of the current
+        SFC order, tolFactor 2, groups of 32"""
+        if self.tree is not None:
+            leaves, layout = self.tree()
+        else:
+            leaves, counts = compute_octree(self.keys(), 64)
+            layout = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
+        sc = self.scalars()
+        box = (sc["xmin"], sc["xmax"], sc["ymin"], sc["ymax"], sc["zmin"], sc["zmax"])
+        x, y, z, h = (self.get(f) for f in ("x", "y", "z", "h"))
+        return group_splits(x, y, z, h, np.asarray(leaves, dtype=np.uint64), np.asarray(layout, dtype=np.uint32),
+                            box, GROUP, 2.0, False)
 
     def sync(self):
         """fullSync / partialSync (ve_hydro_bdt.hpp:165-215)"""
@@ -111,9 +134,12 @@ class BdtOracle(OracleSim):
             perm = np.empty(self.n, dtype=np.uint32)
             self.lib.orc_sim_sync_perm(self.h, ptr(perm))
             self.rung = self.rung[perm]                  # rung is a conserved field
+            self.bounds = self.spatial_groups()
+            self.num_groups = self.bounds.size - 1
             self.groups = np.arange(self.num_groups, dtype=np.uint32)
             self.active = self.groups.copy()
-            self.group_dt[:] = FLT_MAX
+            self.group_dt = np.full(self.num_groups, FLT_MAX, dtype=np.float32)
+            self.group_idx = np.zeros(self.num_groups, dtype=np.uint32)
         else:
             highest = butterfly(ts.substep)
             self.active = self.ts_groups[ts.rung_ranges[0]:ts.rung_ranges[highest]].copy()
@@ -124,10 +150,10 @@ class BdtOracle(OracleSim):
         mask[self.particles(self.active)] = 1
         dt = np.empty(self.n)
         self.lib.orc_sim_forces_active(self.h, ptr(mask), self.min_dt, ptr(dt))
-        pad = self.num_groups * GROUP - self.n
+        starts = self.bounds[:-1].astype(np.int64)
 
         def per_group(a, fill, red):
-            return red(np.concatenate([a, np.full(pad, fill)]).reshape(self.num_groups, GROUP), axis=1)
+            return (np.maximum if red is np.max else np.minimum).reduceat(a, starts)
 
         divv, h = self.get("divv"), self.get("h")
         ax, ay, az = self.get("ax"), self.get("ay"), self.get("az")

@@ -1,5 +1,6 @@
-// Kernels of the block time-step propagator (main/src/propagator/ve_hydro_bdt.hpp). Each listed group is one warp
-// of 32 consecutive particles; the lists are the dt-sorted group ids of one rung or of the active rungs.
+// Kernels of the block time-step propagator (main/src/propagator/ve_hydro_bdt.hpp). Each listed group is one warp:
+// group g holds the particles [bounds[g], bounds[g + 1]) (the spatial target groups, at most 32 particles); the lists
+// are the dt-sorted group ids of one rung or of the active rungs.
 #include <algorithm>
 
 #include "bdt.cuh"
@@ -15,13 +16,15 @@ namespace
 constexpr int kBdtThreads = 256;
 
 //! particle of this thread in list mode (-1: none): lane of group groups[slot], slot = warp of the launch
-__device__ inline long long listedParticle(const uint32_t* groups, unsigned num, size_t n, unsigned* slotOut)
+__device__ inline long long listedParticle(const uint32_t* groups, unsigned num, const uint32_t* bounds,
+                                           unsigned* slotOut)
 {
     size_t slot = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5;
     *slotOut    = unsigned(slot);
     if (slot >= num) { return -1; }
-    size_t i = size_t(groups[slot]) * 32 + (threadIdx.x & 31);
-    return i < n ? (long long)i : -1;
+    uint32_t g = groups[slot];
+    size_t i   = size_t(bounds[g]) + (threadIdx.x & 31);
+    return i < bounds[g + 1] ? (long long)i : -1;
 }
 
 template<class T>
@@ -51,13 +54,13 @@ __global__ void eosRefreshKernel(ChainArrays<T> a, HydroConsts<T> k)
 }
 
 template<class T>
-__global__ void groupDivvKernel(const uint32_t* groups, unsigned num, size_t n, const T* divv, float Krho,
+__global__ void groupDivvKernel(const uint32_t* groups, unsigned num, const uint32_t* bounds, const T* divv, float Krho,
                                 float* groupDt)
 {
     unsigned w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= num) { return; }
-    size_t first = size_t(groups[w]) * 32;
-    size_t last  = min(first + 32, n);
+    size_t first = bounds[groups[w]];
+    size_t last  = bounds[groups[w] + 1];
     // float localMax = max(localMax, divv[i]) per particle: the max of the values rounded once (rounding is monotonic)
     T m = T(-INFINITY);
     for (size_t i = first; i < last; ++i)
@@ -69,13 +72,13 @@ __global__ void groupDivvKernel(const uint32_t* groups, unsigned num, size_t n, 
 }
 
 template<class T>
-__global__ void groupAccKernel(const uint32_t* groups, unsigned num, size_t n, const T* ax, const T* ay, const T* az,
+__global__ void groupAccKernel(const uint32_t* groups, unsigned num, const uint32_t* bounds, const T* ax, const T* ay, const T* az,
                                const double* h, float etaAcc, float* groupDt)
 {
     unsigned w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= num) { return; }
-    size_t first = size_t(groups[w]) * 32;
-    size_t last  = min(first + 32, n);
+    size_t first = bounds[groups[w]];
+    size_t last  = bounds[groups[w] + 1];
     double m     = INFINITY;
     for (size_t i = first; i < last; ++i)
     {
@@ -106,11 +109,11 @@ __device__ inline double energyUpdate(double uOld, double dt, double dtm1, doubl
 }
 
 template<class T>
-__global__ void driftKernel(const uint32_t* groups, unsigned num, size_t n, float dt, float dtBack, RungSteps steps,
+__global__ void driftKernel(const uint32_t* groups, unsigned num, const uint32_t* bounds, float dt, float dtBack, RungSteps steps,
                             const uint64_t* rung, IntegrateArrays<T> a, double cv)
 {
     unsigned slot;
-    long long ii = listedParticle(groups, num, n, &slot);
+    long long ii = listedParticle(groups, num, bounds, &slot);
     if (ii < 0) { return; }
     size_t i      = size_t(ii);
     double dtm1   = double(steps.dtm1[min(rung[i], uint64_t(kMaxRungs - 1))]);
@@ -143,11 +146,11 @@ __device__ inline double foldPeriodic(double v, int k, const DevBox& box)
 }
 
 template<class T>
-__global__ void rungPositionsKernel(const uint32_t* groups, unsigned num, size_t n, float dt, RungSteps steps,
+__global__ void rungPositionsKernel(const uint32_t* groups, unsigned num, const uint32_t* bounds, float dt, RungSteps steps,
                                     const uint64_t* rung, IntegrateArrays<T> a, DevBox box, double cv)
 {
     unsigned slot;
-    long long ii = listedParticle(groups, num, n, &slot);
+    long long ii = listedParticle(groups, num, bounds, &slot);
     if (ii < 0) { return; }
     size_t i      = size_t(ii);
     double dtm1   = double(steps.dtm1[min(rung[i], uint64_t(kMaxRungs - 1))]);
@@ -171,18 +174,18 @@ __global__ void rungPositionsKernel(const uint32_t* groups, unsigned num, size_t
     a.duM1[i] = du;
 }
 
-__global__ void storeRungKernel(const uint32_t* groups, unsigned num, size_t n, uint64_t value, uint64_t* rung)
+__global__ void storeRungKernel(const uint32_t* groups, unsigned num, const uint32_t* bounds, uint64_t value, uint64_t* rung)
 {
     unsigned slot;
-    long long i = listedParticle(groups, num, n, &slot);
+    long long i = listedParticle(groups, num, bounds, &slot);
     if (i >= 0) { rung[i] = value; }
 }
 
-__global__ void listUpdateHKernel(const uint32_t* groups, unsigned num, size_t n, unsigned ng0, const unsigned* nc,
+__global__ void listUpdateHKernel(const uint32_t* groups, unsigned num, const uint32_t* bounds, unsigned ng0, const unsigned* nc,
                                   double* h, uint64_t* keys, unsigned* flag)
 {
     unsigned slot;
-    long long ii = listedParticle(groups, num, n, &slot);
+    long long ii = listedParticle(groups, num, bounds, &slot);
     if (ii < 0) { return; }
     size_t i   = size_t(ii);
     unsigned c = nc[i];
@@ -292,22 +295,22 @@ int launchEosRefresh(const ChainArrays<T>& a, const HydroConsts<T>& k, cudaStrea
 }
 
 template<class T>
-int launchGroupDivv(const uint32_t* groups, unsigned num, size_t n, const T* divv, float Krho, float* groupDt,
+int launchGroupDivv(const uint32_t* groups, unsigned num, const uint32_t* bounds, const T* divv, float Krho, float* groupDt,
                     cudaStream_t s)
 {
     if (num == 0) { return kOk; }
-    groupDivvKernel<T><<<ceilDiv(num, kBdtThreads), kBdtThreads, 0, s>>>(groups, num, n, divv, Krho, groupDt);
+    groupDivvKernel<T><<<ceilDiv(num, kBdtThreads), kBdtThreads, 0, s>>>(groups, num, bounds, divv, Krho, groupDt);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
 }
 
 template<class T>
-int launchGroupAcc(const uint32_t* groups, unsigned num, size_t n, const T* ax, const T* ay, const T* az,
+int launchGroupAcc(const uint32_t* groups, unsigned num, const uint32_t* bounds, const T* ax, const T* ay, const T* az,
                    const double* h, float etaAcc, float* groupDt, cudaStream_t s)
 {
     if (num == 0) { return kOk; }
-    groupAccKernel<T><<<ceilDiv(num, kBdtThreads), kBdtThreads, 0, s>>>(groups, num, n, ax, ay, az, h, etaAcc,
+    groupAccKernel<T><<<ceilDiv(num, kBdtThreads), kBdtThreads, 0, s>>>(groups, num, bounds, ax, ay, az, h, etaAcc,
                                                                          groupDt);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
@@ -315,42 +318,42 @@ int launchGroupAcc(const uint32_t* groups, unsigned num, size_t n, const T* ax, 
 }
 
 template<class T>
-int launchDrift(const uint32_t* groups, unsigned num, size_t n, float dt, float dtBack, RungSteps steps,
+int launchDrift(const uint32_t* groups, unsigned num, const uint32_t* bounds, float dt, float dtBack, RungSteps steps,
                 const uint64_t* rung, const IntegrateArrays<T>& a, double cv, cudaStream_t s)
 {
     if (num == 0) { return kOk; }
-    driftKernel<T><<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, n, dt, dtBack, steps, rung, a, cv);
+    driftKernel<T><<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, bounds, dt, dtBack, steps, rung, a, cv);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
 }
 
 template<class T>
-int launchRungPositions(const uint32_t* groups, unsigned num, size_t n, float dt, RungSteps steps,
+int launchRungPositions(const uint32_t* groups, unsigned num, const uint32_t* bounds, float dt, RungSteps steps,
                         const uint64_t* rung, const IntegrateArrays<T>& a, const DevBox& box, double cv,
                         cudaStream_t s)
 {
     if (num == 0) { return kOk; }
-    rungPositionsKernel<T><<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, n, dt, steps, rung, a, box, cv);
+    rungPositionsKernel<T><<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, bounds, dt, steps, rung, a, box, cv);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
 }
 
-int launchStoreRung(const uint32_t* groups, unsigned num, size_t n, uint64_t value, uint64_t* rung, cudaStream_t s)
+int launchStoreRung(const uint32_t* groups, unsigned num, const uint32_t* bounds, uint64_t value, uint64_t* rung, cudaStream_t s)
 {
     if (num == 0) { return kOk; }
-    storeRungKernel<<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, n, value, rung);
+    storeRungKernel<<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, bounds, value, rung);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
 }
 
-int launchListUpdateH(const uint32_t* groups, unsigned num, size_t n, unsigned ng0, const unsigned* nc, double* h,
+int launchListUpdateH(const uint32_t* groups, unsigned num, const uint32_t* bounds, unsigned ng0, const unsigned* nc, double* h,
                       uint64_t* keys, unsigned* flag, cudaStream_t s)
 {
     if (num == 0) { return kOk; }
-    listUpdateHKernel<<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, n, ng0, nc, h, keys, flag);
+    listUpdateHKernel<<<warpBlocks(num), kBdtThreads, 0, s>>>(groups, num, bounds, ng0, nc, h, keys, flag);
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -408,12 +411,12 @@ int launchSequence(uint32_t* list, unsigned num, uint32_t first, cudaStream_t s)
 
 #define SPHB_BDT_INSTANTIATE(T)                                                                                        \
     template int launchEosRefresh<T>(const ChainArrays<T>&, const HydroConsts<T>&, cudaStream_t);                    \
-    template int launchGroupDivv<T>(const uint32_t*, unsigned, size_t, const T*, float, float*, cudaStream_t);       \
-    template int launchGroupAcc<T>(const uint32_t*, unsigned, size_t, const T*, const T*, const T*, const double*,   \
+    template int launchGroupDivv<T>(const uint32_t*, unsigned, const uint32_t*, const T*, float, float*, cudaStream_t);       \
+    template int launchGroupAcc<T>(const uint32_t*, unsigned, const uint32_t*, const T*, const T*, const T*, const double*,   \
                                    float, float*, cudaStream_t);                                                     \
-    template int launchDrift<T>(const uint32_t*, unsigned, size_t, float, float, RungSteps, const uint64_t*,         \
+    template int launchDrift<T>(const uint32_t*, unsigned, const uint32_t*, float, float, RungSteps, const uint64_t*,         \
                                 const IntegrateArrays<T>&, double, cudaStream_t);                                    \
-    template int launchRungPositions<T>(const uint32_t*, unsigned, size_t, float, RungSteps, const uint64_t*,        \
+    template int launchRungPositions<T>(const uint32_t*, unsigned, const uint32_t*, float, RungSteps, const uint64_t*,        \
                                         const IntegrateArrays<T>&, const DevBox&, double, cudaStream_t);
 
 SPHB_BDT_INSTANTIATE(double)

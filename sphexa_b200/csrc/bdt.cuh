@@ -26,33 +26,33 @@ int launchEosRefresh(const ChainArrays<T>& a, const HydroConsts<T>& k, cudaStrea
 
 //! groupDivvTimestepGpu (sph/include/sph/ts_groups.cu:17-45): groupDt[w] = min(groupDt[w], Krho / |max divv|)
 template<class T>
-int launchGroupDivv(const uint32_t* groups, unsigned num, size_t n, const T* divv, float Krho, float* groupDt,
+int launchGroupDivv(const uint32_t* groups, unsigned num, const uint32_t* bounds, const T* divv, float Krho, float* groupDt,
                     cudaStream_t s);
 
 //! groupAccTimestepGpu (ts_groups.cu:47-80): groupDt[w] = min(groupDt[w], etaAcc (min h^2 / |a|^2)^(1/4))
 template<class T>
-int launchGroupAcc(const uint32_t* groups, unsigned num, size_t n, const T* ax, const T* ay, const T* az,
+int launchGroupAcc(const uint32_t* groups, unsigned num, const uint32_t* bounds, const T* ax, const T* ay, const T* az,
                    const double* h, float etaAcc, float* groupDt, cudaStream_t s);
 
 /*! driftPositionsGpu (sph/include/sph/positions_gpu.cu:45-90): recover the state at the start of the rung's step by
  *  going back dtBack, then go forward dt from there, with the acceleration and x_m1 of that start; no periodic
  *  folding. Updates x, v and temp. */
 template<class T>
-int launchDrift(const uint32_t* groups, unsigned num, size_t n, float dt, float dtBack, RungSteps steps,
+int launchDrift(const uint32_t* groups, unsigned num, const uint32_t* bounds, float dt, float dtBack, RungSteps steps,
                 const uint64_t* rung, const IntegrateArrays<T>& a, double cv, cudaStream_t s);
 
 /*! computePositionsGpu (positions_gpu.cu:117-166) over the groups of one rung: kick-drift by dt with the previous
  *  step of each particle's last rung, energy update, du_m1 = du. box.periodic all zero: no folding. */
 template<class T>
-int launchRungPositions(const uint32_t* groups, unsigned num, size_t n, float dt, RungSteps steps,
+int launchRungPositions(const uint32_t* groups, unsigned num, const uint32_t* bounds, float dt, RungSteps steps,
                         const uint64_t* rung, const IntegrateArrays<T>& a, const DevBox& box, double cv,
                         cudaStream_t s);
 
 //! storeRungGpu (ts_groups.cu:82-104): rung of every particle of the listed groups
-int launchStoreRung(const uint32_t* groups, unsigned num, size_t n, uint64_t value, uint64_t* rung, cudaStream_t s);
+int launchStoreRung(const uint32_t* groups, unsigned num, const uint32_t* bounds, uint64_t value, uint64_t* rung, cudaStream_t s);
 
 //! updateSmoothingLength over the listed groups (sph/include/sph/update_h.hpp:33-47)
-int launchListUpdateH(const uint32_t* groups, unsigned num, size_t n, unsigned ng0, const unsigned* nc, double* h,
+int launchListUpdateH(const uint32_t* groups, unsigned num, const uint32_t* bounds, unsigned ng0, const unsigned* nc, double* h,
                       uint64_t* keys, unsigned* flag, cudaStream_t s);
 
 //! out = ordered bits of max_i max_k |x_k,i - xs_k,i| (minimum image on periodic axes); out must hold the bits of 0

@@ -268,8 +268,9 @@ __device__ __forceinline__ bool targetOf(size_t n, const unsigned* nc, unsigned 
     return true;
 }
 
-/*! The target of this thread: thread i of the launch, or in list mode lane i % 32 of group groupList[i / 32]
- *  (GroupView slices of sph/include/sph/groups.hpp:96-103; a warp is one group). *w receives the list slot. */
+/*! The target of this thread: thread i of the launch, or in list mode lane i % 32 of group groupList[i / 32], whose
+ *  particles are [groupBounds[g], groupBounds[g + 1]) (GroupView slices of sph/include/sph/groups.hpp:96-103; a warp
+ *  is one group of at most 32). *w receives the list slot. */
 template<int kMode, class T>
 __device__ __forceinline__ bool chainTarget(const ChainArrays<T>& a, unsigned ngmax, Target& t, unsigned* w = nullptr)
 {
@@ -278,8 +279,9 @@ __device__ __forceinline__ bool chainTarget(const ChainArrays<T>& a, unsigned ng
         size_t slot = (blockIdx.x * size_t(blockDim.x) + threadIdx.x) >> 5;
         if (w) { *w = unsigned(slot); }
         if (slot >= a.numListed) { return false; }
-        t.i = size_t(__ldg(a.groupList + slot)) * 32 + (threadIdx.x & 31);
-        if (t.i >= a.n) { return false; }
+        uint32_t g = __ldg(a.groupList + slot);
+        t.i        = size_t(__ldg(a.groupBounds + g)) + (threadIdx.x & 31);
+        if (t.i >= __ldg(a.groupBounds + g + 1)) { return false; }
         t.group = t.i >> 5;
         t.lane  = unsigned(t.i & 31);
         t.count = min(a.nc[t.i] - 1u, ngmax);

@@ -127,9 +127,11 @@ struct ChainArrays
     DVRec<T>* dvrec{nullptr}; // set: AV cleaning (HydroVeProp<avClean = true>)
     T* dv[6]{};              // the same six fields as arrays (dV11 .. dV33)
     int threads{128}; // block size of the J-loop launches
-    // block time steps: the launch covers only the groups groupList[0, numListed) (one warp each); MomentumEnergy
+    // block time steps: the launch covers only the groups groupList[0, numListed) (one warp each); group g holds
+    // the particles [groupBounds[g], groupBounds[g + 1]) (at most 32, the spatial target groups); MomentumEnergy
     // then lowers groupDt[w] of listed group w to the Courant step of its particles
     const uint32_t* groupList{nullptr};
+    const uint32_t* groupBounds{nullptr};
     unsigned numListed{0};
     float* groupDt{nullptr};
 };

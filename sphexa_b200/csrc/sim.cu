@@ -676,11 +676,23 @@ int resetBdt(sphb_sim& s)
 int bdtSync(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
-    unsigned G      = unsigned(s.numGroups());
     if (activeRungOf(s.bts.substep, s.bts.numRungs) == 0)
     {
         SPHB_TRY(syncDomain(s));
-        SPHB_TRY(launchSequence(s.grpSfc.data(), G, 0, st)); // computeGroups: fixed groups in SFC order
+        // computeGroups -> computeSpatialGroups (sph/include/sph/groups.hpp:41-74; ve_hydro_bdt.hpp:185): the spatial
+        // target groups of 32 from the focus tree of this sync, tolFactor 2
+        unsigned G = 0;
+        SPHB_TRY(computeGroupSplits(0, s.n, s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fH].data(), SPHB_F64,
+                                    s.ftree.leaves.data(), s.ftree.numLeaves,
+                                    reinterpret_cast<const uint32_t*>(s.ftree.layout.data()), s.box, kWarp, 2.0f,
+                                    s.grpScratch, s.grpBounds, &G, st));
+        s.numBdtGroups = G;
+        SPHB_TRY(s.groupDt.reserve(G));
+        SPHB_TRY(s.groupIdx.reserve(G));
+        SPHB_TRY(s.grpSfc.reserve(G));
+        SPHB_TRY(s.grpTs.reserve(G));
+        SPHB_TRY(s.dtKeys.reserve(G));
+        SPHB_TRY(launchSequence(s.grpSfc.data(), G, 0, st));
         s.activeList = s.grpSfc.data();
         s.numActive  = G;
         std::vector<float> big(G, std::numeric_limits<float>::max());
@@ -722,6 +734,7 @@ int bdtChain(sphb_sim& s)
     HydroConsts<T> k = hydroConsts<T>(s);
     ChainArrays<T> l = a;
     l.groupList      = s.activeList;
+    l.groupBounds    = s.grpBounds.data();
     l.numListed      = s.numActive;
     l.groupDt        = s.groupDt.data();
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sXMass], st));
@@ -734,14 +747,15 @@ int bdtChain(sphb_sim& s)
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sIad], st));
     l.threads = chainThreads(s.mixed, sIad);
     SPHB_TRY(launchIadDivvCurlv(l, k, s.box, st));
-    SPHB_TRY(launchGroupDivv(s.activeList, s.numActive, s.n, a.divv, float(s.p.Krho), s.groupDt.data(), st));
+    SPHB_TRY(launchGroupDivv(s.activeList, s.numActive, s.grpBounds.data(), a.divv, float(s.p.Krho),
+                             s.groupDt.data(), st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sAV], st));
     l.threads = chainThreads(s.mixed, sAV);
     SPHB_TRY(launchAVswitches(l, k, s.box, s.minDt, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sMomentum], st));
     l.threads = chainThreads(s.mixed, sMomentum);
     SPHB_TRY(launchMomentumEnergy(l, k, s.box, st));
-    return launchGroupAcc(s.activeList, s.numActive, s.n, a.ax, a.ay, a.az, s.f[fH].data(), s.etaAcc,
+    return launchGroupAcc(s.activeList, s.numActive, s.grpBounds.data(), a.ax, a.ay, a.az, s.f[fH].data(), s.etaAcc,
                           s.groupDt.data(), st);
 }
 
@@ -815,7 +829,7 @@ int sortGroupDt(sphb_sim& s, unsigned num, float* minDt, float* fastDt, uint32_t
 int bdtComputeRungs(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
-    unsigned G      = unsigned(s.numGroups());
+    unsigned G      = s.numBdtGroups;
     int highRung    = activeRungOf(s.bts.substep, s.bts.numRungs);
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 2, 0, sizeof(unsigned), st));
     if (highRung == 0)
@@ -910,17 +924,17 @@ int bdtIntegrateRungs(sphb_sim& s)
         {
             if (s.bts.dtDrift[i] > 0)
             {
-                SPHB_TRY(launchDrift(list, num, s.n, 0.f, s.bts.dtDrift[i], steps, s.rung.data(), a, cv, st));
+                SPHB_TRY(launchDrift(list, num, s.grpBounds.data(), 0.f, s.bts.dtDrift[i], steps, s.rung.data(), a, cv, st));
             }
-            SPHB_TRY(launchRungPositions(list, num, s.n, s.bts.dtDrift[i] + dt, steps, s.rung.data(), a, box, cv,
+            SPHB_TRY(launchRungPositions(list, num, s.grpBounds.data(), s.bts.dtDrift[i] + dt, steps, s.rung.data(), a, box, cv,
                                          st));
             s.bts.dtm1[i]    = s.bts.dtDrift[i] + dt;
             s.bts.dtDrift[i] = 0;
-            SPHB_TRY(launchStoreRung(list, num, s.n, uint64_t(i), s.rung.data(), st));
+            SPHB_TRY(launchStoreRung(list, num, s.grpBounds.data(), uint64_t(i), s.rung.data(), st));
         }
         else
         {
-            SPHB_TRY(launchDrift(list, num, s.n, s.bts.dtDrift[i] + dt, s.bts.dtDrift[i], steps, s.rung.data(), a, cv,
+            SPHB_TRY(launchDrift(list, num, s.grpBounds.data(), s.bts.dtDrift[i] + dt, s.bts.dtDrift[i], steps, s.rung.data(), a, cv,
                                  st));
             s.bts.dtDrift[i] += dt;
         }
@@ -934,7 +948,7 @@ int bdtIntegrate(sphb_sim& s)
     SPHB_TRY(bdtComputeRungs(s));
     SPHB_TRY(s.mixed ? bdtIntegrateRungs<float>(s) : bdtIntegrateRungs<double>(s));
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 1, 0, sizeof(unsigned), st));
-    SPHB_TRY(launchListUpdateH(s.activeList, s.numActive, s.n, s.p.ng0, s.nc.data(), s.f[fH].data(), s.keys.data(),
+    SPHB_TRY(launchListUpdateH(s.activeList, s.numActive, s.grpBounds.data(), s.p.ng0, s.nc.data(), s.f[fH].data(), s.keys.data(),
                                s.status.data() + 1, st));
     s.hostMsg[13] = 0;
     SPHB_CUDA_TRY(cudaMemcpyAsync(s.hostMsg + 13, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));

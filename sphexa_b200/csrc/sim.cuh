@@ -8,6 +8,7 @@
 
 #include "adjoint.cuh"
 #include "bdt.cuh"
+#include "groups.cuh"
 #include "hydro.cuh"
 #include "integrate.cuh"
 #include "neighbors.cuh"
@@ -144,6 +145,10 @@ struct sphb_sim
     DeviceBuffer<float> groupDt;            // per group of the current group order
     DeviceBuffer<uint32_t> groupIdx;        // sort permutation of groupDt
     DeviceBuffer<uint32_t> grpSfc, grpTs;   // groups_ (SFC order after a full sync) and tsGroups_ (by time step)
+    DeviceBuffer<uint32_t> grpBounds;       // the spatial target groups of the last full sync: group g holds the
+                                            // particles [grpBounds[g], grpBounds[g + 1])
+    DeviceBuffer<int> grpScratch;
+    unsigned numBdtGroups{0};
     DeviceBuffer<uint64_t> dtKeys;
     DeviceBuffer<uint32_t> rungInfo;
     DeviceBuffer<double> xs, ys, zs;        // positions at the last full sync (drift bound of the tree search)

@@ -93,7 +93,7 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sim_upload_fields", "sphb_sim_load_fields", "sphb_sim_store_fields", "sphb_sim_bind_fields",
             "sphb_dataset_xmass", "sphb_dataset_ve_def_gradh", "sphb_ideal_gas_eos",
             "sphb_dataset_iad_divv_curlv", "sphb_dataset_av_switches", "sphb_dataset_momentum_energy",
-            "sphb_dataset_positions", "sphb_dataset_update_h")
+            "sphb_dataset_positions", "sphb_dataset_update_h", "sphb_compute_group_splits")
 
 _lib = None
 
@@ -180,6 +180,8 @@ def load() -> C.CDLL:
         "sphb_dataset_momentum_energy": (C.c_int, [P, S, S, C.POINTER(Box), C.POINTER(C.c_float)]),
         "sphb_dataset_positions": (C.c_int, [P, S, S, C.c_double, C.c_double, C.POINTER(Box)]),
         "sphb_dataset_update_h": (C.c_int, [P, S, S, C.c_uint]),
+        "sphb_compute_group_splits": (C.c_int, [S, S, P, P, P, P, C.c_int, P, S, P, C.POINTER(Box), C.c_uint,
+                                                C.c_float, P, S, C.POINTER(S), P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
