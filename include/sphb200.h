@@ -147,6 +147,18 @@ size_t sphb_sort_by_key_static_max(void);
 int sphb_gather8(const uint32_t* order, size_t n, int num_fields, const void* const* src, void* const* dst,
                  void* stream);
 
+/*! The internal (linked) octree of a cornerstone leaf array in the reference's OctreeData layout
+ *  (cstone/tree/octree.hpp:283-358): nodes sorted by level, then SFC key. With num_internal = (num_leaves - 1) / 7
+ *  and num_nodes = num_leaves + num_internal, the device arrays receive: prefixes [num_nodes] (placeholder-bit
+ *  keys), child_offsets [num_nodes] (first child, 0 for leaves), parents [max(1, (num_nodes - 1) / 8)] (parent of
+ *  every group of 8 siblings), internal_to_leaf [num_nodes] (leaf index, negative for internal nodes),
+ *  leaf_to_internal [num_nodes] (sorted node index by the reference's unsorted index: internal nodes first, then
+ *  leaves); level_range (host, 23 ints) the first node of every level. Host-blocking.
+ *  Replaces cstone::buildOctreeGpu (domain/include/cstone/tree/octree_gpu.cu:137-165) and its CPU twin
+ *  buildOctreeCpu (octree.hpp:170-196). */
+int sphb_build_octree(const uint64_t* leaves, size_t num_leaves, uint64_t* prefixes, int* child_offsets,
+                      int* parents, int* level_range, int* internal_to_leaf, int* leaf_to_internal, void* stream);
+
 /*! The ideal-gas EOS on caller arrays, per particle i in [first, last), in FP64 and stored in each array's type:
  *  rho = kx m / xm, p = rho u (gamma - 1) with u = cv(mui, gamma) temp (or u itself if given),
  *  c = sqrt(gamma u (gamma - 1)), prho = p / (kx m^2 gradh). fields names temp or u, m, kx, xm, gradh (read) and

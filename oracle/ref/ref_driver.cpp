@@ -566,6 +566,26 @@ extern "C"
         return numL;
     }
 
+    /*! @brief the reference's internal octree of a cornerstone leaf array (buildOctreeCpu via updateInternalTree,
+     *  cstone/tree/octree.hpp:170-196,358-364) in its OctreeData layout: prefixes, childOffsets, parents,
+     *  levelRange (maxTreeLevel + 2), internalToLeaf, leafToInternal; returns numNodes */
+    int ref_build_octree(const uint64_t* leaves, size_t numLeaves, uint64_t* prefixes, int* childOffsets,
+                         int* parents, int* levelRange, int* internalToLeaf, int* leafToInternal)
+    {
+        std::vector<uint64_t> tree(leaves, leaves + numLeaves + 1);
+        cstone::OctreeData<uint64_t, CpuTag> octree;
+        octree.resize(cstone::nNodes(tree));
+        cstone::updateInternalTree<uint64_t>(tree, octree.data());
+        int nn = octree.numNodes;
+        std::copy(octree.prefixes.begin(), octree.prefixes.begin() + nn, prefixes);
+        std::copy(octree.childOffsets.begin(), octree.childOffsets.begin() + nn, childOffsets);
+        std::copy(octree.parents.begin(), octree.parents.end(), parents);
+        std::copy(octree.levelRange.begin(), octree.levelRange.end(), levelRange);
+        std::copy(octree.internalToLeaf.begin(), octree.internalToLeaf.begin() + nn, internalToLeaf);
+        std::copy(octree.leafToInternal.begin(), octree.leafToInternal.begin() + nn, leafToInternal);
+        return nn;
+    }
+
     //! @brief reference neighbour search (findneighbors.hpp:77-170) on a fully converged bucket tree of sorted keys
     int ref_find_neighbors(size_t n, const uint64_t* keys, const double* x, const double* y, const double* z,
                            const double* h, const double* lim, int periodic, unsigned bucketSize, unsigned ngmax,

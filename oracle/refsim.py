@@ -230,6 +230,24 @@ def compute_octree(sorted_keys: np.ndarray, bucket: int):
     return leaves[:nl + 1].copy(), counts[:nl].copy()
 
 
+def build_octree(leaves: np.ndarray) -> dict:
+    """The reference's internal octree of a cornerstone leaf array (buildOctreeCpu), OctreeData arrays."""
+    lib = load(False)
+    lib.ref_build_octree.restype = C.c_int
+    lib.ref_build_octree.argtypes = [C.c_void_p, C.c_size_t] + [C.c_void_p] * 6
+    lv = np.ascontiguousarray(leaves, dtype=np.uint64)
+    nl = lv.size - 1
+    nn = nl + (nl - 1) // 7
+    out = {"prefixes": np.zeros(nn, dtype=np.uint64), "childOffsets": np.zeros(nn, dtype=np.int32),
+           "parents": np.zeros(max(1, (nn - 1) // 8), dtype=np.int32), "levelRange": np.zeros(23, dtype=np.int32),
+           "internalToLeaf": np.zeros(nn, dtype=np.int32), "leafToInternal": np.zeros(nn, dtype=np.int32)}
+    got = lib.ref_build_octree(ptr(lv), nl, *[ptr(out[k]) for k in ("prefixes", "childOffsets", "parents",
+                                                                     "levelRange", "internalToLeaf",
+                                                                     "leafToInternal")])
+    assert got == nn
+    return out
+
+
 def find_neighbors(sorted_keys, x, y, z, h, box, periodic, ngmax, bucket=64):
     """Reference neighbour lists (no h iteration) for particles already in SFC order."""
     lib = load(False)

@@ -292,13 +292,16 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             T aMom, bMom, sigma = T(0);
             int branch;
             T atwood = fdiv(fabs(rhoi - rhoj), rhoi + rhoj);
-            if (atwood < k.Atmin)
+            // the forward's branch decision: FP32 compares the thresholds without the division
+            bool belowMin = sizeof(T) == 4 ? fabs(rhoi - rhoj) < k.Atmin * (rhoi + rhoj) : atwood < k.Atmin;
+            bool aboveMax = sizeof(T) == 4 ? fabs(rhoi - rhoj) > k.Atmax * (rhoi + rhoj) : atwood > k.Atmax;
+            if (belowMin)
             {
                 aMom   = xmassi * xmassi;
                 bMom   = xmassj * xmassj;
                 branch = 0;
             }
-            else if (atwood > k.Atmax)
+            else if (aboveMax)
             {
                 aMom   = xmassi * xmassj;
                 bMom   = aMom;

@@ -79,6 +79,18 @@ __device__ __forceinline__ T tableLookup(const T* __restrict__ table, T v)
     return t0 + derivative * (v - T(idx) * dx);
 }
 
+//! Horner evaluation of the FP32 kernel polynomial at t = v^2/2 - 1
+__device__ __forceinline__ float polyEvalT(const float (&c)[kPolyTerms], float t)
+{
+    float acc = c[kPolyTerms - 1];
+#pragma unroll
+    for (int p = kPolyTerms - 2; p >= 0; --p)
+    {
+        acc = fmaf(acc, t, c[p]);
+    }
+    return acc;
+}
+
 //! Horner evaluation of the FP32 kernel polynomial in t = v^2/2 - 1
 __device__ __forceinline__ float polyEval(const float (&c)[kPolyTerms], float v)
 {
@@ -101,6 +113,24 @@ __device__ __forceinline__ T kernelW(const T* __restrict__ table, const HydroCon
         if (k.usePoly) { return v < T(2) ? polyEval(k.wpoly, v) : T(0); }
     }
     return tableLookup(table, v);
+}
+
+/*! W of a pair from its squared separation r2, for a target with hInv = 1/h and hh = hInv^2 / 2. FP32 with the
+ *  polynomial: t = v^2/2 - 1 = r2 hh - 1 directly, zero from t = 1 (v = 2) on, without the square root. Otherwise
+ *  (FP64, or an FP32 simulation whose polynomial fit failed) the table at v = sqrt(r2) hInv, the expression of the
+ *  reference's order. */
+template<class T>
+__device__ __forceinline__ T kernelWr2(const T* __restrict__ table, const HydroConsts<T>& k, T r2, T hInv, T hh)
+{
+    if constexpr (sizeof(T) == 4)
+    {
+        if (k.usePoly)
+        {
+            float t = fmaf(r2, hh, -1.0f);
+            return t < 1.0f ? polyEvalT(k.wpoly, t) : 0.0f;
+        }
+    }
+    return tableLookup(table, T(sqrt(r2)) * hInv);
 }
 
 //! dW/dv, zero from v = 2 on

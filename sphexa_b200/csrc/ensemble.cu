@@ -103,6 +103,7 @@ struct sphb_ensemble
     DeviceBuffer<double> gamma, cv, dt, dtm1, ttot, cons;
     DeviceBuffer<unsigned long long> reduce;
     DeviceBuffer<unsigned> status; // [0] search overflow, [1] h flag, [2] sort look-back timeout
+    DeviceBuffer<uint32_t> sortFlags; // [0] pairs out of order before the tile repair, [1] after it
 
     // trees
     std::vector<std::unique_ptr<GlobalTree>> gtrees;
@@ -325,6 +326,7 @@ int allocate(sphb_ensemble& e)
     SPHB_TRY(e.cons.reserve(size_t(kNumCons) * m));
     SPHB_TRY(e.reduce.reserve(2 * size_t(m)));
     SPHB_TRY(e.status.reserve(4));
+    SPHB_TRY(e.sortFlags.reserve(2));
     SPHB_TRY(e.views.reserve(m));
     SPHB_TRY(e.leafDescs.reserve(m));
     for (auto& ev : e.ev)
@@ -423,21 +425,27 @@ void swapState(sphb_ensemble& e)
 }
 
 /*! keys, segmented sort, gather of 16 fields into the other buffer set, which then becomes the current one (a
- *  captured step records the buffers of its set; the two captured steps alternate) */
+ *  captured step records the buffers of its set; the two captured steps alternate). The sort is decided on the
+ *  device, as the single simulation's nearly-sorted sort is on the host: the particles of the previous step are
+ *  nearly in order within every instance, so the tiles holding out-of-order pairs are repaired in shared memory,
+ *  and the full segmented radix sort (by key over all slots, then stably by instance) runs only if pairs remain out
+ *  of order (every one of its kernels reads that count and returns at once when it is zero). The result is the same
+ *  stable sort either way. */
 int syncBatched(sphb_ensemble& e, bool withLayout)
 {
     cudaStream_t st = e.stream;
     size_t n        = e.slots;
     SPHB_TRY(launchSfcKeys(e.f[0].data(), e.f[1].data(), e.f[2].data(), e.keys.data(), n, e.box, st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(e.keysTmp.data(), e.keys.data(), n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
-    // by key over all slots, then stably by instance: every instance's particles in key order, padding last
-    SPHB_TRY(sortByKeyAsync(e.keysTmp.data(), e.order.data(), n, true, e.sortScratch.data(),
-                            e.sortScratch.capacity(), 0xffu, e.status.data() + 2, st));
+    SPHB_TRY(repairSegmentedAsync(e.keysTmp.data(), e.order.data(), e.segOfSlot.data(), n, e.sortFlags.data(), st));
+    const uint32_t* remaining = e.sortFlags.data() + 1;
+    SPHB_TRY(sortByKeyAsync(e.keysTmp.data(), e.order.data(), n, false, e.sortScratch.data(),
+                            e.sortScratch.capacity(), 0xffu, e.status.data() + 2, st, remaining));
     const void* segSrc[1] = {e.segOfSlot.data()};
     void* segDst[1]       = {e.segKey.data()};
     SPHB_TRY(gather8(e.order.data(), n, 1, segSrc, segDst, st));
     SPHB_TRY(sortByKeyAsync(e.segKey.data(), e.order.data(), n, false, e.sortScratch.data(),
-                            e.sortScratch.capacity(), 0x1u, e.status.data() + 2, st));
+                            e.sortScratch.capacity(), 0x1u, e.status.data() + 2, st, remaining));
     const void* src[16];
     void* dst[16];
     for (int k = 0; k < kFields; ++k)
@@ -451,7 +459,7 @@ int syncBatched(sphb_ensemble& e, bool withLayout)
     dst[15] = e.keysAlt.data();
     SPHB_TRY(gather8(e.order.data(), n, 16, src, dst, st));
     swapState(e);
-    countLaunch(6);
+    countLaunch(9);
     if (e.skin)
     {
         // the skin rows hold build indices: compose this sort into the current-to-build map

@@ -5,6 +5,7 @@
 // reads a few status words per update to drive the convergence loops, as the reference's loops do
 // (cstone/domain/assignment.hpp:114-123, cstone/focus/octree_focus_mpi.hpp:582-599).
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "octree.cuh"
@@ -744,4 +745,89 @@ extern "C" int sphb_compute_octree(const uint64_t* sorted_keys, size_t n, unsign
     }
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
     return size_t(g.numLeaves) + 1 <= capacity ? SPHB_OK : SPHB_ERR_CAPACITY;
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// The linked octree in the reference's OctreeData layout (cstone/tree/octree.hpp:283-358)
+// ------------------------------------------------------------------------------------------------------------------
+namespace sphb
+{
+namespace
+{
+
+//! digitWeight of the reference's binary-radix to octree index map (cstone/sfc/common.hpp:318-322)
+__device__ __forceinline__ int refDigitWeight(int digit)
+{
+    int fourGeqMask = -int(digit >= 4);
+    return ((7 - digit) & fourGeqMask) - (digit & ~fourGeqMask);
+}
+
+/*! internalToLeaf / leafToInternal in the reference's unsorted-index convention (createUnsortedLayoutCpu,
+ *  octree.hpp:77-99 and buildOctreeCpu, :170-196): the unsorted index of leaf l is numInternal + l, that of the
+ *  internal node found at leaf boundary tid (common prefix a multiple of 3 bits) is
+ *  (tid + binaryKeyWeight(key, level)) / 7; internalToLeaf[sorted] = unsorted - numInternal,
+ *  leafToInternal[unsorted] = sorted. */
+__global__ void refNodeMapKernel(const uint64_t* leaves, int numLeaves, int numInternal, const uint64_t* prefixes,
+                                 int numNodes, const int* leafToNode, int* internalToLeaf, int* leafToInternal)
+{
+    int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= numLeaves) { return; }
+    int sortedLeaf                       = leafToNode[tid];
+    internalToLeaf[sortedLeaf]           = tid;
+    leafToInternal[numInternal + tid]    = sortedLeaf;
+    if (tid >= numLeaves - 1) { return; }
+    uint64_t key     = leaves[tid];
+    int prefixLength = int(__clzll(key ^ leaves[tid + 1])) - 1;
+    if (prefixLength % 3 != 0) { return; }
+    int level  = prefixLength / 3;
+    int weight = 0;
+    for (int l = 1; l <= level + 1; ++l)
+    {
+        weight += refDigitWeight(int((key >> (3 * (int(kMaxLevel) - l))) & 7u));
+    }
+    int octIndex    = (tid + weight) / 7;
+    uint64_t prefix = (uint64_t(1) << prefixLength) | (key >> (3 * int(kMaxLevel) - prefixLength));
+    // sorted position of this internal node: prefixes are unique and sorted
+    int lo = 0, hi = numNodes;
+    while (lo < hi)
+    {
+        int mid = (lo + hi) >> 1;
+        if (prefixes[mid] < prefix) { lo = mid + 1; }
+        else { hi = mid; }
+    }
+    internalToLeaf[lo]       = octIndex - numInternal;
+    leafToInternal[octIndex] = lo;
+}
+
+} // namespace
+} // namespace sphb
+
+extern "C" int sphb_build_octree(const uint64_t* leaves, size_t num_leaves, uint64_t* prefixes, int* child_offsets,
+                                 int* parents, int* level_range, int* internal_to_leaf, int* leaf_to_internal,
+                                 void* stream)
+{
+    using namespace sphb;
+    if (!leaves || num_leaves == 0 || num_leaves >= (size_t(1) << 30) || !prefixes || !child_offsets || !parents ||
+        !level_range || !internal_to_leaf || !leaf_to_internal)
+    {
+        return SPHB_ERR_ARG;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    LinkedOctree t;
+    TreeScratch sc;
+    SPHB_TRY(buildLinkedOctree(leaves, int(num_leaves), t, sc, st));
+    int nn = t.numNodes;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(prefixes, t.prefixes.data(), nn * sizeof(uint64_t), cudaMemcpyDeviceToDevice, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(child_offsets, t.childOffsets.data(), nn * sizeof(int), cudaMemcpyDeviceToDevice,
+                                  st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(parents, t.parents.data(), std::max(1, (nn - 1) / 8) * sizeof(int),
+                                  cudaMemcpyDeviceToDevice, st));
+    refNodeMapKernel<<<ceilDiv(num_leaves, 256), 256, 0, st>>>(leaves, t.numLeaves, t.numInternal, t.prefixes.data(),
+                                                                 nn, t.leafToNode.data(), internal_to_leaf,
+                                                                 leaf_to_internal);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    std::memcpy(level_range, t.levelRange, sizeof(t.levelRange));
+    return SPHB_OK;
 }

@@ -64,8 +64,9 @@ SortScratch carve(void* base, size_t n)
 
 //! digit histograms of all 8 byte positions in one sweep over the keys
 __global__ void __launch_bounds__(256) histogramKernel(const uint64_t* __restrict__ keys, size_t n,
-                                                       uint32_t* __restrict__ hist)
+                                                       uint32_t* __restrict__ hist, const uint32_t* gate)
 {
+    if (gate && *gate == 0) { return; }
     __shared__ uint32_t sh[kPasses][kRadix];
     for (int t = threadIdx.x; t < kPasses * kRadix; t += blockDim.x)
     {
@@ -90,8 +91,9 @@ __global__ void __launch_bounds__(256) histogramKernel(const uint64_t* __restric
 }
 
 //! exclusive scan of each pass's 256 digit counts, in place (one block per pass)
-__global__ void histScanKernel(uint32_t* hist)
+__global__ void histScanKernel(uint32_t* hist, const uint32_t* gate)
 {
+    if (gate && *gate == 0) { return; }
     __shared__ uint32_t sh[kRadix];
     uint32_t* h = hist + blockIdx.x * kRadix;
     int t       = threadIdx.x;
@@ -202,6 +204,99 @@ __global__ void __launch_bounds__(kRepairThreads) repairTilesKernel(uint64_t* ke
     }
 }
 
+//! *count += adjacent pairs of one segment out of key order: seg[i] == seg[i + 1] and keys[i] > keys[i + 1]
+__global__ void __launch_bounds__(256) inversionsSegKernel(const uint64_t* __restrict__ keys,
+                                                           const uint64_t* __restrict__ seg, size_t n,
+                                                           uint32_t* count)
+{
+    uint32_t c = 0;
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i + 1 < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        c += (keys[i] > keys[i + 1] && seg[i] == seg[i + 1]) ? 1u : 0u;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    __shared__ uint32_t warpSum[8];
+    if ((threadIdx.x & 31) == 0) { warpSum[threadIdx.x >> 5] = c; }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        uint32_t s = 0;
+        for (int w = 0; w < 8; ++w)
+        {
+            s += warpSum[w];
+        }
+        if (s) { atomicAdd(count, s); }
+    }
+}
+
+/*! repairTilesKernel for an array of contiguous segments (slot ranges that keep their segment): the tile is sorted
+ *  stably by (segment, key), so a tile that straddles two segments keeps each segment's slots within it. */
+__global__ void __launch_bounds__(kRepairThreads) repairTilesSegKernel(uint64_t* keys, uint32_t* vals,
+                                                                      const uint64_t* seg, size_t n, size_t offset)
+{
+    __shared__ uint64_t sk[kRepairTile];
+    __shared__ uint32_t sv[kRepairTile];
+    __shared__ uint16_t sp[kRepairTile];
+    __shared__ uint8_t sg[kRepairTile];
+    size_t t0 = offset + size_t(blockIdx.x) * kRepairTile;
+    if (t0 >= n) { return; }
+    size_t len = min(size_t(kRepairTile), n - t0);
+    bool d     = false;
+    for (size_t q = threadIdx.x; q + 1 < len; q += kRepairThreads)
+    {
+        d = d || (keys[t0 + q] > keys[t0 + q + 1] && seg[t0 + q] == seg[t0 + q + 1]);
+    }
+    if (__syncthreads_or(d) == 0) { return; }
+    // segments are ranked by their order within the tile (they are contiguous and ascending)
+    uint64_t seg0 = seg[t0];
+    for (int q = threadIdx.x; q < kRepairTile; q += kRepairThreads)
+    {
+        bool in = size_t(q) < len;
+        sk[q]   = in ? keys[t0 + q] : ~uint64_t(0);
+        sv[q]   = in ? vals[t0 + q] : 0u;
+        sp[q]   = uint16_t(q);
+        sg[q]   = in ? uint8_t(min(seg[t0 + q] - seg0, uint64_t(254))) : uint8_t(255);
+    }
+    __syncthreads();
+    for (int size = 2; size <= kRepairTile; size <<= 1)
+    {
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+        {
+            for (int q = threadIdx.x; q < kRepairTile; q += kRepairThreads)
+            {
+                int p = q ^ stride;
+                if (p > q)
+                {
+                    bool up      = (q & size) == 0;
+                    bool greater = sg[q] > sg[p] ||
+                                   (sg[q] == sg[p] && (sk[q] > sk[p] || (sk[q] == sk[p] && sp[q] > sp[p])));
+                    if (greater == up)
+                    {
+                        uint64_t k = sk[q];
+                        sk[q]      = sk[p];
+                        sk[p]      = k;
+                        uint32_t v = sv[q];
+                        sv[q]      = sv[p];
+                        sv[p]      = v;
+                        uint16_t o = sp[q];
+                        sp[q]      = sp[p];
+                        sp[p]      = o;
+                        uint8_t g  = sg[q];
+                        sg[q]      = sg[p];
+                        sg[p]      = g;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (size_t q = threadIdx.x; q < len; q += kRepairThreads)
+    {
+        keys[t0 + q] = sk[q];
+        vals[t0 + q] = sv[q];
+    }
+}
+
 /*! One onesweep pass over bits [shift, shift+8).
  *
  * Shared memory: per-warp digit counters (8 x 256), the tile's exclusive digit prefix (256) and the tile index.
@@ -211,8 +306,10 @@ __global__ void __launch_bounds__(kSortThreads) onesweepKernel(const uint64_t* _
                                                                uint64_t* __restrict__ keysOut,
                                                                uint32_t* __restrict__ valsOut, size_t n, int shift,
                                                                const uint32_t* __restrict__ digitOffsets,
-                                                               uint32_t* status, uint32_t* counters)
+                                                               uint32_t* status, uint32_t* counters,
+                                                               const uint32_t* gate)
 {
+    if (gate && *gate == 0) { return; } // the whole pass is skipped: no tile waits on another
     __shared__ uint32_t warpCount[kSortWarps][kRadix];
     __shared__ uint32_t tilePrefix[kRadix];
     __shared__ uint32_t tileIdxSh;
@@ -343,7 +440,7 @@ size_t sortScratchBytes(size_t n)
 namespace
 {
 int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, unsigned passMask,
-              cudaStream_t stream);
+              cudaStream_t stream, const uint32_t* gate = nullptr);
 
 __global__ void orErrorKernel(const uint32_t* err, uint32_t* out)
 {
@@ -367,7 +464,7 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
 
     SPHB_CUDA_TRY(cudaMemsetAsync(s.hist, 0, kPasses * kRadix * sizeof(uint32_t), stream));
     unsigned histBlocks = unsigned(std::min<size_t>(ceilDiv(n, 256 * 16), size_t(smCount()) * 4));
-    histogramKernel<<<histBlocks, 256, 0, stream>>>(keys, n, s.hist);
+    histogramKernel<<<histBlocks, 256, 0, stream>>>(keys, n, s.hist, nullptr);
     SPHB_CUDA_TRY(cudaGetLastError());
 
     // decide on the host which passes are trivial (one digit holds every key)
@@ -441,7 +538,7 @@ int sortNearlySorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, 
 }
 
 int sortByKeyAsync(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void* scratch, size_t scratchBytes,
-                   unsigned passMask, uint32_t* errorOut, cudaStream_t stream)
+                   unsigned passMask, uint32_t* errorOut, cudaStream_t stream, const uint32_t* gate)
 {
     if (n == 0) { return kOk; }
     if (n >= (size_t(1) << 30)) { return kErrArg; }
@@ -454,9 +551,9 @@ int sortByKeyAsync(uint64_t* keys, uint32_t* values, size_t n, bool initValues, 
     }
     SPHB_CUDA_TRY(cudaMemsetAsync(s.hist, 0, kPasses * kRadix * sizeof(uint32_t), stream));
     unsigned histBlocks = unsigned(std::min<size_t>(ceilDiv(n, 256 * 16), size_t(smCount()) * 4));
-    histogramKernel<<<histBlocks, 256, 0, stream>>>(keys, n, s.hist);
+    histogramKernel<<<histBlocks, 256, 0, stream>>>(keys, n, s.hist, gate);
     SPHB_CUDA_TRY(cudaGetLastError());
-    SPHB_TRY(runPasses(keys, values, n, s, passMask, stream));
+    SPHB_TRY(runPasses(keys, values, n, s, passMask, stream, gate));
     if (errorOut) { orErrorKernel<<<1, 1, 0, stream>>>(s.counters + 1, errorOut); }
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -465,11 +562,24 @@ int sortByKeyAsync(uint64_t* keys, uint32_t* values, size_t n, bool initValues, 
 namespace
 {
 
-//! scan the histograms and run the passes of passMask (bit p: digit p), leaving the result in keys/values
-int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, unsigned passMask,
-              cudaStream_t stream)
+//! keys/values from the alternate buffers, unless the gate is closed (the passes did not run)
+__global__ void gatedCopyKernel(const uint64_t* kIn, const uint32_t* vIn, uint64_t* kOut, uint32_t* vOut, size_t n,
+                                const uint32_t* gate)
 {
-    histScanKernel<<<kPasses, kRadix, 0, stream>>>(s.hist);
+    if (*gate == 0) { return; }
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        kOut[i] = kIn[i];
+        vOut[i] = vIn[i];
+    }
+}
+
+//! scan the histograms and run the passes of passMask (bit p: digit p), leaving the result in keys/values; with a
+//! gate, every kernel returns at once when *gate is 0 (device-side decision, capturable)
+int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, unsigned passMask,
+              cudaStream_t stream, const uint32_t* gate)
+{
+    histScanKernel<<<kPasses, kRadix, 0, stream>>>(s.hist, gate);
     SPHB_CUDA_TRY(cudaGetLastError());
     SPHB_CUDA_TRY(cudaMemsetAsync(s.counters + 1, 0, sizeof(uint32_t), stream));
 
@@ -484,12 +594,19 @@ int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, 
         SPHB_CUDA_TRY(cudaMemsetAsync(s.status, 0, tiles * kRadix * sizeof(uint32_t), stream));
         SPHB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(uint32_t), stream));
         onesweepKernel<<<unsigned(tiles), kSortThreads, 0, stream>>>(kIn, vIn, kOut, vOut, n, p * kRadixBits,
-                                                                      s.hist + p * kRadix, s.status, s.counters);
+                                                                      s.hist + p * kRadix, s.status, s.counters,
+                                                                      gate);
         SPHB_CUDA_TRY(cudaGetLastError());
         std::swap(kIn, kOut);
         std::swap(vIn, vOut);
     }
-    if (kIn != keys)
+    if (kIn != keys && gate)
+    {
+        unsigned blocks = unsigned(std::min<size_t>(ceilDiv(n, 256), size_t(smCount()) * 8));
+        gatedCopyKernel<<<blocks, 256, 0, stream>>>(kIn, vIn, keys, values, n, gate);
+        SPHB_CUDA_TRY(cudaGetLastError());
+    }
+    else if (kIn != keys)
     {
         SPHB_CUDA_TRY(cudaMemcpyAsync(keys, kIn, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, stream));
         SPHB_CUDA_TRY(cudaMemcpyAsync(values, vIn, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, stream));
@@ -498,6 +615,23 @@ int runPasses(uint64_t* keys, uint32_t* values, size_t n, const SortScratch& s, 
 }
 
 } // namespace
+
+int repairSegmentedAsync(uint64_t* keys, uint32_t* values, const uint64_t* seg, size_t n, uint32_t* flags,
+                         cudaStream_t stream)
+{
+    SPHB_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * sizeof(uint32_t), stream));
+    if (n == 0) { return kOk; }
+    unsigned blocks = unsigned(std::min<size_t>(ceilDiv(n, 256 * 8), size_t(smCount()) * 8));
+    iotaKernel<<<ceilDiv(n, 256), 256, 0, stream>>>(values, n);
+    inversionsSegKernel<<<blocks, 256, 0, stream>>>(keys, seg, n, flags);
+    repairTilesSegKernel<<<unsigned(ceilDiv(n, size_t(kRepairTile))), kRepairThreads, 0, stream>>>(keys, values, seg,
+                                                                                                   n, 0);
+    repairTilesSegKernel<<<unsigned(ceilDiv(n, size_t(kRepairTile))), kRepairThreads, 0, stream>>>(
+        keys, values, seg, n, kRepairTile / 2);
+    inversionsSegKernel<<<blocks, 256, 0, stream>>>(keys, seg, n, flags + 1);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
 
 // ---------------------------------------------------------------------------------------------------------------
 // Allocation-free variant: the scratch lives in a fixed device array of this library (see sphb_sort_by_key_static)

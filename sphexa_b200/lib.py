@@ -93,7 +93,8 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_sim_upload_fields", "sphb_sim_load_fields", "sphb_sim_store_fields", "sphb_sim_bind_fields",
             "sphb_dataset_xmass", "sphb_dataset_ve_def_gradh", "sphb_ideal_gas_eos",
             "sphb_dataset_iad_divv_curlv", "sphb_dataset_av_switches", "sphb_dataset_momentum_energy",
-            "sphb_dataset_positions", "sphb_dataset_update_h", "sphb_compute_group_splits")
+            "sphb_dataset_positions", "sphb_dataset_update_h", "sphb_compute_group_splits",
+            "sphb_build_octree")
 
 _lib = None
 
@@ -182,6 +183,7 @@ def load() -> C.CDLL:
         "sphb_dataset_update_h": (C.c_int, [P, S, S, C.c_uint]),
         "sphb_compute_group_splits": (C.c_int, [S, S, P, P, P, P, C.c_int, P, S, P, C.POINTER(Box), C.c_uint,
                                                 C.c_float, P, S, C.POINTER(S), P]),
+        "sphb_build_octree": (C.c_int, [P, S, P, P, P, P, P, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
