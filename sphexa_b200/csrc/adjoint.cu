@@ -171,6 +171,34 @@ __device__ __forceinline__ V3<T> sepV(const Sep<T>& r)
 // -------------------------------------------------------------------------------------------------------------------
 // integration (positions.hpp:77-111) and end-of-step h update (update_h.hpp:12-33)
 // -------------------------------------------------------------------------------------------------------------------
+//! add the MomentumEnergy adjoint's vector-atomic neighbour sums (AdjArrays::jacc) into the per-field adjoints
+template<class T>
+__global__ void foldNeighbourSumsKernel(size_t n, AdjArrays<T> g)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    const float4* q = g.jacc + i * 5;
+    float4 a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
+    g.x[i] += a.x;
+    g.y[i] += a.y;
+    g.z[i] += a.z;
+    g.h[i] += a.w;
+    g.vx[i] += b.x;
+    g.vy[i] += b.y;
+    g.vz[i] += b.z;
+    g.c[i] += b.w;
+    g.cij[0][i] += c.x;
+    g.cij[1][i] += c.y;
+    g.cij[2][i] += c.z;
+    g.cij[3][i] += c.w;
+    g.cij[4][i] += d.x;
+    g.cij[5][i] += d.y;
+    g.alpha[i] += d.z;
+    g.prho[i] += d.w;
+    g.xm[i] += e.x;
+    g.vol[i] += e.y;
+}
+
 template<class T>
 __global__ void integrationVjpKernel(AdjointStepArgs s, const unsigned* nc, StateAdj post, StateAdj work,
                                      AdjArrays<T> g)
@@ -420,6 +448,19 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             viB.y += vijB.y;
             viB.z += vijB.z;
             // neighbour side
+            if constexpr (sizeof(T) == 4)
+            {
+                if (g.jacc)
+                {
+                    float4* q = g.jacc + size_t(j) * 5;
+                    atomicAdd(q + 0, make_float4(-rB.x, -rB.y, -rB.z, hjB));
+                    atomicAdd(q + 1, make_float4(-vijB.x, -vijB.y, -vijB.z, cjB));
+                    atomicAdd(q + 2, make_float4(cjCB[0], cjCB[1], cjCB[2], cjCB[3]));
+                    atomicAdd(q + 3, make_float4(cjCB[4], cjCB[5], alphajB, prhojB));
+                    atomicAdd(reinterpret_cast<float2*>(q + 4), make_float2(xmjB, -rhojB * rhoj / hj.vol));
+                    continue;
+                }
+            }
             scatterPos(g, j, rB);
             atomicAdd(g.vx + j, -vijB.x);
             atomicAdd(g.vy + j, -vijB.y);
@@ -1030,7 +1071,16 @@ int stepVjp(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box,
         SPHB_CUDA_TRY(cudaMemsetAsync(f, 0, s.n * sizeof(T), stream));
     }
     integrationVjpKernel<T><<<nb, kChainThreads, 0, stream>>>(s, a.nc, post, work, g);
+    if (sizeof(T) == 4 && g.jacc)
+    {
+        SPHB_CUDA_TRY(cudaMemsetAsync(g.jacc, 0, a.n * 5 * sizeof(float4), stream));
+    }
     momentumEnergyVjpKernel<T><<<nb, kChainThreads, 0, stream>>>(a, k, box, g);
+    if (sizeof(T) == 4 && g.jacc)
+    {
+        foldNeighbourSumsKernel<T><<<ceilDiv(a.n, 256), 256, 0, stream>>>(a.n, g);
+        countLaunch();
+    }
     avSwitchesVjpKernel<T><<<nb, kChainThreads, 0, stream>>>(a, k, box, s.dtAV, s.alphaPre, g, work.f[13],
                                                               s.alphamaxBar);
     divvVjpKernel<T><<<nb, kChainThreads, 0, stream>>>(a, k, box, g);

@@ -27,6 +27,10 @@ struct AdjArrays
     T* gradh;
     T *ax, *ay, *az;
     T* du;
+    /*! FP32 only (may be null): the MomentumEnergy adjoint's neighbour-side sums, 5 float4 per particle
+     *  {x, y, z, h} {vx, vy, vz, c} {c11, c12, c13, c22} {c23, c33, alpha, prho} {xm, vol, -, -}, added with vector
+     *  atomics (5 per pair instead of 18 scalar ones) and folded into the arrays above after that kernel */
+    float4* jacc{nullptr};
 };
 
 //! number of T arrays in AdjArrays

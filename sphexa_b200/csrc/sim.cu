@@ -977,6 +977,7 @@ int allocateAdjoint(sphb_sim& s)
     SPHB_TRY(s.tapeT.reserve(8 * n * s.elemBytes()));
     SPHB_TRY(s.tapeJ.reserve(n));
     SPHB_TRY(s.adjT.reserve(size_t(kNumAdjFields) * n * s.elemBytes()));
+    if (s.mixed) { SPHB_TRY(s.adjJacc.reserve(5 * n)); }
     SPHB_TRY(s.adjWork.reserve(14 * n));
     SPHB_TRY(s.adjScalar.reserve(1));
     return kOk;
@@ -1070,6 +1071,7 @@ int runStepVjp(sphb_sim& s, const double* const* post, double* const* pre, doubl
     {
         *slots[q] = base + size_t(q) * s.n;
     }
+    if constexpr (sizeof(T) == 4) { g.jacc = s.adjJacc.data(); }
     SPHB_CUDA_TRY(cudaMemsetAsync(s.adjScalar.data(), 0, sizeof(double), s.stream));
     SPHB_TRY(stepVjp<T>(a, k, s.box, args, postA, preA, g, work, s.stream));
     double amB = 0;

@@ -102,6 +102,7 @@ struct sphb_sim
     DeviceBuffer<int> tapeJ;
     DeviceBuffer<char> adjT;
     DeviceBuffer<double> adjWork, adjScalar;
+    DeviceBuffer<float4> adjJacc; // FP32 adjoint: vector-atomic neighbour sums of the MomentumEnergy adjoint
     // recorded steps: copies of everything the step adjoint reads, one slot per step of a checkpoint segment
     DeviceBuffer<char> tapeSlots;
     size_t tapeSlotBytes{0};
