@@ -175,6 +175,37 @@ int sphb_ideal_gas_eos(size_t first, size_t last, double mui, double gamma, cons
 int sphb_compute_octree(const uint64_t* sorted_keys, size_t n, unsigned bucket, uint64_t* leaves, uint32_t* counts,
                         size_t capacity, size_t* num_leaves, void* stream);
 
+/*! Leaf counts of a rank's sorted keys in the shared global tree: counts[i] = keys in [leaves[i], leaves[i + 1]).
+ *  leaves holds num_leaves + 1 keys of a cornerstone array. Device arrays; stream-ordered.
+ *  Replaces cstone::computeNodeCounts as cstone::updateOctreeGlobal calls it before its count all-reduce
+ *  (domain/include/cstone/tree/update_mpi.hpp:64-99; csarray.hpp:181-235, GPU twin computeNodeCountsGpu
+ *  csarray_gpu.cu:85-119). */
+int sphb_leaf_counts(const uint64_t* leaves, size_t num_leaves, const uint64_t* sorted_keys, size_t n,
+                     uint32_t* counts, void* stream);
+
+/*! One rebalance step of a cornerstone tree on given (all-reduced) leaf counts: leaves with more than bucket particles
+ *  split, groups of 8 sibling leaves with at most bucket together merge. new_leaves (not aliasing leaves) receives
+ *  *num_new + 1 keys if *num_new + 1 <= capacity (else SPHB_ERR_CAPACITY; *num_new and *converged are always
+ *  written); *converged = 1 if the step changed nothing. Device arrays; host-blocking.
+ *  Replaces cstone::rebalanceDecision + rebalanceTree as updateOctreeGlobal applies them
+ *  (domain/include/cstone/tree/update_mpi.hpp:64-99; csarray.hpp:248-389, GPU twins rebalanceDecisionGpu /
+ *  rebalanceTreeGpu csarray_gpu.cu:121-213). */
+int sphb_rebalance_tree(const uint64_t* leaves, size_t num_leaves, const uint32_t* counts, unsigned bucket,
+                        uint64_t* new_leaves, size_t capacity, size_t* num_new, int* converged, void* stream);
+
+/*! Halo discovery of one rank on the shared global tree (num_leaves + 1 keys). The rank owns the leaves
+ *  [first_leaf, last_leaf); its particles are in SFC order in x, y, z, h (h_dtype SPHB_F32 or SPHB_F64), leaf
+ *  first_leaf + i holding the particles [layout[i], layout[i + 1]) (last_leaf - first_leaf + 1 offsets). The search
+ *  box of an owned leaf is the smallest box holding the leaf's geometric centre and the cube x +- h * 2 search_ext of
+ *  each of its particles (the radius rounded in h's type); flags[l] (num_leaves bytes) becomes 1 for every leaf l
+ *  outside the owned range whose cell overlaps a search box (minimum image on periodic axes), else 0. Device arrays;
+ *  host-blocking. Replaces cstone::FocusedOctree::discoverHalos (domain/include/cstone/focus/
+ *  octree_focus_mpi.hpp:513-571: computeBoundingBoxGpu, focus/source_center_gpu.cu:23-92, and findHalosGpu,
+ *  traversal/collisions.hpp:40-104), on the global tree instead of the focus tree. */
+int sphb_find_halos(const uint64_t* leaves, size_t num_leaves, const double* x, const double* y, const double* z,
+                    const void* h, int h_dtype, const uint32_t* layout, size_t first_leaf, size_t last_leaf,
+                    const sphb_box* box, float search_ext, uint8_t* flags, void* stream);
+
 /*! Spatial target groups of the particles [first, last), which are in SFC order: fixed runs of group_size (32 or 64)
  *  consecutive particles, each split after every particle whose successor lies farther than
  *  min(tol_factor * the run's smallest leaf edge, 2 h) (lengths relative to the box; the leaf edge from leaves

@@ -20,6 +20,7 @@
 #include <string>
 
 #include "cstone/domain/domain.hpp"
+#include "cstone/traversal/collisions.hpp"
 #include "cstone/fields/field_get.hpp"
 #include "sph/particles_data.hpp"
 #include "sph/sph.hpp"
@@ -612,5 +613,89 @@ extern "C"
                                                     sizes.data()};
         cstone::findNeighbors(x, y, z, h, 0, cstone::LocalIndex(n), box, view, ngmax, nbr, count);
         return 0;
+    }
+
+    //! @brief leaf counts of sorted keys in a cornerstone tree (computeNodeCounts, csarray.hpp:181-235)
+    void ref_leaf_counts(const uint64_t* leaves, size_t numLeaves, const uint64_t* keys, size_t n, unsigned* counts)
+    {
+        cstone::computeNodeCounts(leaves, counts, cstone::TreeNodeIndex(numLeaves), std::span<const uint64_t>(keys, n),
+                                  std::numeric_limits<unsigned>::max(), false);
+    }
+
+    /*! @brief one rebalance step on given counts (rebalanceDecision + rebalanceTree, csarray.hpp:309-389);
+     *  returns the new leaf count (newLeaves receives it + 1 keys if it fits), *converged = rebalanceDecision's result */
+    size_t ref_rebalance_tree(const uint64_t* leaves, size_t numLeaves, const unsigned* counts, unsigned bucket,
+                              uint64_t* newLeaves, size_t capacity, int* converged)
+    {
+        std::vector<uint64_t> tree(leaves, leaves + numLeaves + 1), newTree;
+        std::vector<cstone::TreeNodeIndex> ops(numLeaves + 1);
+        *converged = cstone::rebalanceDecision(tree.data(), counts, cstone::TreeNodeIndex(numLeaves), bucket,
+                                               ops.data());
+        cstone::rebalanceTree(tree, newTree, ops.data());
+        size_t nl = newTree.size() - 1;
+        if (nl + 1 <= capacity) { std::copy(newTree.begin(), newTree.end(), newLeaves); }
+        return nl;
+    }
+
+    /*! @brief halo flags per leaf of the rank owning leaves [firstNode, lastNode) of a cornerstone tree, as
+     *  FocusedOctree::discoverHalos computes them on the CPU (octree_focus_mpi.hpp:556-569): leaf search boxes by
+     *  computeBoundingBox started at the leaf centres, then findHalos over the linked octree; the node flags are read
+     *  per leaf through leafToInternal as computeNodeLayout does (layout.hpp:151-177). h is double, or float when hf
+     *  is given. layout: numAssigned + 1 particle offsets. */
+    void ref_find_halos(const uint64_t* leaves, size_t numLeaves, const double* x, const double* y, const double* z,
+                        const double* h, const float* hf, const unsigned* layout, int firstNode, int lastNode,
+                        const double* lim, int periodic, float searchExt, uint8_t* leafFlags)
+    {
+        auto box = mkBox(lim, periodic);
+        std::vector<uint64_t> tree(leaves, leaves + numLeaves + 1);
+        cstone::OctreeData<uint64_t, CpuTag> octree;
+        octree.resize(cstone::nNodes(tree));
+        cstone::updateInternalTree<uint64_t>(tree, octree.data());
+        int nn = octree.numNodes;
+        std::vector<cstone::Vec3<double>> centers(nn), sizes(nn);
+        cstone::nodeFpCenters<uint64_t>(octree.prefixes, centers.data(), sizes.data(), box);
+        const int* l2i = octree.leafToInternal.data() + octree.numInternalNodes;
+        std::vector<cstone::Vec3<double>> searchCenters(numLeaves), searchSizes(numLeaves);
+        for (size_t l = 0; l < numLeaves; ++l)
+        {
+            searchCenters[l] = centers[l2i[l]];
+        }
+        for (int leaf = firstNode; leaf < lastNode; ++leaf)
+        {
+            int i = leaf - firstNode;
+            if (hf)
+            {
+                std::tie(searchCenters[leaf], searchSizes[leaf]) = cstone::computeBoundingBox(
+                    x, y, z, hf, layout[i], layout[i + 1], float(2 * searchExt), searchCenters[leaf]);
+            }
+            else
+            {
+                std::tie(searchCenters[leaf], searchSizes[leaf]) = cstone::computeBoundingBox(
+                    x, y, z, h, layout[i], layout[i + 1], double(2 * searchExt), searchCenters[leaf]);
+            }
+        }
+        std::vector<uint8_t> flags(nn, 0);
+        cstone::findHalos(octree.prefixes.data(), octree.childOffsets.data(), octree.parents.data(), centers.data(),
+                          sizes.data(), tree.data(), searchCenters.data(), searchSizes.data(), box, firstNode,
+                          lastNode, flags.data());
+        for (size_t l = 0; l < numLeaves; ++l)
+        {
+            leafFlags[l] = flags[l2i[l]];
+        }
+    }
+
+    /*! @brief the SFC assignment of numRanks ranks on a global tree (makeSfcAssignment, domaindecomp.hpp:112-127):
+     *  rank boundary keys (numRanks + 1), first leaf of every rank (numRanks + 1) and particles per rank */
+    void ref_sfc_assignment(int numRanks, const unsigned* counts, size_t numLeaves, const uint64_t* leaves,
+                            uint64_t* boundaries, int* treeOffsets, unsigned* rankCounts)
+    {
+        std::vector<unsigned> c(counts, counts + numLeaves);
+        auto a = cstone::makeSfcAssignment(numRanks, c, leaves);
+        for (int r = 0; r <= numRanks; ++r)
+        {
+            boundaries[r]  = a[r];
+            treeOffsets[r] = a.treeOffsetsConst()[r];
+            if (r < numRanks) { rankCounts[r] = a.totalCount(r); }
+        }
     }
 }

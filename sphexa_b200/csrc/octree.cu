@@ -831,3 +831,54 @@ extern "C" int sphb_build_octree(const uint64_t* leaves, size_t num_leaves, uint
     std::memcpy(level_range, t.levelRange, sizeof(t.levelRange));
     return SPHB_OK;
 }
+
+// ------------------------------------------------------------------------------------------------------------------
+// One step of the multi-rank global tree: the caller sums the leaf counts of every rank between the steps
+// (cstone::updateOctreeGlobal, cstone/tree/update_mpi.hpp:64-99)
+// ------------------------------------------------------------------------------------------------------------------
+
+extern "C" int sphb_leaf_counts(const uint64_t* leaves, size_t num_leaves, const uint64_t* sorted_keys, size_t n,
+                                uint32_t* counts, void* stream)
+{
+    using namespace sphb;
+    if (!leaves || !counts || num_leaves == 0 || num_leaves >= (size_t(1) << 30) || (n && !sorted_keys))
+    {
+        return SPHB_ERR_ARG;
+    }
+    return computeLeafCounts(leaves, int(num_leaves), sorted_keys, n, counts, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int sphb_rebalance_tree(const uint64_t* leaves, size_t num_leaves, const uint32_t* counts, unsigned bucket,
+                                   uint64_t* new_leaves, size_t capacity, size_t* num_new, int* converged,
+                                   void* stream)
+{
+    using namespace sphb;
+    if (!leaves || !counts || !new_leaves || !num_new || !converged || bucket == 0 || num_leaves == 0 ||
+        num_leaves >= (size_t(1) << 30) || new_leaves == leaves)
+    {
+        return SPHB_ERR_ARG;
+    }
+    auto st = static_cast<cudaStream_t>(stream);
+    int L   = int(num_leaves);
+    TreeScratch s;
+    SPHB_TRY(s.ints.reserve(L + 2));
+    SPHB_TRY(s.scanTmp.reserve(scanTempInts(L + 1) + 1));
+    SPHB_TRY(s.flags.reserve(1));
+    SPHB_CUDA_TRY(cudaMemsetAsync(s.flags.data(), 0, sizeof(unsigned), st));
+    csNodeOpsKernel<<<ceilDiv(L + 1, 256), 256, 0, st>>>(leaves, counts, L, bucket, s.ints.data(), s.flags.data());
+    countLaunch();
+    SPHB_TRY(exclusiveScan(s.ints.data(), s.ints.data(), L + 1, s.scanTmp.data(), st));
+    int newL       = 0;
+    unsigned anyOp = 0;
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&newL, s.ints.data() + L, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&anyOp, s.flags.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    *num_new   = size_t(newL);
+    *converged = anyOp ? 0 : 1;
+    if (size_t(newL) + 1 > capacity) { return SPHB_ERR_CAPACITY; }
+    rebalanceKernel<<<ceilDiv(L + 1, 256), 256, 0, st>>>(leaves, L, s.ints.data(), new_leaves);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    return SPHB_OK;
+}

@@ -94,7 +94,7 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_dataset_xmass", "sphb_dataset_ve_def_gradh", "sphb_ideal_gas_eos",
             "sphb_dataset_iad_divv_curlv", "sphb_dataset_av_switches", "sphb_dataset_momentum_energy",
             "sphb_dataset_positions", "sphb_dataset_update_h", "sphb_compute_group_splits",
-            "sphb_build_octree")
+            "sphb_build_octree", "sphb_leaf_counts", "sphb_rebalance_tree", "sphb_find_halos")
 
 _lib = None
 
@@ -184,6 +184,9 @@ def load() -> C.CDLL:
         "sphb_compute_group_splits": (C.c_int, [S, S, P, P, P, P, C.c_int, P, S, P, C.POINTER(Box), C.c_uint,
                                                 C.c_float, P, S, C.POINTER(S), P]),
         "sphb_build_octree": (C.c_int, [P, S, P, P, P, P, P, P, P]),
+        "sphb_leaf_counts": (C.c_int, [P, S, P, S, P, P]),
+        "sphb_rebalance_tree": (C.c_int, [P, S, P, C.c_uint, P, S, C.POINTER(S), C.POINTER(C.c_int), P]),
+        "sphb_find_halos": (C.c_int, [P, S, P, P, P, P, C.c_int, P, S, S, C.POINTER(Box), C.c_float, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
