@@ -53,7 +53,7 @@ def ref_rebalance_tree(leaves: np.ndarray, counts: np.ndarray, bucket: int):
     """(new leaves, converged) of one rebalance step"""
     lv = np.ascontiguousarray(leaves, dtype=np.uint64)
     c = np.ascontiguousarray(counts, dtype=np.uint32)
-    cap = 8 * (lv.size + 8) * 8
+    cap = 4096 * lv.size + 8  # a leaf splits into at most 8^4 leaves per step
     out = np.zeros(cap + 1, dtype=np.uint64)
     conv = C.c_int()
     nl = _lib().ref_rebalance_tree(_p(lv), lv.size - 1, _p(c), bucket, _p(out), cap, C.byref(conv))

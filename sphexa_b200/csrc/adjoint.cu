@@ -153,6 +153,10 @@ __device__ __forceinline__ void loadC(const ChainArrays<T>& a, size_t i, T (&c)[
     }
 }
 
+//! 1 / x: IEEE in FP64, the fast approximate division in FP32
+__device__ __forceinline__ double recipT(double x) { return 1.0 / x; }
+__device__ __forceinline__ float recipT(float x) { return __fdividef(1.0f, x); }
+
 //! scatter the adjoint of a neighbour's position (the pair separation is x_i - x_j)
 template<class T>
 __device__ __forceinline__ void scatterPos(const AdjArrays<T>& g, uint32_t j, const V3<T>& rb)
@@ -271,6 +275,8 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
     const T hi = T(hiD), mi = T(pi.m), cI = hr.c, kxi = a.kx[t.i], alphaI = gr.alpha, xmassi = hr.xm;
     const T rhoi = kxi * mi / xmassi, prhoi = hr.prho;
     const T hiInv = T(1) / hi, hiInv3 = hiInv * hiInv * hiInv;
+    // reciprocals and logarithms reused by every pair (FP32: fast division, no IEEE slow path in the pair loop)
+    const T invRhoi = recipT(rhoi), invXmi = recipT(xmassi);
 
     const V3<T> momB = {-k.K * g.ax[t.i], -k.K * g.ay[t.i], -k.K * g.az[t.i]};
     const T duB      = g.du[t.i];
@@ -287,15 +293,28 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
         uint32_t js[kNbChunk];
         loadChunk(a.nidx, t, t.ngPad, q0, js);
         unsigned qn = min(kNbChunk, t.count - q0);
+        // one pair per iteration: unrolled over the chunk, the pair body overflowed the instruction cache
+#pragma unroll 1
         for (unsigned q = 0; q < qn; ++q)
         {
-            uint32_t j     = js[q];
+            uint32_t j     = popChunk(js);
             Pos<T> pj      = posOf(a, j);
             HydroRec<T> hj = loadHydro(a.hrec + j);
             GradRec<T> gj  = loadGrad(a.grec + j);
             const T cj6[6] = {gj.c11, gj.c12, gj.c13, gj.c22, gj.c23, gj.c33};
             V3<T> r        = sepV(separation(pi, pj, 2.0 * hiD, box, k));
-            T dist         = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+            T r2           = r.x * r.x + r.y * r.y + r.z * r.z;
+            T rinv, dist;
+            if constexpr (sizeof(T) == 4)
+            {
+                rinv = rsqrtf(r2);
+                dist = r2 * rinv;
+            }
+            else
+            {
+                dist = sqrt(r2);
+                rinv = T(1) / dist;
+            }
             V3<T> vij      = {hr.vx - hj.vx, hr.vy - hj.vy, hr.vz - hj.vz};
             T v1 = dist * hiInv, v2 = dist * hj.hInv;
             T hjInv3 = hj.hInv * hj.hInv * hj.hInv;
@@ -308,9 +327,10 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             V3<T> tAj = {-crj.x * Wj, -crj.y * Wj, -crj.z * Wj};
 
             T mj = T(pj.m), cj = hj.c, xmassj = hj.xm;
-            T rhoj = fdiv(mj, hj.vol);
-            T rv   = dot3(r, vij);
-            T wij  = fdiv(rv, dist);
+            T rhoj    = fdiv(mj, hj.vol);
+            T invRhoj = fdiv(hj.vol, mj);
+            T rv      = dot3(r, vij);
+            T wij     = rv * rinv;
             T visc = T(0), vijSignal = T(0);
             if (wij < T(0))
             {
@@ -319,7 +339,8 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             }
             T aMom, bMom, sigma = T(0);
             int branch;
-            T atwood = fdiv(fabs(rhoi - rhoj), rhoi + rhoj);
+            // FP32 decides the branch without the division and needs the Atwood number only on the ramp
+            T atwood = sizeof(T) == 4 ? T(0) : fdiv(fabs(rhoi - rhoj), rhoi + rhoj);
             // the forward's branch decision: FP32 compares the thresholds without the division
             bool belowMin = sizeof(T) == 4 ? fabs(rhoi - rhoj) < k.Atmin * (rhoi + rhoj) : atwood < k.Atmin;
             bool aboveMax = sizeof(T) == 4 ? fabs(rhoi - rhoj) > k.Atmax * (rhoi + rhoj) : atwood > k.Atmax;
@@ -337,13 +358,23 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             }
             else
             {
-                sigma  = k.ramp * (atwood - k.Atmin);
-                aMom   = pow(xmassi, T(2) - sigma) * pow(xmassj, sigma);
-                bMom   = pow(xmassj, T(2) - sigma) * pow(xmassi, sigma);
+                if constexpr (sizeof(T) == 4) { atwood = fdiv(fabs(rhoi - rhoj), rhoi + rhoj); }
+                sigma = k.ramp * (atwood - k.Atmin);
+                if constexpr (sizeof(T) == 4)
+                {
+                    T li = log2f(xmassi), lj = log2f(xmassj);
+                    aMom = exp2f((T(2) - sigma) * li + sigma * lj);
+                    bMom = exp2f((T(2) - sigma) * lj + sigma * li);
+                }
+                else
+                {
+                    aMom = pow(xmassi, T(2) - sigma) * pow(xmassj, sigma);
+                    bMom = pow(xmassj, T(2) - sigma) * pow(xmassi, sigma);
+                }
                 branch = 2;
             }
-            T aVisc = fdiv(mj, rhoi) * visc;
-            T bVisc = fdiv(mj, rhoj) * visc;
+            T aVisc = mj * invRhoi * visc;
+            T bVisc = mj * invRhoj * visc;
             V3<T> aViscV = {T(0.5) * (aVisc * tAi.x + bVisc * tAj.x), T(0.5) * (aVisc * tAi.y + bVisc * tAj.y),
                             T(0.5) * (aVisc * tAi.z + bVisc * tAj.z)};
             T momI = mj * prhoi * aMom;
@@ -367,9 +398,9 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             T bMomB = momJB * mj * hj.prho;
             prhoiB += momIB * mj * aMom;
             T prhojB = momJB * mj * bMom;
-            T viscB  = aViscB * mj / rhoi + bViscB * mj / rhoj;
-            rhoiB -= aViscB * aVisc / rhoi;
-            T rhojB = -bViscB * bVisc / rhoj;
+            T viscB  = aViscB * mj * invRhoi + bViscB * mj * invRhoj;
+            rhoiB -= aViscB * aVisc * invRhoi;
+            T rhojB = -bViscB * bVisc * invRhoj;
             T wijB = T(0), alphajB = T(0), cjB = T(0);
             if (wij < T(0))
             {
@@ -396,19 +427,21 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             }
             else
             {
-                xmiB += aMomB * (T(2) - sigma) * aMom / xmassi + bMomB * sigma * bMom / xmassi;
-                xmjB      = aMomB * sigma * aMom / xmassj + bMomB * (T(2) - sigma) * bMom / xmassj;
+                T invXmj  = recipT(xmassj);
+                xmiB += (aMomB * (T(2) - sigma) * aMom + bMomB * sigma * bMom) * invXmi;
+                xmjB      = (aMomB * sigma * aMom + bMomB * (T(2) - sigma) * bMom) * invXmj;
                 T lnr     = log(xmassj) - log(xmassi);
                 T sigmaB  = (aMomB * aMom - bMomB * bMom) * lnr;
                 T atB     = sigmaB * k.ramp;
                 T D       = rhoi + rhoj;
                 T sgn     = rhoi > rhoj ? T(1) : T(-1);
-                rhoiB += atB * (sgn - atwood) / D;
-                rhojB += atB * (-sgn - atwood) / D;
+                T invD = recipT(D);
+                rhoiB += atB * (sgn - atwood) * invD;
+                rhojB += atB * (-sgn - atwood) * invD;
             }
             // wij = rv / dist, rv = r . vij
-            T rvB   = wijB / dist;
-            T distB = -wijB * wij / dist;
+            T rvB   = wijB * rinv;
+            T distB = -wijB * wij * rinv;
             V3<T> rB = {rvB * vij.x, rvB * vij.y, rvB * vij.z};
             vijB.x += rvB * r.x;
             vijB.y += rvB * r.y;
@@ -436,7 +469,7 @@ __global__ void __launch_bounds__(kChainThreads) momentumEnergyVjpKernel(ChainAr
             distB += v2B * hj.hInv;
             if (dist > T(0))
             {
-                T f = distB / dist;
+                T f = distB * rinv;
                 rB.x += f * r.x;
                 rB.y += f * r.y;
                 rB.z += f * r.z;
@@ -710,9 +743,11 @@ __global__ void __launch_bounds__(kChainThreads) divvVjpKernel(ChainArrays<T> a,
         uint32_t js[kNbChunk];
         loadChunk(a.nidx, t, t.ngPad, q0, js);
         unsigned qn = min(kNbChunk, t.count - q0);
+        // one pair per iteration: the chunk stays in registers and the loop body is not replicated
+#pragma unroll 1
         for (unsigned q = 0; q < qn; ++q)
         {
-            uint32_t j     = js[q];
+            uint32_t j     = popChunk(js);
             Pos<T> pj      = posOf(a, j);
             HydroRec<T> hj = loadHydro(a.hrec + j);
             V3<T> r        = sepV(separation(pi, pj, 2.0 * hiD, box, k));
@@ -822,9 +857,11 @@ __global__ void __launch_bounds__(kChainThreads) iadVjpKernel(ChainArrays<T> a, 
         uint32_t js[kNbChunk];
         loadChunk(a.nidx, t, t.ngPad, q0, js);
         unsigned qn = min(kNbChunk, t.count - q0);
+        // one pair per iteration: the chunk stays in registers and the loop body is not replicated
+#pragma unroll 1
         for (unsigned q = 0; q < qn; ++q)
         {
-            uint32_t j     = js[q];
+            uint32_t j     = popChunk(js);
             Pos<T> pj      = posOf(a, j);
             HydroRec<T> hj = loadHydro(a.hrec + j);
             V3<T> r        = sepV(separation(pi, pj, 2.0 * hiD, box, k));
@@ -929,9 +966,11 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhVjpKernel(ChainArrays
         uint32_t js[kNbChunk];
         loadChunk(a.nidx, t, t.ngPad, q0, js);
         unsigned qn = min(kNbChunk, t.count - q0);
+        // one pair per iteration: the chunk stays in registers and the loop body is not replicated
+#pragma unroll 1
         for (unsigned q = 0; q < qn; ++q)
         {
-            uint32_t j = js[q];
+            uint32_t j = popChunk(js);
             Pos<T> pj  = posOf(a, j);
             V3<T> r    = sepV(separation(pi, pj, 2.0 * hiD, box, k));
             T dist     = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
@@ -989,9 +1028,11 @@ __global__ void __launch_bounds__(kChainThreads) xmassVjpKernel(ChainArrays<T> a
         uint32_t js[kNbChunk];
         loadChunk(a.nidx, t, t.ngPad, q0, js);
         unsigned qn = min(kNbChunk, t.count - q0);
+        // one pair per iteration: the chunk stays in registers and the loop body is not replicated
+#pragma unroll 1
         for (unsigned q = 0; q < qn; ++q)
         {
-            uint32_t j = js[q];
+            uint32_t j = popChunk(js);
             Pos<T> pj  = posOf(a, j);
             V3<T> r    = sepV(separation(pi, pj, 2.0 * hiD, box, k));
             T dist     = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);

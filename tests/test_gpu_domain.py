@@ -66,11 +66,17 @@ def test_tree_steps_over_summed_counts(lib):
             assert np.array_equal(got, od.ref_leaf_counts(leaves, rank_keys[r]))
             total += got
         cap = 8 * leaves.size + 8
-        out = torch.zeros(cap + 1, dtype=torch.int64, device="cuda")
         num, conv = C.c_size_t(), C.c_int()
         dc = _dev(total.view(np.int32), torch)
-        L.check(lib.sphb_rebalance_tree(L.ptr(dl), leaves.size - 1, L.ptr(dc), 16, L.ptr(out), cap, C.byref(num),
-                                        C.byref(conv), None), "rebalance")
+        while True:
+            out = torch.zeros(cap + 1, dtype=torch.int64, device="cuda")
+            rc = lib.sphb_rebalance_tree(L.ptr(dl), leaves.size - 1, L.ptr(dc), 16, L.ptr(out), cap, C.byref(num),
+                                         C.byref(conv), None)
+            if rc != L.SPHB_ERR_CAPACITY:
+                break
+            assert num.value + 1 > cap
+            cap = num.value + 1
+        L.check(rc, "rebalance")
         ref_new, ref_conv = od.ref_rebalance_tree(leaves, total, 16)
         new = out.cpu().numpy().view(np.uint64)[:num.value + 1]
         assert bool(conv.value) == ref_conv
