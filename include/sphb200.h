@@ -539,8 +539,9 @@ void* sphb_ensemble_stream(sphb_ensemble* ens);
 /* 5. Measurement helper                                                                                            */
 /* ---------------------------------------------------------------------------------------------------------------- */
 
-/*! Measure the CUDA-core FMA throughput of the current device: which = 0 for FP32, 1 for FP64. Runs a short
- *  register-resident FMA kernel over all SMs and returns the achieved TFLOP/s (2 flops per FMA) in *tflops.
+/*! Measure the CUDA-core FMA throughput of the current device: which = 0 for FP32, 1 for FP64, 2 for packed FP32
+ *  (two FP32 FMAs per instruction, sm_100 FFMA2). Runs a short register-resident FMA kernel over all SMs and returns
+ *  the achieved TFLOP/s (2 flops per FMA) in *tflops.
  *  No counterpart in the reference: it supplies the roofline denominator of the FP32/FP64-bound neighbour sums. */
 int sphb_probe_fma_peak(int which, double* tflops);
 

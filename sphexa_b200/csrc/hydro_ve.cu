@@ -76,6 +76,7 @@ __global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArr
     T xmassi   = a.xm[t.i];
     T hInv     = T(1) / hi;
     T h3Inv    = hInv * hInv * hInv;
+    [[maybe_unused]] float hhV = 0.5f * float(hInv) * float(hInv);
 
     BlockSum<T> kxS(xmassi), whomegaS(-T(3) * xmassi), wrho0S(-T(3) * mi);
     for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
@@ -91,12 +92,38 @@ __global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArr
             Pos<T> pj  = posOf(a, j);
             Sep<T> r   = separation(pi, pj, 2.0 * hiD, box, k);
             T r2       = r.rx * r.rx + r.ry * r.ry + r.rz * r.rz;
-            // FP32: r from one rsqrt; FP64: the reference's square root
-            T dist     = sizeof(T) == 4 ? T(r2 * rsqrtf(float(r2))) : T(sqrt(r2));
-            T vloc     = dist * hInv;
-            T w        = kernelW(a.wh, k, vloc);
-            T dw       = kernelDW(a.whd, k, vloc);
-            T dterh    = -(T(3) * w + vloc * dw);
+            T w, dterh;
+            if constexpr (sizeof(T) == 4)
+            {
+                if (k.usePoly)
+                {
+                    // t = v^2/2 - 1 from r2 (no square root); W and dW's polynomial side by side in packed FP32
+                    // (sm_100 FFMA2); v dW = v^2 P'(t) = 2 (t + 1) P'(t) (0.638 -> 0.624 ms at 128^3)
+                    float tt   = fmaf(r2, hhV, -1.0f);
+                    float2 acc = make_float2(k.wpoly[kPolyTerms - 1], k.dwpoly[kPolyTerms - 1]);
+#pragma unroll
+                    for (int p = kPolyTerms - 2; p >= 0; --p)
+                    {
+                        acc = __ffma2_rn(acc, make_float2(tt, tt), make_float2(k.wpoly[p], k.dwpoly[p]));
+                    }
+                    bool in = tt < 1.0f;
+                    w       = in ? acc.x : 0.0f;
+                    dterh   = in ? -(3.0f * acc.x + 2.0f * (tt + 1.0f) * acc.y) : 0.0f;
+                }
+                else
+                {
+                    T vloc = T(r2 * rsqrtf(float(r2))) * hInv;
+                    w      = kernelW(a.wh, k, vloc);
+                    dterh  = -(T(3) * w + vloc * kernelDW(a.whd, k, vloc));
+                }
+            }
+            else
+            {
+                T vloc = T(sqrt(r2)) * hInv;
+                w      = kernelW(a.wh, k, vloc);
+                T dw   = kernelDW(a.whd, k, vloc);
+                dterh  = -(T(3) * w + vloc * dw);
+            }
             T xmassj   = __ldg(a.xm + j);
             kxS.add(w * xmassj);
             whomegaS.add(dterh * xmassj);
@@ -589,6 +616,8 @@ __global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode &
         T kxi         = a.kx[t.i];
         T alphaI      = gr.alpha;
         T xmassi      = hr.xm;
+        // FP32: log2 xm_i for the Atwood ramp's xm_i^(2-s) xm_j^s = exp2((2-s) log2 xm_i + s log2 xm_j)
+        T lxi         = sizeof(T) == 4 ? T(log2f(float(xmassi))) : T(0);
         T rhoi        = kxi * mi / xmassi;
         T invRhoi     = T(1) / rhoi;
         T prhoi       = hr.prho;
@@ -606,101 +635,197 @@ __global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode &
 
         // the term of one neighbour j, added to the five sums
         auto pairTerm = [&](uint32_t j) {
-            Pos<T> pj      = posOf(a, j);
-            HydroRec<T> hj = loadHydro(a.hrec + j);
-            GradRec<T> gj  = loadGrad(a.grec + j);
-            Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
-            T r2           = r.rx * r.rx + r.ry * r.ry + r.rz * r.rz;
-            // FP32: 1/r from one rsqrt (r and w_ij = r.v / r without a square root or a division), m_j / rho_j as
-            // vol_j, and the Atwood thresholds compared without a division (1.68 -> 1.58 ms at 128^3; the errors
-            // against FP64 unchanged)
-            T rinv, dist;
-            if constexpr (sizeof(T) == 4)
+            if constexpr (sizeof(T) == 4 && !(kMode & kModeAvClean))
             {
-                rinv = rsqrtf(r2);
-                dist = r2 * rinv;
-            }
-            else { dist = sqrt(r2); }
-            T vxij         = hr.vx - hj.vx;
-            T vyij         = hr.vy - hj.vy;
-            T vzij         = hr.vz - hj.vz;
-            T v1           = dist * hiInv;
-            T v2           = dist * hj.hInv;
-            T hjInv3       = hj.hInv * hj.hInv * hj.hInv;
-            T Wi           = hiInv3 * kernelW(a.wh, k, v1);
-            T Wj           = hjInv3 * kernelW(a.wh, k, v2);
+                // FP32: the i and j halves of the pair side by side in packed FP32 (sm_100 FFMA2/FMUL2): the IAD
+                // gradients tA = -(C r) W, their products with v_ij and the momentum coefficients. The viscous
+                // term joins the momentum sums as (m_j prho_i a_mom + aVisc/2) tA_i + (m_j prho_j b_mom + bVisc/2)
+                // tA_j (1.54 -> 1.48 ms at 128^3; the errors against FP64 unchanged)
+                Pos<T> pj      = posOf(a, j);
+                HydroRec<T> hj = loadHydro(a.hrec + j);
+                GradRec<T> gj  = loadGrad(a.grec + j);
+                Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+                float r2       = r.rx * r.rx + r.ry * r.ry + r.rz * r.rz;
+                float rinv     = rsqrtf(r2);
+                float dist     = r2 * rinv;
+                float vxij     = hr.vx - hj.vx;
+                float vyij     = hr.vy - hj.vy;
+                float vzij     = hr.vz - hj.vz;
 
-            T tA1i = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
-            T tA2i = -(gr.c12 * r.rx + gr.c22 * r.ry + gr.c23 * r.rz) * Wi;
-            T tA3i = -(gr.c13 * r.rx + gr.c23 * r.ry + gr.c33 * r.rz) * Wi;
-            T tA1j = -(gj.c11 * r.rx + gj.c12 * r.ry + gj.c13 * r.rz) * Wj;
-            T tA2j = -(gj.c12 * r.rx + gj.c22 * r.ry + gj.c23 * r.rz) * Wj;
-            T tA3j = -(gj.c13 * r.rx + gj.c23 * r.ry + gj.c33 * r.rz) * Wj;
+                float v1 = dist * hiInv, v2 = dist * hj.hInv;
+                float hjInv3 = hj.hInv * hj.hInv * hj.hInv;
+                float2 W = make_float2(-hiInv3 * kernelW(a.wh, k, v1), -hjInv3 * kernelW(a.wh, k, v2));
 
-            T mj     = T(pj.m);
-            T cj     = hj.c;
-            T xmassj = hj.xm;
-            T rhoj   = fdiv(mj, hj.vol);
+                // tA = -(C r) W of i and j side by side
+                float2 RX  = make_float2(r.rx, r.rx), RY = make_float2(r.ry, r.ry), RZ = make_float2(r.rz, r.rz);
+                float2 tA1 = __ffma2_rn(make_float2(gr.c13, gj.c13), RZ,
+                                        __ffma2_rn(make_float2(gr.c12, gj.c12), RY,
+                                                   __fmul2_rn(make_float2(gr.c11, gj.c11), RX)));
+                float2 tA2 = __ffma2_rn(make_float2(gr.c23, gj.c23), RZ,
+                                        __ffma2_rn(make_float2(gr.c22, gj.c22), RY,
+                                                   __fmul2_rn(make_float2(gr.c12, gj.c12), RX)));
+                float2 tA3 = __ffma2_rn(make_float2(gr.c33, gj.c33), RZ,
+                                        __ffma2_rn(make_float2(gr.c23, gj.c23), RY,
+                                                   __fmul2_rn(make_float2(gr.c13, gj.c13), RX)));
+                tA1 = __fmul2_rn(tA1, W);
+                tA2 = __fmul2_rn(tA2, W);
+                tA3 = __fmul2_rn(tA3, W);
 
-            T rv   = r.rx * vxij + r.ry * vyij + r.rz * vzij;
-            if constexpr (kMode & kModeAvClean)
-            {
-                T gradVj[6];
-                loadDV(a.dvrec + j, gradVj);
-                rv += avRvCorrection(r.rx, r.ry, r.rz, v1 < v2 ? v1 : v2, etaCrit, gradVi, gradVj);
-            }
-            T wij;
-            if constexpr (sizeof(T) == 4) { wij = rv * rinv; }
-            else { wij = fdiv(rv, dist); }
-            T visc = T(0);
-            if (wij < T(0))
-            {
-                T vijSignal = (alphaI + gj.alpha) * T(0.25) * (ci + cj) - T(2) * wij;
-                visc        = -vijSignal * wij;
-            }
-            T vijsignal = T(0.5) * (ci + cj) - T(2) * wij;
-            maxvsignalI = vijsignal > maxvsignalI ? vijsignal : maxvsignalI;
+                float mj     = float(pj.m);
+                float cj     = hj.c;
+                float xmassj = hj.xm;
+                float rhoj   = fdiv(mj, hj.vol);
+                float rv     = r.rx * vxij + r.ry * vyij + r.rz * vzij;
+                float wij    = rv * rinv;
+                float visc   = 0.0f;
+                if (wij < 0.0f)
+                {
+                    float vijSignal = (alphaI + gj.alpha) * 0.25f * (ci + cj) - 2.0f * wij;
+                    visc            = -vijSignal * wij;
+                }
+                float vijsignal = 0.5f * (ci + cj) - 2.0f * wij;
+                maxvsignalI     = vijsignal > maxvsignalI ? vijsignal : maxvsignalI;
 
-            T aMom, bMom;
-            T dRho = fabs(rhoi - rhoj), sRho = rhoi + rhoj;
-            if (sizeof(T) == 4 ? dRho < k.Atmin * sRho : fdiv(dRho, sRho) < k.Atmin)
-            {
-                aMom = xmassi * xmassi;
-                bMom = xmassj * xmassj;
-            }
-            else if (sizeof(T) == 4 ? dRho > k.Atmax * sRho : fdiv(dRho, sRho) > k.Atmax)
-            {
-                aMom = xmassi * xmassj;
-                bMom = aMom;
+                float aMom, bMom;
+                float dRho = fabsf(rhoi - rhoj), sRho = rhoi + rhoj;
+                if (dRho < k.Atmin * sRho)
+                {
+                    aMom = xmassi * xmassi;
+                    bMom = xmassj * xmassj;
+                }
+                else if (dRho > k.Atmax * sRho)
+                {
+                    aMom = xmassi * xmassj;
+                    bMom = aMom;
+                }
+                else
+                {
+                    float sigma = k.ramp * (fdiv(dRho, sRho) - k.Atmin);
+                    float lxj   = log2f(xmassj);
+                    aMom        = exp2f((2.0f - sigma) * lxi + sigma * lxj);
+                    bMom        = exp2f((2.0f - sigma) * lxj + sigma * lxi);
+                }
+                float aVisc = mj * invRhoi * visc;
+                float bVisc = hj.vol * visc;
+                // (tA_i . v_ij, tA_j . v_ij)
+                float2 dv = __ffma2_rn(tA3, make_float2(vzij, vzij),
+                                       __ffma2_rn(tA2, make_float2(vyij, vyij),
+                                                  __fmul2_rn(tA1, make_float2(vxij, vxij))));
+                aViscE.add(0.5f * (aVisc * dv.x + bVisc * dv.y));
+                energyS.add(mj * aMom * dv.x);
+                float cI = mj * prhoi * aMom + 0.5f * aVisc;
+                float cJ = mj * hj.prho * bMom + 0.5f * bVisc;
+                momX.add(cI * tA1.x + cJ * tA1.y);
+                momY.add(cI * tA2.x + cJ * tA2.y);
+                momZ.add(cI * tA3.x + cJ * tA3.y);
             }
             else
             {
-                T sigma = k.ramp * (fdiv(dRho, sRho) - k.Atmin);
-                aMom    = pow(xmassi, T(2) - sigma) * pow(xmassj, sigma);
-                bMom    = pow(xmassj, T(2) - sigma) * pow(xmassi, sigma);
-            }
+                Pos<T> pj      = posOf(a, j);
+                HydroRec<T> hj = loadHydro(a.hrec + j);
+                GradRec<T> gj  = loadGrad(a.grec + j);
+                Sep<T> r       = separation(pi, pj, 2.0 * hiD, box, k);
+                T r2           = r.rx * r.rx + r.ry * r.ry + r.rz * r.rz;
+                // FP32: 1/r from one rsqrt (r and w_ij = r.v / r without a square root or a division), m_j / rho_j as
+                // vol_j, and the Atwood thresholds compared without a division (1.68 -> 1.58 ms at 128^3; the errors
+                // against FP64 unchanged)
+                T rinv, dist;
+                if constexpr (sizeof(T) == 4)
+                {
+                    rinv = rsqrtf(r2);
+                    dist = r2 * rinv;
+                }
+                else { dist = sqrt(r2); }
+                T vxij         = hr.vx - hj.vx;
+                T vyij         = hr.vy - hj.vy;
+                T vzij         = hr.vz - hj.vz;
+                T v1           = dist * hiInv;
+                T v2           = dist * hj.hInv;
+                T hjInv3       = hj.hInv * hj.hInv * hj.hInv;
+                T Wi           = hiInv3 * kernelW(a.wh, k, v1);
+                T Wj           = hjInv3 * kernelW(a.wh, k, v2);
 
-            T aVisc, bVisc;
-            if constexpr (sizeof(T) == 4)
-            {
-                aVisc = mj * invRhoi * visc;
-                bVisc = hj.vol * visc;
+                T tA1i = -(gr.c11 * r.rx + gr.c12 * r.ry + gr.c13 * r.rz) * Wi;
+                T tA2i = -(gr.c12 * r.rx + gr.c22 * r.ry + gr.c23 * r.rz) * Wi;
+                T tA3i = -(gr.c13 * r.rx + gr.c23 * r.ry + gr.c33 * r.rz) * Wi;
+                T tA1j = -(gj.c11 * r.rx + gj.c12 * r.ry + gj.c13 * r.rz) * Wj;
+                T tA2j = -(gj.c12 * r.rx + gj.c22 * r.ry + gj.c23 * r.rz) * Wj;
+                T tA3j = -(gj.c13 * r.rx + gj.c23 * r.ry + gj.c33 * r.rz) * Wj;
+
+                T mj     = T(pj.m);
+                T cj     = hj.c;
+                T xmassj = hj.xm;
+                T rhoj   = fdiv(mj, hj.vol);
+
+                T rv   = r.rx * vxij + r.ry * vyij + r.rz * vzij;
+                if constexpr (kMode & kModeAvClean)
+                {
+                    T gradVj[6];
+                    loadDV(a.dvrec + j, gradVj);
+                    rv += avRvCorrection(r.rx, r.ry, r.rz, v1 < v2 ? v1 : v2, etaCrit, gradVi, gradVj);
+                }
+                T wij;
+                if constexpr (sizeof(T) == 4) { wij = rv * rinv; }
+                else { wij = fdiv(rv, dist); }
+                T visc = T(0);
+                if (wij < T(0))
+                {
+                    T vijSignal = (alphaI + gj.alpha) * T(0.25) * (ci + cj) - T(2) * wij;
+                    visc        = -vijSignal * wij;
+                }
+                T vijsignal = T(0.5) * (ci + cj) - T(2) * wij;
+                maxvsignalI = vijsignal > maxvsignalI ? vijsignal : maxvsignalI;
+
+                T aMom, bMom;
+                T dRho = fabs(rhoi - rhoj), sRho = rhoi + rhoj;
+                if (sizeof(T) == 4 ? dRho < k.Atmin * sRho : fdiv(dRho, sRho) < k.Atmin)
+                {
+                    aMom = xmassi * xmassi;
+                    bMom = xmassj * xmassj;
+                }
+                else if (sizeof(T) == 4 ? dRho > k.Atmax * sRho : fdiv(dRho, sRho) > k.Atmax)
+                {
+                    aMom = xmassi * xmassj;
+                    bMom = aMom;
+                }
+                else
+                {
+                    T sigma = k.ramp * (fdiv(dRho, sRho) - k.Atmin);
+                    if constexpr (sizeof(T) == 4)
+                    {
+                        T lxj = log2f(xmassj);
+                        aMom  = exp2f((T(2) - sigma) * lxi + sigma * lxj);
+                        bMom  = exp2f((T(2) - sigma) * lxj + sigma * lxi);
+                    }
+                    else
+                    {
+                        aMom = pow(xmassi, T(2) - sigma) * pow(xmassj, sigma);
+                        bMom = pow(xmassj, T(2) - sigma) * pow(xmassi, sigma);
+                    }
+                }
+
+                T aVisc, bVisc;
+                if constexpr (sizeof(T) == 4)
+                {
+                    aVisc = mj * invRhoi * visc;
+                    bVisc = hj.vol * visc;
+                }
+                else
+                {
+                    aVisc = fdiv(mj, rhoi) * visc;
+                    bVisc = fdiv(mj, rhoj) * visc;
+                }
+                T aViscX = T(0.5) * (aVisc * tA1i + bVisc * tA1j);
+                T aViscY = T(0.5) * (aVisc * tA2i + bVisc * tA2j);
+                T aViscZ = T(0.5) * (aVisc * tA3i + bVisc * tA3j);
+                aViscE.add(aViscX * vxij + aViscY * vyij + aViscZ * vzij);
+                energyS.add(mj * aMom * (vxij * tA1i + vyij * tA2i + vzij * tA3i));
+                T momI = mj * prhoi * aMom;
+                T momJ = mj * hj.prho * bMom;
+                momX.add(momI * tA1i + momJ * tA1j + aViscX);
+                momY.add(momI * tA2i + momJ * tA2j + aViscY);
+                momZ.add(momI * tA3i + momJ * tA3j + aViscZ);
             }
-            else
-            {
-                aVisc = fdiv(mj, rhoi) * visc;
-                bVisc = fdiv(mj, rhoj) * visc;
-            }
-            T aViscX = T(0.5) * (aVisc * tA1i + bVisc * tA1j);
-            T aViscY = T(0.5) * (aVisc * tA2i + bVisc * tA2j);
-            T aViscZ = T(0.5) * (aVisc * tA3i + bVisc * tA3j);
-            aViscE.add(aViscX * vxij + aViscY * vyij + aViscZ * vzij);
-            energyS.add(mj * aMom * (vxij * tA1i + vyij * tA2i + vzij * tA3i));
-            T momI = mj * prhoi * aMom;
-            T momJ = mj * hj.prho * bMom;
-            momX.add(momI * tA1i + momJ * tA1j + aViscX);
-            momY.add(momI * tA2i + momJ * tA2j + aViscY);
-            momZ.add(momI * tA3i + momJ * tA3j + aViscZ);
         };
         for (unsigned q0 = 0; q0 < t.count; q0 += kNbChunk)
         {
@@ -710,7 +835,7 @@ __global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode &
             if constexpr (sizeof(T) == 4)
             {
                 // one pair per iteration: the unrolled 8-pair body overflowed the instruction cache (2.04 -> 1.71 ms
-                // at 128^3)
+                // at 128^3); unrolled by 2 or 4 it ran slower too (1.59 against 1.48 ms)
 #pragma unroll 1
                 for (unsigned q = 0; q < qn; ++q)
                 {
