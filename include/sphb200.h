@@ -369,7 +369,10 @@ int sphb_sim_store_state(sphb_sim* sim, double* const* fields, uint64_t* id, int
  *  on the device, so a Dataset with the reference's default types (a mix of float and double) passes as it is. */
 int sphb_sim_upload_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
 
-/*! sphb_sim_load_state with the caller's own element types (the fields of sphb_sim_upload_fields). */
+/*! sphb_sim_load_state with the caller's own element types (the fields of sphb_sim_upload_fields). From host memory,
+ *  the copies of temp, vx, vy, vz, x_m1, y_m1, z_m1, du_m1 and alpha may still run when the call returns: they run
+ *  beside the sync, the neighbour search and XMass of the next step, which read only x, y, z, h and m. The host
+ *  arrays must stay unchanged until the next call on the simulation returns (every call waits for the copies). */
 int sphb_sim_load_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
 
 /*! Copy fields out by name, each converted to the element type of its descriptor: any name of

@@ -108,19 +108,44 @@ const sphb_field* findDesc(const sphb_field* f, int num, const char* name)
     return nullptr;
 }
 
-//! the conserved fields and ids of a typed upload or load: into s.f[k] (FP64) and s.idAlt
-int importConserved(sphb_sim& s, const sphb_field* f, int num, bool onDevice)
+/*! the conserved fields and ids of a typed upload or load: into s.f[k] (FP64) and s.idAlt. With lateCopy (a load
+ *  from host memory), temp, v, x_m1, du_m1 and alpha go through the copy stream, after every earlier use of their
+ *  buffers on the compute stream, and the compute stream waits for them only where the step first reads them
+ *  (simimpl::waitLateFields): their transfer overlaps the sync, the search and XMass. */
+int importConserved(sphb_sim& s, const sphb_field* f, int num, bool onDevice, bool lateCopy = false)
 {
     if (!f || num <= 0) { return kErrArg; }
     for (int k = 0; k < kNumConserved; ++k)
     {
         const sphb_field* d = findDesc(f, num, kConservedNames[k]);
         if (!d || !d->data || (d->dtype != SPHB_F32 && d->dtype != SPHB_F64)) { return kErrArg; }
+    }
+    const sphb_field* idDesc = findDesc(f, num, "id");
+    if (!idDesc || !idDesc->data || idDesc->dtype != SPHB_U64) { return kErrArg; }
+    bool split = lateCopy && !onDevice && s.copyStream;
+    int numFirst = split ? int(fTemp) : int(kNumConserved);
+    for (int k = 0; k < numFirst; ++k)
+    {
+        const sphb_field* d = findDesc(f, num, kConservedNames[k]);
         SPHB_TRY(importArray(d->data, d->dtype, onDevice, s.f[k].data(), SPHB_F64, s.n, s.fAlt[k].data(), s.stream));
     }
-    const sphb_field* d = findDesc(f, num, "id");
-    if (!d || !d->data || d->dtype != SPHB_U64) { return kErrArg; }
-    return importArray(d->data, SPHB_U64, onDevice, s.idAlt.data(), SPHB_U64, s.n, nullptr, s.stream);
+    SPHB_TRY(importArray(idDesc->data, SPHB_U64, onDevice, s.idAlt.data(), SPHB_U64, s.n, nullptr, s.stream));
+    if (split)
+    {
+        // the late copies start after the early ones and the ids (and after every earlier use of their buffers):
+        // issued at once, the copy engine would interleave them and delay what the step needs first
+        SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
+        SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
+        for (int k = fTemp; k < kNumConserved; ++k)
+        {
+            const sphb_field* d = findDesc(f, num, kConservedNames[k]);
+            SPHB_TRY(importArray(d->data, d->dtype, false, s.f[k].data(), SPHB_F64, s.n, s.fAlt[k].data(),
+                                 s.copyStream));
+        }
+        SPHB_CUDA_TRY(cudaEventRecord(s.lateReady, s.copyStream));
+        s.latePending = true;
+    }
+    return kOk;
 }
 
 //! names a binding may use: every field this library keeps, plus the EOS outputs rho and p and the energy u
@@ -297,6 +322,7 @@ using namespace sphb;
 
 extern "C" int sphb_sim_upload_fields(sphb_sim* s, const sphb_field* fields, int num_fields, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s) { return SPHB_ERR_ARG; }
     SPHB_TRY(importConserved(*s, fields, num_fields, on_device != 0));
     s->id.swap(s->idAlt);
@@ -307,12 +333,14 @@ extern "C" int sphb_sim_load_fields(sphb_sim* s, const sphb_field* fields, int n
 {
     if (!s) { return SPHB_ERR_ARG; }
     if (!s->uploaded) { return SPHB_ERR_STATE; }
-    SPHB_TRY(importConserved(*s, fields, num_fields, on_device != 0));
+    SPHB_TRY(simimpl::waitLateFields(*s, true)); // a previous load's late fields, before this one's replace them
+    SPHB_TRY(importConserved(*s, fields, num_fields, on_device != 0, true));
     return simimpl::finishLoad(*s);
 }
 
 extern "C" int sphb_sim_store_fields(sphb_sim* s, const sphb_field* fields, int num_fields, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !fields || num_fields <= 0) { return SPHB_ERR_ARG; }
     for (int q = 0; q < num_fields; ++q)
     {
@@ -343,6 +371,7 @@ extern "C" int sphb_sim_store_fields(sphb_sim* s, const sphb_field* fields, int 
 
 extern "C" int sphb_sim_bind_fields(sphb_sim* s, const sphb_field* fields, int num_fields)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !fields || num_fields <= 0) { return SPHB_ERR_ARG; }
     if (s->bdt || s->p.av_clean) { return SPHB_ERR_STATE; }
     std::vector<sphb_sim::Binding> b;
@@ -359,6 +388,7 @@ extern "C" int sphb_sim_bind_fields(sphb_sim* s, const sphb_field* fields, int n
 
 extern "C" int sphb_dataset_xmass(sphb_sim* s, size_t first, size_t last, const sphb_box* box)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     if (!box) { return SPHB_ERR_ARG; }
     for (int k = 0; k < 3; ++k)
@@ -390,6 +420,7 @@ extern "C" int sphb_dataset_xmass(sphb_sim* s, size_t first, size_t last, const 
 
 extern "C" int sphb_dataset_ve_def_gradh(sphb_sim* s, size_t first, size_t last, const sphb_box* box)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     SPHB_TRY(checkBox(*s, box));
     SPHB_TRY(importBound(*s, {"xm", "temp", "vx", "vy", "vz"}));
@@ -440,6 +471,7 @@ extern "C" int sphb_ideal_gas_eos(size_t first, size_t last, double mui, double 
 
 extern "C" int sphb_dataset_iad_divv_curlv(sphb_sim* s, size_t first, size_t last, const sphb_box* box)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     SPHB_TRY(checkBox(*s, box));
     SPHB_TRY(importBound(*s, {"vx", "vy", "vz", "xm", "kx", "c", "prho"}));
@@ -452,6 +484,7 @@ extern "C" int sphb_dataset_iad_divv_curlv(sphb_sim* s, size_t first, size_t las
 
 extern "C" int sphb_dataset_av_switches(sphb_sim* s, size_t first, size_t last, const sphb_box* box, double min_dt)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     SPHB_TRY(checkBox(*s, box));
     if (!(min_dt > 0.0)) { return SPHB_ERR_ARG; }
@@ -468,6 +501,7 @@ extern "C" int sphb_dataset_av_switches(sphb_sim* s, size_t first, size_t last, 
 extern "C" int sphb_dataset_momentum_energy(sphb_sim* s, size_t first, size_t last, const sphb_box* box,
                                             float* min_dt_courant)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     SPHB_TRY(checkBox(*s, box));
     SPHB_TRY(importBound(*s, {"vx", "vy", "vz", "xm", "kx", "c", "prho", "c11", "c12", "c13", "c22", "c23", "c33",
@@ -487,6 +521,7 @@ extern "C" int sphb_dataset_momentum_energy(sphb_sim* s, size_t first, size_t la
 extern "C" int sphb_dataset_positions(sphb_sim* s, size_t first, size_t last, double dt, double dt_m1,
                                       const sphb_box* box)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     SPHB_TRY(checkBox(*s, box));
     if (!(dt > 0.0) || !(dt_m1 > 0.0)) { return SPHB_ERR_ARG; }
@@ -500,6 +535,7 @@ extern "C" int sphb_dataset_positions(sphb_sim* s, size_t first, size_t last, do
 
 extern "C" int sphb_dataset_update_h(sphb_sim* s, size_t first, size_t last, unsigned ng0)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     SPHB_TRY(boundEntry(s, first, last));
     if (ng0 == 0) { return SPHB_ERR_ARG; }
     SPHB_TRY(importBound(*s, {"nc", "h"}));

@@ -635,13 +635,14 @@ __global__ void __launch_bounds__(kChainMaxThreads, (sizeof(T) == 4 && !(kMode &
 
         // the term of one neighbour j, added to the five sums
         auto pairTerm = [&](uint32_t j) {
-            if constexpr (sizeof(T) == 4 && !(kMode & (kModeAvClean | kModeBatch)))
+            if constexpr (sizeof(T) == 4 && !(kMode & kModeAvClean))
             {
                 // FP32: the i and j halves of the pair side by side in packed FP32 (sm_100 FFMA2/FMUL2): the IAD
                 // gradients tA = -(C r) W, their products with v_ij and the momentum coefficients. The viscous
                 // term joins the momentum sums as (m_j prho_i a_mom + aVisc/2) tA_i + (m_j prho_j b_mom + bVisc/2)
-                // tA_j (1.54 -> 1.48 ms at 128^3; the errors against FP64 unchanged). Not in the ensemble's batch
-                // form: with the per-slot instance data it spills at 80 registers (4.97 against 4.84 ms unpacked)
+                // tA_j (1.54 -> 1.48 ms at 128^3; the errors against FP64 unchanged). The ensemble's batch form
+                // takes the same body, so that its members stay bit-identical to single simulations (it spills a
+                // little there: 4.97 ms per step for 64 members, against 4.84 with the scalar body)
                 Pos<T> pj      = posOf(a, j);
                 HydroRec<T> hj = loadHydro(a.hrec + j);
                 GradRec<T> gj  = loadGrad(a.grec + j);

@@ -147,6 +147,7 @@ int syncDomain(sphb_sim& s)
 
     if (!identity)
     {
+        SPHB_TRY(simimpl::waitLateFields(s));
         // reorder every conserved field and the ids into SFC order
         const void* src[kNumConserved + 2];
         void* dst[kNumConserved + 2];
@@ -370,6 +371,9 @@ int allocateSkin(sphb_sim& s)
     SPHB_CUDA_TRY(cudaStreamCreateWithPriority(&s.sideStream, cudaStreamNonBlocking, greatestPriority));
     SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.skinFork, cudaEventDisableTiming));
     SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.skinJoin, cudaEventDisableTiming));
+    SPHB_CUDA_TRY(cudaStreamCreateWithFlags(&s.copyStream, cudaStreamNonBlocking));
+    SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.copyFork, cudaEventDisableTiming));
+    SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.lateReady, cudaEventDisableTiming));
     return kOk;
 }
 
@@ -488,6 +492,8 @@ int searchNeighbors(sphb_sim& s)
 int runStage(sphb_sim& s, int stage)
 {
     cudaStream_t st = s.stream;
+    // the sync (unless it reorders), the search and XMass read only x, y, z, h and m
+    if (stage > sXMass) { SPHB_TRY(simimpl::waitLateFields(s)); }
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[stage], st));
     switch (stage)
     {
@@ -1153,6 +1159,13 @@ extern "C" int sphb_sim_destroy(sphb_sim* s)
         cudaStreamSynchronize(s->sideStream);
         cudaStreamDestroy(s->sideStream);
     }
+    if (s->copyStream)
+    {
+        cudaStreamSynchronize(s->copyStream);
+        cudaStreamDestroy(s->copyStream);
+    }
+    if (s->copyFork) { cudaEventDestroy(s->copyFork); }
+    if (s->lateReady) { cudaEventDestroy(s->lateReady); }
     if (s->skinFork) { cudaEventDestroy(s->skinFork); }
     if (s->skinJoin) { cudaEventDestroy(s->skinJoin); }
     if (s->hostMsg) { cudaFreeHost(s->hostMsg); }
@@ -1162,6 +1175,7 @@ extern "C" int sphb_sim_destroy(sphb_sim* s)
 
 extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const uint64_t* id, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !fields || !id) { return SPHB_ERR_ARG; }
     cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     for (int k = 0; k < kNumConserved; ++k)
@@ -1175,6 +1189,7 @@ extern "C" int sphb_sim_upload(sphb_sim* s, const double* const* fields, const u
 
 extern "C" int sphb_sim_initial_sync(sphb_sim* s)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s) { return SPHB_ERR_ARG; }
     if (!s->uploaded) { return SPHB_ERR_STATE; }
     s->skinValid = false;
@@ -1185,6 +1200,8 @@ extern "C" int sphb_sim_initial_sync(sphb_sim* s)
 
 extern "C" int sphb_sim_compute_forces(sphb_sim* s)
 {
+    // no wait here: the stages wait for a typed load's late fields where they first read them, and the conserved
+    // stage returns to the host after that
     if (!s) { return SPHB_ERR_ARG; }
     if (!s->uploaded || s->bdt) { return SPHB_ERR_STATE; }
     return computeForces(*s);
@@ -1192,6 +1209,7 @@ extern "C" int sphb_sim_compute_forces(sphb_sim* s)
 
 extern "C" int sphb_sim_integrate(sphb_sim* s)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s) { return SPHB_ERR_ARG; }
     if (!s->forcesDone) { return SPHB_ERR_STATE; }
     return integrateStep(*s);
@@ -1206,6 +1224,7 @@ extern "C" int sphb_sim_step(sphb_sim* s)
 
 extern "C" int sphb_sim_bdt_enable(sphb_sim* s, double eta_acc)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !(eta_acc > 0.0)) { return SPHB_ERR_ARG; }
     if (s->taping) { return SPHB_ERR_ARG; } // the adjoint has no block time-step variant
     SPHB_TRY(allocateBdt(*s));
@@ -1219,6 +1238,7 @@ extern "C" int sphb_sim_bdt_enable(sphb_sim* s, double eta_acc)
 
 extern "C" int sphb_sim_bdt_step(sphb_sim* s)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s) { return SPHB_ERR_ARG; }
     if (!s->uploaded || !s->bdt) { return SPHB_ERR_STATE; }
     SPHB_TRY(bdtComputeForces(*s));
@@ -1269,6 +1289,13 @@ extern "C" int sphb_sim_av_switches(sphb_sim* s) { return stageEntry(s, sAV); }
 
 extern "C" int sphb_sim_momentum_energy(sphb_sim* s, double* min_dt_courant)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     int rc = stageEntry(s, sMomentum);
     if (rc != SPHB_OK || !min_dt_courant) { return rc; }
     unsigned long long bits = 0;
@@ -1280,6 +1307,7 @@ extern "C" int sphb_sim_momentum_energy(sphb_sim* s, double* min_dt_courant)
 
 extern "C" int sphb_sim_conserved(sphb_sim* s, double* out)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     int rc = stageEntry(s, sConserved);
     if (rc != SPHB_OK || !out) { return rc; }
     double v[5] = {s->ecin, s->eint, s->etot, s->linmom, s->angmom};
@@ -1360,6 +1388,7 @@ bool findField(sphb_sim* s, const char* name, void** ptr, int* kind)
 
 extern "C" int sphb_sim_get_field(sphb_sim* s, const char* name, double* out, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !name || !out) { return SPHB_ERR_ARG; }
     void* ptr = nullptr;
     int kind  = 0;
@@ -1391,6 +1420,7 @@ extern "C" int sphb_sim_get_field(sphb_sim* s, const char* name, double* out, in
 
 extern "C" int sphb_sim_set_field(sphb_sim* s, const char* name, const double* in, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !name || !in) { return SPHB_ERR_ARG; }
     void* ptr = nullptr;
     int kind  = 0;
@@ -1430,6 +1460,7 @@ extern "C" int sphb_sim_set_field(sphb_sim* s, const char* name, const double* i
 
 extern "C" int sphb_sim_scalars(sphb_sim* s, double* out)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !out) { return SPHB_ERR_ARG; }
     double v[18] = {s->minDt,  s->minDt_m1,          s->minDtCourant,     s->minDtRho,  s->ttot,     s->etot,
                     s->ecin,   s->eint,              s->linmom,           s->angmom,    s->totalNeighbors,
@@ -1441,6 +1472,7 @@ extern "C" int sphb_sim_scalars(sphb_sim* s, double* out)
 
 extern "C" int sphb_sim_tree(sphb_sim* s, size_t* num_leaves, uint64_t* leaves, uint32_t* counts, uint32_t* layout)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !num_leaves) { return SPHB_ERR_ARG; }
     int L       = s->ftree.numLeaves;
     *num_leaves = size_t(L);
@@ -1461,6 +1493,7 @@ extern "C" int sphb_sim_tree(sphb_sim* s, size_t* num_leaves, uint64_t* leaves, 
 
 extern "C" int sphb_sim_neighbors(sphb_sim* s, uint32_t* out)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !out) { return SPHB_ERR_ARG; }
     size_t ng    = s->p.ngmax;
     unsigned pad = paddedNgmax(s->p.ngmax);
@@ -1479,6 +1512,7 @@ extern "C" int sphb_sim_neighbors(sphb_sim* s, uint32_t* out)
 
 extern "C" int sphb_sim_stage_times(sphb_sim* s, float* out)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !out) { return SPHB_ERR_ARG; }
     std::memcpy(out, s->stageMs, sizeof(s->stageMs));
     return SPHB_OK;
@@ -1497,6 +1531,7 @@ extern "C" void* sphb_sim_stream(sphb_sim* s) { return s ? static_cast<void*>(s-
 
 extern "C" int sphb_sim_load_state(sphb_sim* s, const double* const* fields, const uint64_t* id, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !fields || !id) { return SPHB_ERR_ARG; }
     if (!s->uploaded) { return SPHB_ERR_STATE; }
     cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
@@ -1511,6 +1546,7 @@ extern "C" int sphb_sim_load_state(sphb_sim* s, const double* const* fields, con
 
 extern "C" int sphb_sim_store_state(sphb_sim* s, double* const* fields, uint64_t* id, int on_device)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !fields || !id) { return SPHB_ERR_ARG; }
     cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
     for (int k = 0; k < kNumConserved; ++k)
@@ -1525,6 +1561,7 @@ extern "C" int sphb_sim_store_state(sphb_sim* s, double* const* fields, uint64_t
 
 extern "C" int sphb_sim_set_fixed_dt(sphb_sim* s, double dt)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !(dt >= 0.0)) { return SPHB_ERR_ARG; }
     s->fixedDt = dt;
     if (dt > 0)
@@ -1537,6 +1574,7 @@ extern "C" int sphb_sim_set_fixed_dt(sphb_sim* s, double dt)
 
 extern "C" int sphb_sim_set_params(sphb_sim* s, const sphb_params* p)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !p) { return SPHB_ERR_ARG; }
     if (p->ng0 != s->p.ng0 || p->ngmax != s->p.ngmax || p->precision != s->p.precision ||
         p->sinc_index != s->p.sinc_index || p->bucket_focus != s->p.bucket_focus || p->av_clean != s->p.av_clean ||
@@ -1556,6 +1594,7 @@ extern "C" int sphb_sim_set_params(sphb_sim* s, const sphb_params* p)
 extern "C" int sphb_sim_step_vjp(sphb_sim* s, const double* const* adj_post, double* const* adj_pre,
                                  double* alphamax_bar)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !adj_post || !adj_pre) { return SPHB_ERR_ARG; }
     for (int f = 0; f < kNumConserved; ++f)
     {
@@ -1578,6 +1617,7 @@ extern "C" int sphb_sim_step_vjp(sphb_sim* s, const double* const* adj_post, dou
 
 extern "C" int sphb_sim_tape_reserve(sphb_sim* s, int slots)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || slots < 1) { return SPHB_ERR_ARG; }
     if (!s->uploaded || s->p.av_clean) { return SPHB_ERR_STATE; }
     if (!s->hPre.data()) { SPHB_TRY(allocateAdjoint(*s)); }
@@ -1594,6 +1634,7 @@ extern "C" int sphb_sim_tape_reserve(sphb_sim* s, int slots)
 
 extern "C" int sphb_sim_step_record(sphb_sim* s, int slot)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || slot < 0) { return SPHB_ERR_ARG; }
     if (!s->uploaded || !(s->fixedDt > 0) || slot >= s->numTapeSlots) { return SPHB_ERR_STATE; }
     s->taping = true;
@@ -1607,6 +1648,7 @@ extern "C" int sphb_sim_step_record(sphb_sim* s, int slot)
 extern "C" int sphb_sim_step_vjp_recorded(sphb_sim* s, int slot, const double* const* adj_post,
                                           double* const* adj_pre, double* alphamax_bar)
 {
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
     if (!s || !adj_post || !adj_pre || slot < 0) { return SPHB_ERR_ARG; }
     for (int f = 0; f < kNumConserved; ++f)
     {
@@ -1627,6 +1669,14 @@ namespace sphb
 namespace simimpl
 {
 int runStage(sphb_sim& s, int stage) { return runStageChecked(s, stage); }
+int waitLateFields(sphb_sim& s, bool host)
+{
+    if (!s.latePending) { return kOk; }
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.stream, s.lateReady, 0));
+    if (host) { SPHB_CUDA_TRY(cudaEventSynchronize(s.lateReady)); }
+    s.latePending = false;
+    return kOk;
+}
 bool findField(sphb_sim& s, const char* name, void** ptr, int* kind) { return ::findField(&s, name, ptr, kind); }
 double cv(const sphb_sim& s) { return idealGasCv(s.p.mui, s.p.gamma); }
 

@@ -118,6 +118,12 @@ struct sphb_sim
     DeviceBuffer<unsigned> skinWork; // [0], [1]: deferred by the check / by the iteration, then the two lists
     DeviceBuffer<unsigned> skinGroupD;
     cudaStream_t sideStream{nullptr}; // the tree search of deferred groups, beside the refilter
+    // typed loads from host memory: the fields the step first reads after XMass (temp, v, x_m1, du_m1, alpha) are
+    // copied on copyStream while the sync, the search and XMass run; lateReady marks their arrival, and latePending
+    // says that the compute stream has not waited for it yet
+    cudaStream_t copyStream{nullptr};
+    cudaEvent_t copyFork{nullptr}, lateReady{nullptr};
+    bool latePending{false};
     cudaEvent_t skinFork{nullptr}, skinJoin{nullptr};
     unsigned skinCap{0};
     bool skinValid{false};    // rows match the particles' current indices (up to the tracked permutation)
@@ -203,5 +209,8 @@ int finishUpload(sphb_sim& s);
 int finishLoad(sphb_sim& s);
 //! computePositions of the global step with time steps dt, dt_m1 (kick-drift and energy update, FP64)
 int positions(sphb_sim& s, double dt, double dtM1);
+//! the compute stream waits for the late fields of a typed host load, if any are still in flight; with host, the
+//! calling thread waits for them too (entry points other than the step: their caller may reuse the host arrays)
+int waitLateFields(sphb_sim& s, bool host = false);
 } // namespace simimpl
 } // namespace sphb
