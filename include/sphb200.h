@@ -129,8 +129,8 @@ int sphb_sort_by_key_nearly_sorted(uint64_t* keys, uint32_t* values, size_t n, v
  *  12.6 MB inside this library. The array is reserved on a device when the library's device code is loaded there
  *  (with lazy module loading, at the first call on that device at the latest) and kept until the process exits.
  *  n may be at most sphb_sort_by_key_static_max() (1,048,576); larger n returns SPHB_ERR_CAPACITY and sorts
- *  nothing. The first call in a CUDA context looks up the array's device address (once per context); make that
- *  first call before any stream capture. Like sphb_sort_by_key, every call blocks the calling host thread: it
+ *  nothing. The first call in a CUDA context looks up the array's device address (once per context). Like
+ *  sphb_sort_by_key, every call blocks the calling host thread: it
  *  waits for the stream twice (the digit histogram and the error word are read back). All calls share the one
  *  array: calls that overlap on the GPU (on different streams or from different threads) race with each other, so
  *  run them one after another. The array keeps the previous call's contents; every call clears what it needs
