@@ -33,8 +33,9 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _particles(seed, periodic):
-    """clumped particles in the unit box, h giving about 40 neighbours where the density is mean"""
+def _particles(seed, periodic, h32=False):
+    """clumped particles in the unit box, h giving about 40 neighbours where the density is mean (float32 h with
+    h32, the reference's default type for h)"""
     rng = np.random.default_rng(seed)
     centers = rng.uniform(0.1, 0.9, (6, 3))
     which = rng.integers(0, 6, N)
@@ -43,6 +44,8 @@ def _particles(seed, periodic):
     h = 0.5 * (40.0 / (N * 4.18879)) ** (1 / 3) * rng.uniform(0.7, 1.3, N)
     ids = np.arange(N, dtype=np.int64)
     m = rng.uniform(0.5, 1.5, N).astype(np.float32)
+    if h32:
+        h = h.astype(np.float32)
     return p[:, 0].copy(), p[:, 1].copy(), p[:, 2].copy(), h, ids, m
 
 
@@ -56,7 +59,7 @@ def _moved(x, y, z, ids, periodic, seed):
     return out
 
 
-def _worker(rank, world, port, outdir, periodic, seed):
+def _worker(rank, world, port, outdir, periodic, seed, h32=False):
     import datetime
     import torch
     import torch.distributed as dist
@@ -66,7 +69,7 @@ def _worker(rank, world, port, outdir, periodic, seed):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
-    x, y, z, h, ids, m = _particles(seed, periodic)
+    x, y, z, h, ids, m = _particles(seed, periodic, h32)
     mine = np.random.default_rng(seed + 1).permutation(N) % world == rank
     t = {k: torch.from_numpy(np.ascontiguousarray(v[mine])) for k, v in
          dict(x=x, y=y, z=z, h=h, id=ids, m=m).items()}
@@ -90,10 +93,10 @@ def _worker(rank, world, port, outdir, periodic, seed):
     dist.destroy_process_group()
 
 
-def _check(outdir, world, periodic, seed):
+def _check(outdir, world, periodic, seed, h32=False):
     from oracle import domain as od
     from oracle import refsim
-    x, y, z, h, ids, m = _particles(seed, periodic)
+    x, y, z, h, ids, m = _particles(seed, periodic, h32)
     for rep in range(2):
         res = [dict(np.load(os.path.join(outdir, f"rank{r}_rep{rep}.npz"))) for r in range(world)]
         box = tuple(res[0]["box"])
@@ -165,11 +168,11 @@ def _moved_all(res, world, periodic, seed, x, y, z):
     return nx, ny, nz
 
 
-@pytest.mark.parametrize("world,periodic", [(2, True), (3, True), (2, False)])
-def test_domain_sync_and_halos_gloo(tmp_path, world, periodic):
+@pytest.mark.parametrize("world,periodic,h32", [(2, True, False), (3, True, False), (2, False, False), (2, True, True)])
+def test_domain_sync_and_halos_gloo(tmp_path, world, periodic, h32):
     from oracle import refsim
     if not refsim.available():
         pytest.skip("reference oracle not built")
     seed = 11 + world
-    mp.spawn(_worker, args=(world, _free_port(), str(tmp_path), periodic, seed), nprocs=world, join=True)
-    _check(str(tmp_path), world, periodic, seed)
+    mp.spawn(_worker, args=(world, _free_port(), str(tmp_path), periodic, seed, h32), nprocs=world, join=True)
+    _check(str(tmp_path), world, periodic, seed, h32)
