@@ -314,6 +314,9 @@ class Domain:
         for a in [y, z, h] + list(props.values()):
             if a.numel() != n or a.device != x.device:
                 raise ValueError("particle arrays differ in length or device")
+        if self._owned is not None and n != self.n_particles_with_halos:
+            raise ValueError(f"sync after the first takes the arrays the previous sync returned "
+                             f"({self.n_particles_with_halos} rows), got {n}")
         s, e = self._owned if self._owned is not None else (0, n)
         own = [a[s:e] for a in (x, y, z, h)] + [a[s:e] for a in props.values()]
         self._update_box(*own[:3])
