@@ -622,9 +622,12 @@ def noh_leg(side=160, steps=150, warmup=3) -> dict:
     a = torch.cuda.Event(enable_timing=True)
     b = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    stage_sum = {}
     a.record(stream)
     for _ in range(steps):
         sim.step()
+        for k, v in sim.stage_times().items():
+            stage_sum[k] = stage_sum.get(k, 0.0) + v
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b)
@@ -633,7 +636,8 @@ def noh_leg(side=160, steps=150, warmup=3) -> dict:
     out = {"workload": f"noh-{side}^3 lattice cut to r <= 0.5 ({n:,} particles), open box, mixed precision",
            "particles": n, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
            "particle_steps_per_s": n * steps / (ms * 1e-3), "max_density": float(rho.max()),
-           "time": s["ttot"], "energy_drift": abs(s["etot"] - e0) / abs(e0)}
+           "time": s["ttot"], "energy_drift": abs(s["etot"] - e0) / abs(e0),
+           "stage_ms": {k: round(v / steps, 4) for k, v in stage_sum.items()}, "neighbor_search": sim.search_stats()}
     sim.close()
     return out
 
