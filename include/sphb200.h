@@ -369,6 +369,14 @@ int sphb_sim_store_state(sphb_sim* sim, double* const* fields, uint64_t* id, int
  *  on the device, so a Dataset with the reference's default types (a mix of float and double) passes as it is. */
 int sphb_sim_upload_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
 
+/*! One step of a caller that keeps the particle state in host memory, in its own element types: the typed load of in
+ *  (host arrays, the fields of sphb_sim_upload_fields), sphb_sim_step, and the typed store of out (host arrays of any
+ *  fields sphb_sim_store_fields accepts). Returns after every output is in host memory. The same results as the
+ *  three calls one after another; the copies overlap the step where the data allow: the load's late fields as in
+ *  sphb_sim_load_fields, and the outputs m and id (final after the sync) and alpha (final after the AV switches)
+ *  leave the device while the later stages run. */
+int sphb_sim_step_fields(sphb_sim* sim, const sphb_field* in, int num_in, const sphb_field* out, int num_out);
+
 /*! sphb_sim_load_state with the caller's own element types (the fields of sphb_sim_upload_fields). From host memory,
  *  the copies of temp, vx, vy, vz, x_m1, y_m1, z_m1, du_m1 and alpha may still run when the call returns: they run
  *  beside the sync, the neighbour search and XMass of the next step, which read only x, y, z, h and m. The host

@@ -369,6 +369,98 @@ extern "C" int sphb_sim_store_fields(sphb_sim* s, const sphb_field* fields, int 
     return SPHB_OK;
 }
 
+namespace sphb
+{
+namespace
+{
+//! an output field of sphb_sim_step_fields: its device buffer and element types
+struct OutField
+{
+    const sphb_field* d;
+    void* ptr;
+    int src;
+    bool done;
+};
+
+/*! start the device-to-host copies of the named output fields on the copy stream, after the compute stream's work
+ *  so far (their values are final: the step changes them no more). Converted fields go through their own staging
+ *  slot of s.earlyStage. */
+int exportEarly(sphb_sim& s, std::vector<OutField>& out, std::initializer_list<const char*> names, size_t& slot)
+{
+    SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
+    for (const char* name : names)
+    {
+        for (auto& o : out)
+        {
+            if (o.done || std::strcmp(o.d->name, name) != 0) { continue; }
+            const void* from = o.ptr;
+            if (o.src != o.d->dtype)
+            {
+                char* stage = s.earlyStage.data() + slot * s.n * 8;
+                ++slot;
+                SPHB_TRY(convert(o.ptr, o.src, stage, o.d->dtype, s.n, s.copyStream));
+                from = stage;
+            }
+            SPHB_CUDA_TRY(cudaMemcpyAsync(o.d->data, from, s.n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost,
+                                          s.copyStream));
+            o.done = true;
+        }
+    }
+    return kOk;
+}
+} // namespace
+} // namespace sphb
+
+extern "C" int sphb_sim_step_fields(sphb_sim* s, const sphb_field* in, int num_in, const sphb_field* out,
+                                    int num_out)
+{
+    if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }
+    if (!s || !in || !out || num_in <= 0 || num_out <= 0) { return SPHB_ERR_ARG; }
+    if (!s->uploaded) { return SPHB_ERR_STATE; }
+    if (s->bdt) { return SPHB_ERR_STATE; }
+    std::vector<OutField> outs;
+    for (int q = 0; q < num_out; ++q)
+    {
+        const sphb_field& d = out[q];
+        void* ptr           = nullptr;
+        int kind            = 0;
+        if (!d.name || !d.data || !validDtype(d.dtype)) { return SPHB_ERR_ARG; }
+        if (!simimpl::findField(*s, d.name, &ptr, &kind)) { return SPHB_ERR_ARG; }
+        int src = dtypeOfKind(*s, kind);
+        if ((src == SPHB_U64) != (d.dtype == SPHB_U64)) { return SPHB_ERR_ARG; }
+        outs.push_back({out + q, ptr, src, false});
+    }
+    SPHB_TRY(s->earlyStage.reserve(3 * s->n * 8));
+    SPHB_TRY(importConserved(*s, in, num_in, false, true));
+    SPHB_TRY(simimpl::finishLoad(*s));
+    size_t slot = 0;
+    for (int stage = sSync; stage <= sConserved; ++stage)
+    {
+        SPHB_TRY(simimpl::runStage(*s, stage));
+        // m and the ids are final once the sync has ordered them; alpha once the AV switches have updated it
+        if (stage == sSync) { SPHB_TRY(exportEarly(*s, outs, {"m", "id"}, slot)); }
+        if (stage == sAV) { SPHB_TRY(exportEarly(*s, outs, {"alpha"}, slot)); }
+    }
+    SPHB_TRY(sphb_sim_integrate(s));
+    for (auto& o : outs)
+    {
+        if (o.done) { continue; }
+        const void* from = o.ptr;
+        if (o.src != o.d->dtype)
+        {
+            SPHB_TRY(s->typedStage.reserve(s->n * 8));
+            SPHB_TRY(convert(o.ptr, o.src, s->typedStage.data(), o.d->dtype, s->n, s->stream));
+            from = s->typedStage.data();
+        }
+        SPHB_CUDA_TRY(cudaMemcpyAsync(o.d->data, from, s->n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost,
+                                      s->stream));
+    }
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->copyStream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
+    return SPHB_OK;
+}
+
 extern "C" int sphb_sim_bind_fields(sphb_sim* s, const sphb_field* fields, int num_fields)
 {
     if (s) { SPHB_TRY(simimpl::waitLateFields(*s, true)); }

@@ -371,9 +371,6 @@ int allocateSkin(sphb_sim& s)
     SPHB_CUDA_TRY(cudaStreamCreateWithPriority(&s.sideStream, cudaStreamNonBlocking, greatestPriority));
     SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.skinFork, cudaEventDisableTiming));
     SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.skinJoin, cudaEventDisableTiming));
-    SPHB_CUDA_TRY(cudaStreamCreateWithFlags(&s.copyStream, cudaStreamNonBlocking));
-    SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.copyFork, cudaEventDisableTiming));
-    SPHB_CUDA_TRY(cudaEventCreateWithFlags(&s.lateReady, cudaEventDisableTiming));
     return kOk;
 }
 
@@ -1135,6 +1132,10 @@ extern "C" int sphb_sim_create(sphb_sim** out, size_t n, const sphb_box* box, co
     s->minDt    = params->minDt;
     s->minDt_m1 = params->minDt_m1;
     int rc      = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess ? kOk : kErrCuda;
+    // the copy stream and its events of the typed host loads and sphb_sim_step_fields
+    if (rc == kOk && cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking) != cudaSuccess) { rc = kErrCuda; }
+    if (rc == kOk && cudaEventCreateWithFlags(&s->copyFork, cudaEventDisableTiming) != cudaSuccess) { rc = kErrCuda; }
+    if (rc == kOk && cudaEventCreateWithFlags(&s->lateReady, cudaEventDisableTiming) != cudaSuccess) { rc = kErrCuda; }
     if (rc == kOk) { rc = allocateSim(*s); }
     if (rc != kOk)
     {

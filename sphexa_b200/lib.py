@@ -90,7 +90,8 @@ EXPORTED = ("sphb_default_params", "sphb_version", "sphb_compute_sfc_keys", "sph
             "sphb_ensemble_set_threads", "sphb_ensemble_autotune", "sphb_ensemble_step", "sphb_ensemble_size", "sphb_ensemble_search_stats",
             "sphb_ensemble_stage_times",
             "sphb_ensemble_get_field", "sphb_ensemble_scalars", "sphb_ensemble_stream",
-            "sphb_sim_upload_fields", "sphb_sim_load_fields", "sphb_sim_store_fields", "sphb_sim_bind_fields",
+            "sphb_sim_upload_fields", "sphb_sim_load_fields", "sphb_sim_store_fields",
+            "sphb_sim_step_fields", "sphb_sim_bind_fields",
             "sphb_dataset_xmass", "sphb_dataset_ve_def_gradh", "sphb_ideal_gas_eos",
             "sphb_dataset_iad_divv_curlv", "sphb_dataset_av_switches", "sphb_dataset_momentum_energy",
             "sphb_dataset_positions", "sphb_dataset_update_h", "sphb_compute_group_splits",
@@ -172,6 +173,7 @@ def load() -> C.CDLL:
         "sphb_sim_upload_fields": (C.c_int, [P, P, C.c_int, C.c_int]),
         "sphb_sim_load_fields": (C.c_int, [P, P, C.c_int, C.c_int]),
         "sphb_sim_store_fields": (C.c_int, [P, P, C.c_int, C.c_int]),
+        "sphb_sim_step_fields": (C.c_int, [P, P, C.c_int, P, C.c_int]),
         "sphb_sim_bind_fields": (C.c_int, [P, P, C.c_int]),
         "sphb_dataset_xmass": (C.c_int, [P, S, S, C.POINTER(Box)]),
         "sphb_dataset_ve_def_gradh": (C.c_int, [P, S, S, C.POINTER(Box)]),

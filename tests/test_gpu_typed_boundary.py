@@ -217,3 +217,38 @@ def test_host_load_overlapped_copies_equal_device_load(lib):
             assert np.array_equal(a.get(f), b.get(f)), (step, f)
         assert np.array_equal(a.get("id"), b.get("id"))
     assert a.scalars()["minDt"] == b.scalars()["minDt"]
+
+
+def test_step_fields_equals_load_step_store(lib):
+    """sphb_sim_step_fields (the load, the step and the store in one call, with m, id and alpha copied out while the
+    later stages run) gives the same host state as the three calls one after another, over five round trips with
+    the same pinned arrays as input and output."""
+    import torch
+    from sphexa_b200 import ic as icm
+    from sphexa_b200 import lib as L
+    from sphexa_b200.simulation import Simulation
+    ic = icm.sedov(24)
+    a = Simulation(ic, "mixed")
+    b = Simulation(ic, "mixed")
+    n = a.n
+
+    def buffers():
+        d = {f: torch.empty(n, dtype=torch.float64 if f in DOUBLE_FIELDS else torch.float32, pin_memory=True)
+             for f in CONSERVED}
+        d["id"] = torch.empty(n, dtype=torch.int64, pin_memory=True)
+        return d
+
+    ha, hb = buffers(), buffers()
+    ta, tb = L.make_fields(ha), L.make_fields(hb)
+    L.check(lib.sphb_sim_store_fields(a.h, ta, len(ta), 0), "store a")
+    L.check(lib.sphb_sim_store_fields(b.h, tb, len(tb), 0), "store b")
+    for step in range(5):
+        L.check(lib.sphb_sim_step_fields(a.h, ta, len(ta), ta, len(ta)), "step_fields")
+        L.check(lib.sphb_sim_load_fields(b.h, tb, len(tb), 0), "load")
+        b.step()
+        L.check(lib.sphb_sim_store_fields(b.h, tb, len(tb), 0), "store")
+        for f in list(CONSERVED) + ["id"]:
+            assert np.array_equal(ha[f].numpy(), hb[f].numpy()), (step, f)
+    for f in CONSERVED:
+        assert np.array_equal(a.get(f), b.get(f)), f
+    assert a.scalars()["minDt"] == b.scalars()["minDt"]
