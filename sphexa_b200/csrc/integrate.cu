@@ -236,7 +236,55 @@ __global__ void minMaxKernel(const double* v, size_t n, unsigned long long* out)
     }
 }
 
+//! out[0..6) = ordered bits of the running min/max of x, y and z (after minMax3InitKernel)
+__global__ void minMax3InitKernel(unsigned long long* out)
+{
+    int k = threadIdx.x;
+    if (k < 6) { out[k] = (k & 1) ? orderedBits(-INFINITY) : orderedBits(INFINITY); }
+}
+
+//! the three axes' extrema in one pass: min and max of x, y and z, a per-warp reduction and one atomic per value
+__global__ void minMax3Kernel(const double* x, const double* y, const double* z, size_t n, unsigned long long* out)
+{
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+    {
+        double v[3] = {x[i], y[i], z[i]};
+        for (int k = 0; k < 3; ++k)
+        {
+            lo[k] = fmin(lo[k], v[k]);
+            hi[k] = fmax(hi[k], v[k]);
+        }
+    }
+    for (int k = 0; k < 3; ++k)
+    {
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            lo[k] = fmin(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], off));
+            hi[k] = fmax(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], off));
+        }
+    }
+    if ((threadIdx.x & 31) == 0)
+    {
+        for (int k = 0; k < 3; ++k)
+        {
+            atomicMin(out + 2 * k, orderedBits(lo[k]));
+            atomicMax(out + 2 * k + 1, orderedBits(hi[k]));
+        }
+    }
+}
+
 } // namespace
+
+int minMax3(const double* x, const double* y, const double* z, size_t n, unsigned long long* out6, cudaStream_t s)
+{
+    minMax3InitKernel<<<1, 32, 0, s>>>(out6);
+    int blocks = int(std::min<size_t>(std::max<size_t>(ceilDiv(n, 256), 1), size_t(smCount()) * 4));
+    minMax3Kernel<<<blocks, 256, 0, s>>>(x, y, z, n, out6);
+    countLaunch(2);
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
 
 FixedFrame fixedFrameOf(const DevBox& box)
 {

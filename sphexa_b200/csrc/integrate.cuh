@@ -51,5 +51,7 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
 
 //! out2 = ordered bits of (min, max) of v
 int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s);
+//! the extrema of x, y and z into out6 as ordered bits {min x, max x, min y, max y, min z, max z}, stream-ordered
+int minMax3(const double* x, const double* y, const double* z, size_t n, unsigned long long* out6, cudaStream_t s);
 
 } // namespace sphb

@@ -105,9 +105,12 @@ struct LevelRange
     int r[kMaxLevel + 2];
 };
 
-__global__ void linkKernel(const uint64_t* prefixes, const int* nodeToLeaf, int numNodes, LevelRange lr,
+__global__ void linkKernel(const uint64_t* prefixes, const int* nodeToLeaf, int numNodes, const int* levelRange,
                            int* childOffsets, int* parents)
 {
+    __shared__ LevelRange lr;
+    if (threadIdx.x < kMaxLevel + 2) { lr.r[threadIdx.x] = levelRange[threadIdx.x]; }
+    __syncthreads();
     int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= numNodes) { return; }
     if (nodeToLeaf[p] >= 0)
@@ -458,20 +461,14 @@ int buildLinkedOctree(const uint64_t* leaves, int numLeaves, LinkedOctree& t, Tr
     }
     mapNodesKernel<<<ceilDiv(nn, 256), 256, 0, stream>>>(ids, nn, t.numInternal, t.nodeToLeaf.data(),
                                                          t.leafToNode.data());
-    int* dLevelRange = s.ints.data(); // reuse: offsets are no longer needed
-    levelRangeKernel<<<1, 32, 0, stream>>>(t.prefixes.data(), nn, dLevelRange);
+    // the level ranges stay on the device: the link kernel reads them there (no host round trip per tree build)
+    SPHB_TRY(t.levelRangeD.reserve(kMaxLevel + 2));
+    levelRangeKernel<<<1, 32, 0, stream>>>(t.prefixes.data(), nn, t.levelRangeD.data());
     countLaunch(2);
     SPHB_CUDA_TRY(cudaGetLastError());
-    SPHB_CUDA_TRY(cudaMemcpyAsync(t.levelRange, dLevelRange, sizeof(t.levelRange), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
-    LevelRange lr;
-    for (int l = 0; l < int(kMaxLevel) + 2; ++l)
-    {
-        lr.r[l] = t.levelRange[l];
-    }
     SPHB_CUDA_TRY(cudaMemsetAsync(t.parents.data(), 0, sizeof(int) * std::max(1, (nn - 1) / 8), stream));
-    linkKernel<<<ceilDiv(nn, 256), 256, 0, stream>>>(t.prefixes.data(), t.nodeToLeaf.data(), nn, lr,
-                                                     t.childOffsets.data(), t.parents.data());
+    linkKernel<<<ceilDiv(nn, 256), 256, 0, stream>>>(t.prefixes.data(), t.nodeToLeaf.data(), nn,
+                                                     t.levelRangeD.data(), t.childOffsets.data(), t.parents.data());
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     return kOk;
@@ -828,7 +825,8 @@ extern "C" int sphb_build_octree(const uint64_t* leaves, size_t num_leaves, uint
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     SPHB_CUDA_TRY(cudaStreamSynchronize(st));
-    std::memcpy(level_range, t.levelRange, sizeof(t.levelRange));
+    SPHB_CUDA_TRY(
+        cudaMemcpy(level_range, t.levelRangeD.data(), (kMaxLevel + 2) * sizeof(int), cudaMemcpyDeviceToHost));
     return SPHB_OK;
 }
 

@@ -25,7 +25,7 @@ struct LinkedOctree
     DeviceBuffer<unsigned> nodeCounts;   // [numNodes] particles per node
     DeviceBuffer<double> centers;        // [3*numNodes] geometric centre (x,y,z interleaved)
     DeviceBuffer<double> sizes;          // [3*numNodes] half edge lengths
-    int levelRange[kMaxLevel + 2]{};     // host copy of the first node index per level
+    DeviceBuffer<int> levelRangeD;       // [kMaxLevel + 2] the first node index per level
 };
 
 //! scratch shared by the tree routines

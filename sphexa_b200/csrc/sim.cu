@@ -89,18 +89,20 @@ int updateBox(sphb_sim& s)
     bool anyOpen = !s.hbox.periodic[0] || !s.hbox.periodic[1] || !s.hbox.periodic[2];
     if (!anyOpen || s.boxFromCaller) { return kOk; }
     double fit[6];
+    // the extrema of all three axes in one pass and one read back
+    SPHB_TRY(s.boxExtrema.reserve(6));
+    SPHB_TRY(minMax3(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.n, s.boxExtrema.data(), s.stream));
+    unsigned long long mm[6];
+    SPHB_CUDA_TRY(cudaMemcpyAsync(mm, s.boxExtrema.data(), sizeof(mm), cudaMemcpyDeviceToHost, s.stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
     for (int k = 0; k < 3; ++k)
     {
         fit[2 * k]     = s.hbox.lo[k];
         fit[2 * k + 1] = s.hbox.hi[k];
         if (!s.hbox.periodic[k])
         {
-            SPHB_TRY(minMax(s.f[fX + k].data(), s.n, s.reduce.data() + 2, s.stream));
-            unsigned long long mm[2];
-            SPHB_CUDA_TRY(cudaMemcpyAsync(mm, s.reduce.data() + 2, sizeof(mm), cudaMemcpyDeviceToHost, s.stream));
-            SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
-            fit[2 * k]     = fromOrderedBits(mm[0]);
-            fit[2 * k + 1] = fromOrderedBits(mm[1]);
+            fit[2 * k]     = fromOrderedBits(mm[2 * k]);
+            fit[2 * k + 1] = fromOrderedBits(mm[2 * k + 1]);
         }
     }
     if (!s.boxFirstCall)

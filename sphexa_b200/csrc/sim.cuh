@@ -175,6 +175,7 @@ struct sphb_sim
     bool boxFromCaller{false};   // the bound dataset's box is the caller's: the sync does not refit open axes
     bool lastSyncIdentity{true}; // the last domain sync found the particles already in SFC order
     DeviceBuffer<char> typedStage;
+    DeviceBuffer<unsigned long long> boxExtrema; // open axes: min/max of x, y, z as ordered bits
     DeviceBuffer<char> earlyStage; // sphb_sim_step_fields: converted outputs copied out before the step ends
 
     cudaEvent_t ev[kNumStages + 1]{};
