@@ -535,11 +535,18 @@ int globalTreeStep(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s
                                                              s.ints.data(), s.flags.data());
     countLaunch();
     SPHB_TRY(exclusiveScan(s.ints.data(), s.ints.data(), L + 1, s.scanTmp.data(), stream));
-    int newL = 0;
-    unsigned anyOp = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&newL, s.ints.data() + L, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&anyOp, s.flags.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+    // the counts of the current leaves, before knowing whether they change: in the steady state nothing splits or
+    // merges and one read back serves both decisions
+    SPHB_TRY(computeLeafCounts(g.leaves.data(), L, keys, n, g.counts.data(), stream));
+    maxCountKernel<<<ceilDiv(L, 256), 256, 0, stream>>>(g.counts.data(), L, s.flags.data());
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    unsigned msg[3]; // new leaf count, any op, largest count
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg, s.ints.data() + L, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 1, s.flags.data(), 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    int newL       = int(msg[0]);
+    unsigned anyOp = msg[1];
     if (anyOp)
     {
         // every op 1 would give the same leaves: the rebalance runs only when a node splits or merges
@@ -551,17 +558,16 @@ int globalTreeStep(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s
         g.leaves.swap(g.leavesAlt);
         g.numLeaves = newL;
         g.hostStale = true;
+        SPHB_TRY(g.counts.reserve(newL));
+        SPHB_TRY(computeLeafCounts(g.leaves.data(), newL, keys, n, g.counts.data(), stream));
+        SPHB_CUDA_TRY(cudaMemsetAsync(s.flags.data() + 1, 0, sizeof(unsigned), stream));
+        maxCountKernel<<<ceilDiv(newL, 256), 256, 0, stream>>>(g.counts.data(), newL, s.flags.data());
+        countLaunch();
+        SPHB_CUDA_TRY(cudaGetLastError());
+        SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 2, s.flags.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
     }
-    SPHB_TRY(g.counts.reserve(newL));
-    SPHB_TRY(computeLeafCounts(g.leaves.data(), newL, keys, n, g.counts.data(), stream));
-    maxCountKernel<<<ceilDiv(newL, 256), 256, 0, stream>>>(g.counts.data(), newL, s.flags.data());
-    countLaunch();
-    SPHB_CUDA_TRY(cudaGetLastError());
-    unsigned flags[2];
-    SPHB_CUDA_TRY(cudaMemcpyAsync(flags, s.flags.data(), sizeof(flags), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
-    bool converged = flags[0] == 0;
-    *maxCount      = converged ? 0u : flags[1];
+    *maxCount = anyOp ? msg[2] : 0u;
     return kOk;
 }
 
