@@ -38,9 +38,10 @@ KERNEL_STAGES = ("sync", "neighbors", "xmass", "ve_def_gradh_eos", "iad_divv_cur
 #: Sedov 96^3 (884,736 particles), mixed precision: dram__bytes_read.sum + dram__bytes_write.sum / particles. The
 #: neighbour stage's figure is its refilter of the skin rows (the kernel of every step but the row builds).
 NCU_TRAFFIC = {("neighbors", "mixed"): (718.09e6 + 318.53e6) / 884736,
-               ("iad_divv_curlv", "mixed"): (412.24e6 + 73.40e6) / 884736,
-               ("av_switches", "mixed"): (474.71e6 + 29.72e6) / 884736,
-               ("momentum_energy", "mixed"): (437.29e6 + 20.36e6) / 884736}
+               ("ve_def_gradh_eos", "mixed"): (400.35e6 + 35.16e6) / 884736,
+               ("iad_divv_curlv", "mixed"): (412.38e6 + 73.86e6) / 884736,
+               ("av_switches", "mixed"): (479.95e6 + 30.57e6) / 884736,
+               ("momentum_energy", "mixed"): (437.15e6 + 21.03e6) / 884736}
 
 
 def parse():
