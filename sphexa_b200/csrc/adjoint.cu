@@ -153,6 +153,22 @@ __device__ __forceinline__ void loadC(const ChainArrays<T>& a, size_t i, T (&c)[
     }
 }
 
+/*! the distance of a pair from its squared separation: FP64 by the square root, FP32 by one rsqrt, which also gives
+ *  rinv = 1 / dist for the divisions by the distance (0 for coincident particles, whose terms the kernels skip) */
+__device__ __forceinline__ void distOf(double r2, double& dist, double& rinv)
+{
+    dist = sqrt(r2);
+    rinv = 0.0;
+}
+__device__ __forceinline__ void distOf(float r2, float& dist, float& rinv)
+{
+    rinv = r2 > 0.0f ? rsqrtf(r2) : 0.0f;
+    dist = r2 * rinv;
+}
+//! x / dist: IEEE in FP64, by the reciprocal from distOf in FP32
+__device__ __forceinline__ double overDist(double x, double dist, double) { return x / dist; }
+__device__ __forceinline__ float overDist(float x, float, float rinv) { return x * rinv; }
+
 //! 1 / x: IEEE in FP64, the fast approximate division in FP32
 __device__ __forceinline__ double recipT(double x) { return 1.0 / x; }
 __device__ __forceinline__ float recipT(float x) { return __fdividef(1.0f, x); }
@@ -638,14 +654,17 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesVjpKernel(ChainArrays
                 uint32_t jl[kNbChunk];
                 loadChunk(a.nidx, t, t.ngPad, q0, jl);
                 unsigned qn = min(kNbChunk, t.count - q0);
+                // one pair per iteration, as the other adjoint pair loops
+#pragma unroll 1
                 for (unsigned q = 0; q < qn; ++q)
                 {
-                    uint32_t j     = jl[q];
+                    uint32_t j     = popChunk(jl);
                     Pos<T> pj      = posOf(a, j);
                     HydroRec<T> hj = loadHydro(a.hrec + j);
                     T divvJ        = __ldg(reinterpret_cast<const T*>(a.grec + j) + 6);
                     V3<T> r        = sepV(separation(pi, pj, 2.0 * hiD, box, k));
-                    T dist         = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+                    T dist, rinv;
+                    distOf(r.x * r.x + r.y * r.y + r.z * r.z, dist, rinv);
                     T v            = dist * hiInv;
                     T wk, dwk;
                     kernelWD(a.wh, k, v, wk, dwk);
@@ -666,7 +685,7 @@ __global__ void __launch_bounds__(kChainThreads) avSwitchesVjpKernel(ChainArrays
                     hiB += WiB * (-T(3) * Wi * hiInv) - vB * v * hiInv;
                     if (dist > T(0))
                     {
-                        T fd = vB * hiInv / dist;
+                        T fd = overDist(vB * hiInv, dist, rinv);
                         rB.x += fd * r.x;
                         rB.y += fd * r.y;
                         rB.z += fd * r.z;
@@ -751,7 +770,8 @@ __global__ void __launch_bounds__(kChainThreads) divvVjpKernel(ChainArrays<T> a,
             Pos<T> pj      = posOf(a, j);
             HydroRec<T> hj = loadHydro(a.hrec + j);
             V3<T> r        = sepV(separation(pi, pj, 2.0 * hiD, box, k));
-            T dist         = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+            T dist, rinv;
+            distOf(r.x * r.x + r.y * r.y + r.z * r.z, dist, rinv);
             T v            = dist * hiInv;
             T wk, dwk;
             kernelWD(a.wh, k, v, wk, dwk);
@@ -776,7 +796,7 @@ __global__ void __launch_bounds__(kChainThreads) divvVjpKernel(ChainArrays<T> a,
             hiB -= vB * v * hiInv;
             if (dist > T(0))
             {
-                T fd = vB * hiInv / dist;
+                T fd = overDist(vB * hiInv, dist, rinv);
                 rB.x += fd * r.x;
                 rB.y += fd * r.y;
                 rB.z += fd * r.z;
@@ -865,7 +885,8 @@ __global__ void __launch_bounds__(kChainThreads) iadVjpKernel(ChainArrays<T> a, 
             Pos<T> pj      = posOf(a, j);
             HydroRec<T> hj = loadHydro(a.hrec + j);
             V3<T> r        = sepV(separation(pi, pj, 2.0 * hiD, box, k));
-            T dist         = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+            T dist, rinv;
+            distOf(r.x * r.x + r.y * r.y + r.z * r.z, dist, rinv);
             T v            = dist * hiInv;
             T wk, dwk;
             kernelWD(a.wh, k, v, wk, dwk);
@@ -880,7 +901,7 @@ __global__ void __launch_bounds__(kChainThreads) iadVjpKernel(ChainArrays<T> a, 
             hiB -= vB * v * hiInv;
             if (dist > T(0))
             {
-                T fd = vB * hiInv / dist;
+                T fd = overDist(vB * hiInv, dist, rinv);
                 rB.x += fd * r.x;
                 rB.y += fd * r.y;
                 rB.z += fd * r.z;
@@ -973,7 +994,8 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhVjpKernel(ChainArrays
             uint32_t j = popChunk(js);
             Pos<T> pj  = posOf(a, j);
             V3<T> r    = sepV(separation(pi, pj, 2.0 * hiD, box, k));
-            T dist     = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+            T dist, rinv;
+            distOf(r.x * r.x + r.y * r.y + r.z * r.z, dist, rinv);
             T v        = dist * hInv;
             T w, dw, d, dd;
             kernelWD(a.wh, k, v, w, dw);
@@ -988,7 +1010,7 @@ __global__ void __launch_bounds__(kChainThreads) veDefGradhVjpKernel(ChainArrays
             hiB -= vB * v * hInv;
             if (dist > T(0))
             {
-                T fd     = vB * hInv / dist;
+                T fd     = overDist(vB * hInv, dist, rinv);
                 V3<T> rB = {fd * r.x, fd * r.y, fd * r.z};
                 xiB.x += rB.x;
                 xiB.y += rB.y;
@@ -1035,7 +1057,8 @@ __global__ void __launch_bounds__(kChainThreads) xmassVjpKernel(ChainArrays<T> a
             uint32_t j = popChunk(js);
             Pos<T> pj  = posOf(a, j);
             V3<T> r    = sepV(separation(pi, pj, 2.0 * hiD, box, k));
-            T dist     = sqrt(r.x * r.x + r.y * r.y + r.z * r.z);
+            T dist, rinv;
+            distOf(r.x * r.x + r.y * r.y + r.z * r.z, dist, rinv);
             T v        = dist * hInv;
             T w, dw;
             kernelWD(a.wh, k, v, w, dw);
@@ -1043,7 +1066,7 @@ __global__ void __launch_bounds__(kChainThreads) xmassVjpKernel(ChainArrays<T> a
             hiB -= vB * v * hInv;
             if (dist > T(0))
             {
-                T fd     = vB * hInv / dist;
+                T fd     = overDist(vB * hInv, dist, rinv);
                 V3<T> rB = {fd * r.x, fd * r.y, fd * r.z};
                 xiB.x += rB.x;
                 xiB.y += rB.y;
