@@ -435,26 +435,37 @@ extern "C" int sphb_sim_step_fields(sphb_sim* s, const sphb_field* in, int num_i
     SPHB_TRY(importConserved(*s, in, num_in, false, true));
     SPHB_TRY(simimpl::finishLoad(*s));
     size_t slot = 0;
+    // on an error return, the copies already started still finish before the call returns
+    auto fail = [&](int rc) {
+        cudaStreamSynchronize(s->copyStream);
+        cudaStreamSynchronize(s->stream);
+        return rc;
+    };
     for (int stage = sSync; stage <= sConserved; ++stage)
     {
-        SPHB_TRY(simimpl::runStage(*s, stage));
+        int rc = simimpl::runStage(*s, stage);
         // m and the ids are final once the sync has ordered them; alpha once the AV switches have updated it
-        if (stage == sSync) { SPHB_TRY(exportEarly(*s, outs, {"m", "id"}, slot)); }
-        if (stage == sAV) { SPHB_TRY(exportEarly(*s, outs, {"alpha"}, slot)); }
+        if (rc == kOk && stage == sSync) { rc = exportEarly(*s, outs, {"m", "id"}, slot); }
+        if (rc == kOk && stage == sAV) { rc = exportEarly(*s, outs, {"alpha"}, slot); }
+        if (rc != kOk) { return fail(rc); }
     }
-    SPHB_TRY(sphb_sim_integrate(s));
+    if (int rc = sphb_sim_integrate(s); rc != SPHB_OK) { return fail(rc); }
     for (auto& o : outs)
     {
         if (o.done) { continue; }
         const void* from = o.ptr;
         if (o.src != o.d->dtype)
         {
-            SPHB_TRY(s->typedStage.reserve(s->n * 8));
-            SPHB_TRY(convert(o.ptr, o.src, s->typedStage.data(), o.d->dtype, s->n, s->stream));
+            int rc = s->typedStage.reserve(s->n * 8);
+            if (rc == kOk) { rc = convert(o.ptr, o.src, s->typedStage.data(), o.d->dtype, s->n, s->stream); }
+            if (rc != kOk) { return fail(rc); }
             from = s->typedStage.data();
         }
-        SPHB_CUDA_TRY(cudaMemcpyAsync(o.d->data, from, s->n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost,
-                                      s->stream));
+        if (cudaMemcpyAsync(o.d->data, from, s->n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost, s->stream) !=
+            cudaSuccess)
+        {
+            return fail(SPHB_ERR_CUDA);
+        }
     }
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->copyStream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
