@@ -26,8 +26,10 @@ using namespace chain;
 // ---------------------------------------------------------------------------------------------------------------
 // XMass: rho0_i = (m_i + sum_j W_ij m_j) K / h_i^3, xm_i = m_i / rho0_i (sph/include/sph/hydro_ve/xmass_kern.hpp:50-79)
 // ---------------------------------------------------------------------------------------------------------------
+// FP32: at most 32 registers, eight 256-thread blocks per SM: more gathers in flight (0.348 -> 0.325 ms at 128^3)
 template<class T, int kMode>
-__global__ void __launch_bounds__(kChainMaxThreads) xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads, sizeof(T) == 4 ? 8 : 0)
+    xmassKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
     if (!chainTarget<kMode>(a, k.ngmax, t)) { return; }
@@ -64,8 +66,11 @@ __global__ void __launch_bounds__(kChainMaxThreads) xmassKernel(ChainArrays<T> a
 // VeDefGradh (sph/include/sph/hydro_ve/ve_def_gradh_kern.hpp:43-90) + ideal-gas EOS (hydro_ve/eos.hpp:52-94,
 // sph/include/sph/eos.hpp:19-50); writes kx, gradh, prho, c and the hydro record of the particle.
 // ---------------------------------------------------------------------------------------------------------------
+// FP32: at most 40 registers, six 256-thread blocks per SM, for the gathers' latency (0.625 -> 0.566 ms at 128^3,
+// though it spills a little; 48 registers gave 0.588, 32 gave 0.582)
 template<class T, int kMode>
-__global__ void __launch_bounds__(kChainMaxThreads) veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
+__global__ void __launch_bounds__(kChainMaxThreads, sizeof(T) == 4 ? 6 : 0)
+    veDefGradhEosKernel(ChainArrays<T> a, HydroConsts<T> k, DevBox box)
 {
     Target t;
     if (!chainTarget<kMode>(a, k.ngmax, t)) { return; }
