@@ -372,14 +372,16 @@ int sphb_sim_upload_fields(sphb_sim* sim, const sphb_field* fields, int num_fiel
 /*! One step of a caller that keeps the particle state in host memory, in its own element types: the typed load of in
  *  (host arrays, the fields of sphb_sim_upload_fields), sphb_sim_step, and the typed store of out (host arrays of any
  *  fields sphb_sim_store_fields accepts). Returns after every output is in host memory. The same results as the
- *  three calls one after another; the copies overlap the step where the data allow: the load's late fields as in
- *  sphb_sim_load_fields, and the outputs m and id (final after the sync) and alpha (final after the AV switches)
- *  leave the device while the later stages run. */
+ *  three calls one after another; the copies overlap the step where the data allow: the load's copies as in
+ *  sphb_sim_load_fields; the outputs m and id (final after the sync) and alpha (final after the AV switches) leave
+ *  the device while the later stages run; of the rest, the fields in their own type leave first, while the others
+ *  are converted. */
 int sphb_sim_step_fields(sphb_sim* sim, const sphb_field* in, int num_in, const sphb_field* out, int num_out);
 
 /*! sphb_sim_load_state with the caller's own element types (the fields of sphb_sim_upload_fields). From host memory,
- *  the copies of temp, vx, vy, vz, x_m1, y_m1, z_m1, du_m1 and alpha may still run when the call returns: they run
- *  beside the sync, the neighbour search and XMass of the next step, which read only x, y, z, h and m. The host
+ *  x, y, z and m are copied first; the copies of the other fields may still run when the call returns, in the order
+ *  the next step reads them: h and the ids beside its sync (unless the sync reorders the particles), temp, vx, vy,
+ *  vz and alpha beside the neighbour search and XMass, and x_m1, y_m1, z_m1 and du_m1 beside the J-loops. The host
  *  arrays must stay unchanged until the next call on the simulation returns (every call waits for the copies). */
 int sphb_sim_load_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
 

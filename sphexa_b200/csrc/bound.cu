@@ -109,9 +109,10 @@ const sphb_field* findDesc(const sphb_field* f, int num, const char* name)
 }
 
 /*! the conserved fields and ids of a typed upload or load: into s.f[k] (FP64) and s.idAlt. With lateCopy (a load
- *  from host memory), temp, v, x_m1, du_m1 and alpha go through the copy stream, after every earlier use of their
- *  buffers on the compute stream, and the compute stream waits for them only where the step first reads them
- *  (simimpl::waitLateFields): their transfer overlaps the sync, the search and XMass. */
+ *  from host memory) only x, y, z and m go through the compute stream. The rest follows on the copy stream, after
+ *  every earlier use of their buffers on the compute stream, in three groups; the compute stream waits for each only
+ *  where the step first reads it (simimpl::waitMidFields, waitLateGroup). h and the ids overlap the sync (unless it
+ *  reorders); temp, v and alpha the search and XMass; x_m1, y_m1, z_m1 and du_m1 the J-loops. */
 int importConserved(sphb_sim& s, const sphb_field* f, int num, bool onDevice, bool lateCopy = false)
 {
     if (!f || num <= 0) { return kErrArg; }
@@ -123,27 +124,58 @@ int importConserved(sphb_sim& s, const sphb_field* f, int num, bool onDevice, bo
     const sphb_field* idDesc = findDesc(f, num, "id");
     if (!idDesc || !idDesc->data || idDesc->dtype != SPHB_U64) { return kErrArg; }
     bool split = lateCopy && !onDevice && s.copyStream;
-    int numFirst = split ? int(fTemp) : int(kNumConserved);
-    for (int k = 0; k < numFirst; ++k)
+    for (int k = 0; k < kNumConserved; ++k)
     {
+        // split: x, y, z and m here (the sync reads nothing else unless it reorders), the rest below
+        if (split && k != fX && k != fY && k != fZ && k != fM) { continue; }
         const sphb_field* d = findDesc(f, num, kConservedNames[k]);
         SPHB_TRY(importArray(d->data, d->dtype, onDevice, s.f[k].data(), SPHB_F64, s.n, s.fAlt[k].data(), s.stream));
     }
-    SPHB_TRY(importArray(idDesc->data, SPHB_U64, onDevice, s.idAlt.data(), SPHB_U64, s.n, nullptr, s.stream));
-    if (split)
+    if (!split)
     {
-        // the late copies start after the early ones and the ids (and after every earlier use of their buffers):
-        // issued at once, the copy engine would interleave them and delay what the step needs first
-        SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
-        SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
-        for (int k = fTemp; k < kNumConserved; ++k)
+        SPHB_TRY(importArray(idDesc->data, SPHB_U64, onDevice, s.idAlt.data(), SPHB_U64, s.n, nullptr, s.stream));
+        return kOk;
+    }
+    // the other copies start after x, y, z and m (and after every earlier use of their buffers), in the order the step
+    // reads them: issued at once, the copy engine would interleave them and delay what the step needs first. Within
+    // each group the copies go first and the conversions of narrower fields after them, so that the copy engine does
+    // not wait for a kernel between two copies (the copy stream has the highest priority, so that its conversions
+    // do not wait for the blocks of the step's kernels either)
+    SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
+    auto group = [&](int which, cudaEvent_t ready) -> int {
+        // which: -1 h (with the ids), else a late group
+        auto inGroup = [&](int k) { return which < 0 ? k == fH : simimpl::lateGroupOf(k) == which; };
+        for (int k = fH; k < kNumConserved; ++k)
+        {
+            if (!inGroup(k)) { continue; }
+            const sphb_field* d = findDesc(f, num, kConservedNames[k]);
+            void* dst           = d->dtype == SPHB_F64 ? s.f[k].data() : s.fAlt[k].data();
+            SPHB_CUDA_TRY(cudaMemcpyAsync(dst, d->data, s.n * widthOf(d->dtype), cudaMemcpyHostToDevice,
+                                          s.copyStream));
+        }
+        if (which < 0)
+        {
+            SPHB_CUDA_TRY(cudaMemcpyAsync(s.idAlt.data(), idDesc->data, s.n * sizeof(uint64_t),
+                                          cudaMemcpyHostToDevice, s.copyStream));
+        }
+        for (int k = fH; k < kNumConserved; ++k)
         {
             const sphb_field* d = findDesc(f, num, kConservedNames[k]);
-            SPHB_TRY(importArray(d->data, d->dtype, false, s.f[k].data(), SPHB_F64, s.n, s.fAlt[k].data(),
-                                 s.copyStream));
+            if (inGroup(k) && d->dtype != SPHB_F64)
+            {
+                SPHB_TRY(convert(s.fAlt[k].data(), d->dtype, s.f[k].data(), SPHB_F64, s.n, s.copyStream));
+            }
         }
-        SPHB_CUDA_TRY(cudaEventRecord(s.lateReady, s.copyStream));
-        s.latePending = true;
+        SPHB_CUDA_TRY(cudaEventRecord(ready, s.copyStream));
+        return kOk;
+    };
+    SPHB_TRY(group(-1, s.midReady));
+    s.midPending = true;
+    for (int g = 0; g < sphb_sim::kLateGroups; ++g)
+    {
+        SPHB_TRY(group(g, s.lateReady[g]));
+        s.latePending[g] = true;
     }
     return kOk;
 }
@@ -373,14 +405,22 @@ namespace sphb
 {
 namespace
 {
-//! an output field of sphb_sim_step_fields: its device buffer and element types
+//! an output field of sphb_sim_step_fields: the caller's descriptor and the element type of the device buffer
 struct OutField
 {
     const sphb_field* d;
-    void* ptr;
     int src;
     bool done;
 };
+
+/*! the device buffer of an output field at the moment of its copy: a reordering sync swaps the field buffers, so the
+ *  pointer is looked up after the stages that may swap them, never before the step */
+void* outBuffer(sphb_sim& s, const OutField& o)
+{
+    void* ptr = nullptr;
+    int kind  = 0;
+    return simimpl::findField(s, o.d->name, &ptr, &kind) ? ptr : nullptr;
+}
 
 /*! start the device-to-host copies of the named output fields on the copy stream, after the compute stream's work
  *  so far (their values are final: the step changes them no more). Converted fields go through their own staging
@@ -394,18 +434,55 @@ int exportEarly(sphb_sim& s, std::vector<OutField>& out, std::initializer_list<c
         for (auto& o : out)
         {
             if (o.done || std::strcmp(o.d->name, name) != 0) { continue; }
-            const void* from = o.ptr;
+            const void* from = outBuffer(s, o);
+            if (!from) { return kErrArg; }
             if (o.src != o.d->dtype)
             {
                 char* stage = s.earlyStage.data() + slot * s.n * 8;
                 ++slot;
-                SPHB_TRY(convert(o.ptr, o.src, stage, o.d->dtype, s.n, s.copyStream));
+                SPHB_TRY(convert(from, o.src, stage, o.d->dtype, s.n, s.copyStream));
                 from = stage;
             }
             SPHB_CUDA_TRY(cudaMemcpyAsync(o.d->data, from, s.n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost,
                                           s.copyStream));
             o.done = true;
         }
+    }
+    return kOk;
+}
+/*! the outputs left after the step: the fields in their own type are copied straight from their buffers on the copy
+ *  stream while the compute stream converts the others into their staging slots; the converted ones follow */
+int exportFinal(sphb_sim& s, std::vector<OutField>& out, size_t& slot)
+{
+    SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
+    std::vector<std::pair<OutField*, const char*>> converted;
+    for (auto& o : out)
+    {
+        if (o.done) { continue; }
+        const void* from = outBuffer(s, o);
+        if (!from) { return kErrArg; }
+        if (o.src == o.d->dtype)
+        {
+            SPHB_CUDA_TRY(cudaMemcpyAsync(o.d->data, from, s.n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost,
+                                          s.copyStream));
+        }
+        else
+        {
+            char* stage = s.earlyStage.data() + slot * s.n * 8;
+            ++slot;
+            SPHB_TRY(convert(from, o.src, stage, o.d->dtype, s.n, s.stream));
+            converted.push_back({&o, stage});
+        }
+        o.done = true;
+    }
+    if (converted.empty()) { return kOk; }
+    SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
+    for (const auto& c : converted)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(c.first->d->data, c.second, s.n * widthOf(c.first->d->dtype),
+                                      cudaMemcpyDeviceToHost, s.copyStream));
     }
     return kOk;
 }
@@ -429,9 +506,15 @@ extern "C" int sphb_sim_step_fields(sphb_sim* s, const sphb_field* in, int num_i
         if (!simimpl::findField(*s, d.name, &ptr, &kind)) { return SPHB_ERR_ARG; }
         int src = dtypeOfKind(*s, kind);
         if ((src == SPHB_U64) != (d.dtype == SPHB_U64)) { return SPHB_ERR_ARG; }
-        outs.push_back({out + q, ptr, src, false});
+        outs.push_back({out + q, src, false});
     }
-    SPHB_TRY(s->earlyStage.reserve(3 * s->n * 8));
+    // one staging slot per converted output: their copies run while later conversions and kernels do
+    size_t numConverted = 0;
+    for (const auto& o : outs)
+    {
+        numConverted += o.src != o.d->dtype ? 1 : 0;
+    }
+    SPHB_TRY(s->earlyStage.reserve(std::max<size_t>(numConverted, 1) * s->n * 8));
     SPHB_TRY(importConserved(*s, in, num_in, false, true));
     SPHB_TRY(simimpl::finishLoad(*s));
     size_t slot = 0;
@@ -444,29 +527,15 @@ extern "C" int sphb_sim_step_fields(sphb_sim* s, const sphb_field* in, int num_i
     for (int stage = sSync; stage <= sConserved; ++stage)
     {
         int rc = simimpl::runStage(*s, stage);
-        // m and the ids are final once the sync has ordered them; alpha once the AV switches have updated it
-        if (rc == kOk && stage == sSync) { rc = exportEarly(*s, outs, {"m", "id"}, slot); }
+        // m and the ids are final once the sync has ordered them, alpha once the AV switches have updated it. m and
+        // the ids are copied out from IAD on, when the loaded fields have arrived: earlier, the two directions would
+        // share the link while the step waits for the loaded fields
+        if (rc == kOk && stage == sIad) { rc = exportEarly(*s, outs, {"m", "id"}, slot); }
         if (rc == kOk && stage == sAV) { rc = exportEarly(*s, outs, {"alpha"}, slot); }
         if (rc != kOk) { return fail(rc); }
     }
     if (int rc = sphb_sim_integrate(s); rc != SPHB_OK) { return fail(rc); }
-    for (auto& o : outs)
-    {
-        if (o.done) { continue; }
-        const void* from = o.ptr;
-        if (o.src != o.d->dtype)
-        {
-            int rc = s->typedStage.reserve(s->n * 8);
-            if (rc == kOk) { rc = convert(o.ptr, o.src, s->typedStage.data(), o.d->dtype, s->n, s->stream); }
-            if (rc != kOk) { return fail(rc); }
-            from = s->typedStage.data();
-        }
-        if (cudaMemcpyAsync(o.d->data, from, s->n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost, s->stream) !=
-            cudaSuccess)
-        {
-            return fail(SPHB_ERR_CUDA);
-        }
-    }
+    if (int rc = exportFinal(*s, outs, slot); rc != kOk) { return fail(rc); }
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->copyStream));
     SPHB_CUDA_TRY(cudaStreamSynchronize(s->stream));
     return SPHB_OK;

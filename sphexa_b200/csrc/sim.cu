@@ -128,6 +128,11 @@ int updateBox(sphb_sim& s)
 int syncDomain(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
+    // late fields a previous reordering sync left ungathered are put in its order before this one reorders again
+    for (int g = 0; g < sphb_sim::kLateGroups; ++g)
+    {
+        if (s.lateGatherPending[g]) { SPHB_TRY(simimpl::waitLateGroup(s, g)); }
+    }
     SPHB_TRY(updateBox(s));
     s.boxFirstCall = false;
     SPHB_TRY(launchSfcKeys(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.keys.data(), s.n, s.box, st));
@@ -143,24 +148,33 @@ int syncDomain(sphb_sim& s)
                            s.skinMoved.data(), s.n, st));
         s.skinBuild.swap(s.skinBuildAlt);
         s.skinAnyMoved = true;
-        ++s.searchStats[4];
+        s.syncRemapped = true;
     }
     SPHB_TRY(updateGlobalTree(s.gtree, s.keys.data(), s.n, s.ts, st));
 
     if (!identity)
     {
-        SPHB_TRY(simimpl::waitLateFields(s));
-        // reorder every conserved field and the ids into SFC order
+        SPHB_TRY(simimpl::waitMidFields(s));
+        // reorder every conserved field and the ids into SFC order; the late groups of a typed host load still in
+        // flight are gathered with the same order once they arrive (waitLateGroup): the rest of the sync, the search
+        // and XMass read none of them
         const void* src[kNumConserved + 2];
         void* dst[kNumConserved + 2];
+        bool now[kNumConserved];
+        int numFields = 0;
         for (int k = 0; k < kNumConserved; ++k)
         {
-            src[k] = s.f[k].data();
-            dst[k] = s.fAlt[k].data();
+            int g  = simimpl::lateGroupOf(k);
+            now[k] = g < 0 || !s.latePending[g];
+            if (g >= 0 && s.latePending[g]) { s.lateGatherPending[g] = true; }
+            if (!now[k]) { continue; }
+            src[numFields] = s.f[k].data();
+            dst[numFields] = s.fAlt[k].data();
+            ++numFields;
         }
-        src[kNumConserved] = s.id.data();
-        dst[kNumConserved] = s.idAlt.data();
-        int numFields      = kNumConserved + 1;
+        src[numFields] = s.id.data();
+        dst[numFields] = s.idAlt.data();
+        ++numFields;
         if (s.bdt)
         {
             src[numFields] = s.rung.data();
@@ -170,7 +184,7 @@ int syncDomain(sphb_sim& s)
         SPHB_TRY(gather8(s.order.data(), s.n, numFields, src, dst, st));
         for (int k = 0; k < kNumConserved; ++k)
         {
-            s.f[k].swap(s.fAlt[k]);
+            if (now[k]) { s.f[k].swap(s.fAlt[k]); }
         }
         s.id.swap(s.idAlt);
         if (s.bdt) { s.rung.swap(s.rungAlt); }
@@ -393,6 +407,10 @@ int searchNeighbors(sphb_sim& s)
                              s.box, np, s.nidx.data(), s.nc.data(), s.status.data(), st);
     };
 
+    SPHB_TRY(simimpl::resolveIdCheck(s));
+    // a remap counts once the rows are known to be kept (a pending id comparison may drop them)
+    if (s.syncRemapped && s.skinValid) { ++s.searchStats[4]; }
+    s.syncRemapped = false;
     bool useSkin = s.p.nb_skin > 0.0 && !s.taping;
     if (!useSkin || s.skinHoldoff > 0)
     {
@@ -491,14 +509,18 @@ int searchNeighbors(sphb_sim& s)
 int runStage(sphb_sim& s, int stage)
 {
     cudaStream_t st = s.stream;
-    // the sync (unless it reorders), the search and XMass read only x, y, z, h and m
-    if (stage > sXMass) { SPHB_TRY(simimpl::waitLateFields(s)); }
+    // the sync (unless it reorders), the search and XMass read only x, y, z, h and m; the force stages no x_m1, y_m1,
+    // z_m1 or du_m1
+    if (stage > sXMass) { SPHB_TRY(simimpl::waitLateGroup(s, 0)); }
+    if (stage >= sConserved) { SPHB_TRY(simimpl::waitLateFields(s)); }
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[stage], st));
     switch (stage)
     {
     case sSync: return syncDomain(s);
     case sNeighbors:
     {
+        // h and the ids of a typed host load
+        SPHB_TRY(simimpl::waitMidFields(s));
         if (s.taping)
         {
             SPHB_CUDA_TRY(cudaMemcpyAsync(s.hPre.data(), s.f[fH].data(), s.n * sizeof(double),
@@ -1135,9 +1157,26 @@ extern "C" int sphb_sim_create(sphb_sim** out, size_t n, const sphb_box* box, co
     s->minDt_m1 = params->minDt_m1;
     int rc      = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess ? kOk : kErrCuda;
     // the copy stream and its events of the typed host loads and sphb_sim_step_fields
-    if (rc == kOk && cudaStreamCreateWithFlags(&s->copyStream, cudaStreamNonBlocking) != cudaSuccess) { rc = kErrCuda; }
+    int leastPriority = 0, greatestPriority = 0;
+    if (rc == kOk && cudaDeviceGetStreamPriorityRange(&leastPriority, &greatestPriority) != cudaSuccess)
+    {
+        rc = kErrCuda;
+    }
+    if (rc == kOk &&
+        cudaStreamCreateWithPriority(&s->copyStream, cudaStreamNonBlocking, greatestPriority) != cudaSuccess)
+    {
+        rc = kErrCuda;
+    }
     if (rc == kOk && cudaEventCreateWithFlags(&s->copyFork, cudaEventDisableTiming) != cudaSuccess) { rc = kErrCuda; }
-    if (rc == kOk && cudaEventCreateWithFlags(&s->lateReady, cudaEventDisableTiming) != cudaSuccess) { rc = kErrCuda; }
+    for (auto& e : s->lateReady)
+    {
+        if (rc == kOk && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) { rc = kErrCuda; }
+    }
+    if (rc == kOk && cudaEventCreateWithFlags(&s->midReady, cudaEventDisableTiming) != cudaSuccess) { rc = kErrCuda; }
+    if (rc == kOk && cudaEventCreateWithFlags(&s->idCheckDone, cudaEventDisableTiming) != cudaSuccess)
+    {
+        rc = kErrCuda;
+    }
     if (rc == kOk) { rc = allocateSim(*s); }
     if (rc != kOk)
     {
@@ -1168,7 +1207,12 @@ extern "C" int sphb_sim_destroy(sphb_sim* s)
         cudaStreamDestroy(s->copyStream);
     }
     if (s->copyFork) { cudaEventDestroy(s->copyFork); }
-    if (s->lateReady) { cudaEventDestroy(s->lateReady); }
+    for (auto& e : s->lateReady)
+    {
+        if (e) { cudaEventDestroy(e); }
+    }
+    if (s->midReady) { cudaEventDestroy(s->midReady); }
+    if (s->idCheckDone) { cudaEventDestroy(s->idCheckDone); }
     if (s->skinFork) { cudaEventDestroy(s->skinFork); }
     if (s->skinJoin) { cudaEventDestroy(s->skinJoin); }
     if (s->hostMsg) { cudaFreeHost(s->hostMsg); }
@@ -1672,12 +1716,93 @@ namespace sphb
 namespace simimpl
 {
 int runStage(sphb_sim& s, int stage) { return runStageChecked(s, stage); }
+int waitMidFields(sphb_sim& s)
+{
+    if (!s.midPending) { return kOk; }
+    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.stream, s.midReady, 0));
+    s.midPending = false;
+    if (s.idCheckPending)
+    {
+        // the loaded ids (now s.id) against the previous ones (s.idAlt), before a reordering sync reuses idAlt; the
+        // host reads the flag where it decides between the rows and the tree search
+        SPHB_TRY(idsDiffer(s.id.data(), s.idAlt.data(), s.n, s.skinWork.data(), s.stream));
+        s.hostMsg[14] = 1;
+        SPHB_CUDA_TRY(cudaMemcpyAsync(s.hostMsg + 14, s.skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                      s.stream));
+        SPHB_CUDA_TRY(cudaEventRecord(s.idCheckDone, s.stream));
+    }
+    return kOk;
+}
+
+int resolveIdCheck(sphb_sim& s)
+{
+    if (!s.idCheckPending) { return kOk; }
+    SPHB_TRY(waitMidFields(s));
+    SPHB_CUDA_TRY(cudaEventSynchronize(s.idCheckDone));
+    unsigned differ = 1;
+    std::memcpy(&differ, s.hostMsg + 14, sizeof(differ));
+    if (differ) { s.skinValid = false; }
+    s.idCheckPending = false;
+    return kOk;
+}
+
+int lateGroupOf(int field)
+{
+    switch (field)
+    {
+    case fTemp:
+    case fVx:
+    case fVy:
+    case fVz:
+    case fAlpha: return 0;
+    case fXm1:
+    case fYm1:
+    case fZm1:
+    case fDuM1: return 1;
+    default: return -1;
+    }
+}
+
+int waitLateGroup(sphb_sim& s, int group)
+{
+    SPHB_TRY(waitMidFields(s));
+    if (s.latePending[group])
+    {
+        SPHB_CUDA_TRY(cudaStreamWaitEvent(s.stream, s.lateReady[group], 0));
+        s.latePending[group] = false;
+    }
+    if (s.lateGatherPending[group])
+    {
+        // the group's fields into the order of the last sync (which gathered the others)
+        const void* src[kNumConserved];
+        void* dst[kNumConserved];
+        int numFields = 0;
+        for (int k = 0; k < kNumConserved; ++k)
+        {
+            if (lateGroupOf(k) != group) { continue; }
+            src[numFields] = s.f[k].data();
+            dst[numFields] = s.fAlt[k].data();
+            ++numFields;
+        }
+        SPHB_TRY(gather8(s.order.data(), s.n, numFields, src, dst, s.stream));
+        for (int k = 0; k < kNumConserved; ++k)
+        {
+            if (lateGroupOf(k) == group) { s.f[k].swap(s.fAlt[k]); }
+        }
+        s.lateGatherPending[group] = false;
+    }
+    return kOk;
+}
+
 int waitLateFields(sphb_sim& s, bool host)
 {
-    if (!s.latePending) { return kOk; }
-    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.stream, s.lateReady, 0));
-    if (host) { SPHB_CUDA_TRY(cudaEventSynchronize(s.lateReady)); }
-    s.latePending = false;
+    for (int g = 0; g < sphb_sim::kLateGroups; ++g)
+    {
+        bool pending = s.latePending[g];
+        SPHB_TRY(waitLateGroup(s, g));
+        if (host && pending) { SPHB_CUDA_TRY(cudaEventSynchronize(s.lateReady[g])); }
+    }
+    if (host) { SPHB_TRY(resolveIdCheck(s)); }
     return kOk;
 }
 bool findField(sphb_sim& s, const char* name, void** ptr, int* kind) { return ::findField(&s, name, ptr, kind); }
@@ -1712,6 +1837,14 @@ int finishLoad(sphb_sim& s)
     }
     // the skin rows stay usable when every index holds the same particle as before (positions and h may differ
     // arbitrarily: the next refilter checks them against the build)
+    if (s.midPending)
+    {
+        // the ids are still in flight on the copy stream: compared once they arrive (waitMidFields), read by the
+        // host before the neighbour search
+        s.id.swap(s.idAlt);
+        s.idCheckPending = true;
+        return kOk;
+    }
     SPHB_TRY(idsDiffer(s.id.data(), s.idAlt.data(), s.n, s.skinWork.data(), s.stream));
     unsigned differ = 1;
     SPHB_CUDA_TRY(cudaMemcpyAsync(&differ, s.skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, s.stream));
@@ -1723,6 +1856,7 @@ int finishLoad(sphb_sim& s)
 
 int positions(sphb_sim& s, double dt, double dtM1)
 {
+    SPHB_TRY(waitLateFields(s));
     s.minDt    = dt;
     s.minDt_m1 = dtM1;
     double c   = idealGasCv(s.p.mui, s.p.gamma);

@@ -118,17 +118,27 @@ struct sphb_sim
     DeviceBuffer<unsigned> skinWork; // [0], [1]: deferred by the check / by the iteration, then the two lists
     DeviceBuffer<unsigned> skinGroupD;
     cudaStream_t sideStream{nullptr}; // the tree search of deferred groups, beside the refilter
-    // typed loads from host memory: the fields the step first reads after XMass (temp, v, x_m1, du_m1, alpha) are
-    // copied on copyStream while the sync, the search and XMass run; lateReady marks their arrival, and latePending
-    // says that the compute stream has not waited for it yet
+    // typed loads from host memory: x, y, z and m come first on the compute stream; the rest follows on copyStream in
+    // the order the step reads it: h and the ids while the sync runs (midReady: read by a reordering sync's gather,
+    // else by the search); temp, v and alpha, first read by VeDefGradh and IAD, while the search and XMass run (late
+    // group 0); x_m1, y_m1, z_m1 and du_m1, first read by the integration, while the J-loops run (late group 1).
+    // midPending / latePending say that the compute stream has not waited for them yet; lateGatherPending, that a
+    // reordering sync left the group to be gathered once it arrives; idCheckPending, that the comparison of the loaded
+    // ids with the previous ones (whether the skin rows stay usable) is on its way to hostMsg[14] (idCheckDone)
+    static constexpr int kLateGroups = 2;
     cudaStream_t copyStream{nullptr};
-    cudaEvent_t copyFork{nullptr}, lateReady{nullptr};
-    bool latePending{false};
+    cudaEvent_t copyFork{nullptr}, midReady{nullptr}, idCheckDone{nullptr};
+    cudaEvent_t lateReady[kLateGroups]{};
+    bool midPending{false};
+    bool latePending[kLateGroups]{};
+    bool lateGatherPending[kLateGroups]{};
+    bool idCheckPending{false};
     cudaEvent_t skinFork{nullptr}, skinJoin{nullptr};
     unsigned skinCap{0};
     bool skinValid{false};    // rows match the particles' current indices (up to the tracked permutation)
     bool skinAnyMoved{false}; // some index holds another particle than at the build (skinBuild, skinMoved valid)
     bool skinFiltered{false}; // this step's lists came from the rows
+    bool syncRemapped{false}; // the last sync composed its order into the rows' index map (counted at the search)
     int skinAge{0};           // steps since the build
     int skinHoldoff{0};       // steps left of plain tree searches after rows proved short-lived
     unsigned skinDeferredLast{0};
@@ -211,8 +221,20 @@ int finishUpload(sphb_sim& s);
 int finishLoad(sphb_sim& s);
 //! computePositions of the global step with time steps dt, dt_m1 (kick-drift and energy update, FP64)
 int positions(sphb_sim& s, double dt, double dtM1);
-//! the compute stream waits for the late fields of a typed host load, if any are still in flight; with host, the
-//! calling thread waits for them too (entry points other than the step: their caller may reuse the host arrays)
+//! the compute stream waits for h and the ids of a typed host load, if they are still in flight, and compares the
+//! ids with the previous ones when skin rows exist
+int waitMidFields(sphb_sim& s);
+//! late group of a conserved field of a typed host load (temp, v, alpha: 0; x_m1, y_m1, z_m1, du_m1: 1; -1 for the
+//! fields copied before them)
+int lateGroupOf(int field);
+//! the compute stream waits for one late group of a typed host load if it is still in flight, and gathers it if a
+//! reordering sync left it
+int waitLateGroup(sphb_sim& s, int group);
+//! the compute stream waits for every field of a typed host load still in flight and gathers the late ones a
+//! reordering sync left; with host, the calling thread waits for them too and learns the id comparison (entry points
+//! other than the step: their caller may reuse the host arrays)
 int waitLateFields(sphb_sim& s, bool host = false);
+//! the host learns the result of a pending id comparison; rows whose indices now hold other particles are dropped
+int resolveIdCheck(sphb_sim& s);
 } // namespace simimpl
 } // namespace sphb

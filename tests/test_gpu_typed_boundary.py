@@ -184,11 +184,24 @@ def test_typed_store_and_load_round_trip(lib):
         assert np.array_equal(a.get(f), b.get(f)), f
 
 
+def _shuffle(bufs, seed):
+    """the same random particle order for every array of every buffer set (host or device tensors)"""
+    import torch
+    n = next(iter(bufs[0].values())).numel()
+    perm = torch.from_numpy(np.random.default_rng(seed).permutation(n))
+    for d in bufs:
+        for f, t in d.items():
+            t.copy_(t[perm.to(t.device)].clone())
+
+
 def test_host_load_overlapped_copies_equal_device_load(lib):
-    """A typed load from host memory leaves temp, v, x_m1, du_m1 and alpha in flight beside the next step's sync,
-    search and XMass. Seven round trips (store to pinned host buffers in the reference's default types, load, step)
-    give the same states, bit for bit, as the same round trips through device buffers, where every copy is ordered
-    on the simulation's stream."""
+    """A typed load from host memory leaves h, m and the ids in flight beside the next step's keys, sort and trees,
+    temp, v and alpha beside the sync, the search and XMass, and x_m1, y_m1, z_m1 and du_m1 beside the J-loops. Seven
+    round trips (store to pinned host
+    buffers in the reference's default types, load, step) give the same states, bit for bit, as the same round trips
+    through device buffers, where every copy is ordered on the simulation's stream. Twice the stored particles are
+    shuffled before the load: the sync then reorders all of them while the late fields are still in flight (they
+    are gathered once they arrive), and the ids no longer match the skin rows, which both simulations drop alike."""
     import torch
     from sphexa_b200 import ic as icm
     from sphexa_b200 import lib as L
@@ -209,6 +222,10 @@ def test_host_load_overlapped_copies_equal_device_load(lib):
     for step in range(7):
         L.check(lib.sphb_sim_store_fields(a.h, ta, len(ta), 0), "store host")
         L.check(lib.sphb_sim_store_fields(b.h, tb, len(tb), 1), "store device")
+        if step in (3, 5):
+            torch.cuda.synchronize()
+            _shuffle([ha, db], step)
+            torch.cuda.synchronize()
         L.check(lib.sphb_sim_load_fields(a.h, ta, len(ta), 0), "load host")
         L.check(lib.sphb_sim_load_fields(b.h, tb, len(tb), 1), "load device")
         a.step()
@@ -217,6 +234,8 @@ def test_host_load_overlapped_copies_equal_device_load(lib):
             assert np.array_equal(a.get(f), b.get(f)), (step, f)
         assert np.array_equal(a.get("id"), b.get("id"))
     assert a.scalars()["minDt"] == b.scalars()["minDt"]
+    assert a.search_stats() == b.search_stats()
+    assert a.search_stats()["skin_builds"] >= 3, a.search_stats()
 
 
 def test_step_fields_equals_load_step_store(lib):
@@ -243,6 +262,8 @@ def test_step_fields_equals_load_step_store(lib):
     L.check(lib.sphb_sim_store_fields(a.h, ta, len(ta), 0), "store a")
     L.check(lib.sphb_sim_store_fields(b.h, tb, len(tb), 0), "store b")
     for step in range(5):
+        if step == 2:
+            _shuffle([ha, hb], step)
         L.check(lib.sphb_sim_step_fields(a.h, ta, len(ta), ta, len(ta)), "step_fields")
         L.check(lib.sphb_sim_load_fields(b.h, tb, len(tb), 0), "load")
         b.step()
@@ -252,3 +273,4 @@ def test_step_fields_equals_load_step_store(lib):
     for f in CONSERVED:
         assert np.array_equal(a.get(f), b.get(f)), f
     assert a.scalars()["minDt"] == b.scalars()["minDt"]
+    assert a.search_stats() == b.search_stats()
