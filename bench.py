@@ -818,7 +818,8 @@ def cpu_baseline(ic, n, steps=REF_STEPS, warmup=REF_WARMUP):
     return {"value": n / best, "unit": UNIT, "cores": int(os.environ["OMP_NUM_THREADS"]), "kind": "reference",
             "cpu_model": model, "build": (f"oracle/_ref/libsphref_timed_{isa}.so: -O3, default FP contraction, "
                                           f"x86-64-{isa}") if isa else "oracle/_ref/libsphref_mixed.so",
-            "step_s": {"median": med, "min": min(times), "max": max(times), "mean": sum(times) / len(times)},
+            "step_s": {"median": statistics.median(times), "min": best, "max": max(times),
+                       "mean": sum(times) / len(times)},
             "sample": f"{steps} steps after {warmup} warm-up of the same Sedov workload ({n:,} particles), reference "
                       f"CPU code with its default types (f64 coordinates, f32 hydro fields), wall clock of each step, "
                       f"the fastest"}
