@@ -380,8 +380,9 @@ int sphb_sim_step_fields(sphb_sim* sim, const sphb_field* in, int num_in, const 
 
 /*! sphb_sim_load_state with the caller's own element types (the fields of sphb_sim_upload_fields). From host memory,
  *  x, y, z and m are copied first; the copies of the other fields may still run when the call returns, in the order
- *  the next step reads them: h and the ids beside its sync (unless the sync reorders the particles), temp, vx, vy,
- *  vz and alpha beside the neighbour search and XMass, and x_m1, y_m1, z_m1 and du_m1 beside the J-loops. The host
+ *  the next step reads them: h and the ids beside its sync (unless the sync reorders the particles), temp beside
+ *  the neighbour search, vx, vy, vz and alpha beside XMass and VeDefGradh, and x_m1, y_m1, z_m1 and du_m1 beside the
+ *  J-loops. The host
  *  arrays must stay unchanged until the next call on the simulation returns (every call waits for the copies). */
 int sphb_sim_load_fields(sphb_sim* sim, const sphb_field* fields, int num_fields, int on_device);
 

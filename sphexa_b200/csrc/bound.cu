@@ -108,6 +108,19 @@ const sphb_field* findDesc(const sphb_field* f, int num, const char* name)
     return nullptr;
 }
 
+/*! a host-to-device copy as pieces of at most 4 MiB, so that small copies of the compute stream, which may share
+ *  the copy engine, wait behind one piece at most */
+int copyInPieces(void* dst, const void* src, size_t bytes, cudaStream_t stream)
+{
+    constexpr size_t kPiece = size_t(4) << 20;
+    for (size_t off = 0; off < bytes; off += kPiece)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(static_cast<char*>(dst) + off, static_cast<const char*>(src) + off,
+                                      std::min(kPiece, bytes - off), cudaMemcpyHostToDevice, stream));
+    }
+    return kOk;
+}
+
 /*! the conserved fields and ids of a typed upload or load: into s.f[k] (FP64) and s.idAlt. With lateCopy (a load
  *  from host memory) only x, y, z and m go through the compute stream. The rest follows on the copy stream, after
  *  every earlier use of their buffers on the compute stream, in three groups; the compute stream waits for each only
@@ -151,14 +164,9 @@ int importConserved(sphb_sim& s, const sphb_field* f, int num, bool onDevice, bo
             if (!inGroup(k)) { continue; }
             const sphb_field* d = findDesc(f, num, kConservedNames[k]);
             void* dst           = d->dtype == SPHB_F64 ? s.f[k].data() : s.fAlt[k].data();
-            SPHB_CUDA_TRY(cudaMemcpyAsync(dst, d->data, s.n * widthOf(d->dtype), cudaMemcpyHostToDevice,
-                                          s.copyStream));
+            SPHB_TRY(copyInPieces(dst, d->data, s.n * widthOf(d->dtype), s.copyStream));
         }
-        if (which < 0)
-        {
-            SPHB_CUDA_TRY(cudaMemcpyAsync(s.idAlt.data(), idDesc->data, s.n * sizeof(uint64_t),
-                                          cudaMemcpyHostToDevice, s.copyStream));
-        }
+        if (which < 0) { SPHB_TRY(copyInPieces(s.idAlt.data(), idDesc->data, s.n * sizeof(uint64_t), s.copyStream)); }
         for (int k = fH; k < kNumConserved; ++k)
         {
             const sphb_field* d = findDesc(f, num, kConservedNames[k]);
@@ -679,8 +687,7 @@ extern "C" int sphb_dataset_momentum_energy(sphb_sim* s, size_t first, size_t la
     SPHB_TRY(importBound(*s, {"vx", "vy", "vz", "xm", "kx", "c", "prho", "c11", "c12", "c13", "c22", "c23", "c33",
                               "divv", "alpha"}));
     SPHB_TRY(packRecords(*s, true));
-    unsigned long long init = orderedBits(INFINITY);
-    SPHB_CUDA_TRY(cudaMemcpyAsync(s->reduce.data() + 1, &init, sizeof(init), cudaMemcpyHostToDevice, s->stream));
+    SPHB_TRY(setWords(s->reduce.data() + 1, 1, orderedBits(INFINITY), 0, s->stream));
     SPHB_TRY(simimpl::runStage(*s, sMomentum));
     SPHB_TRY(exportBound(*s, {"ax", "ay", "az", "du"}));
     unsigned long long bits = 0;

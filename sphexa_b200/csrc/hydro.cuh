@@ -124,6 +124,9 @@ struct ChainArrays
     ChainTape<T> tape;
     BatchView batch;
     AVRec<T>* avrec{nullptr};
+    // VeDefGradh leaves the velocity of the hydro record to launchPackVelocity (the velocities of a typed host load
+    // still in flight)
+    bool recordNoVelocity{false};
     DVRec<T>* dvrec{nullptr}; // set: AV cleaning (HydroVeProp<avClean = true>)
     T* dv[6]{};              // the same six fields as arrays (dV11 .. dV33)
     int threads{128}; // block size of the J-loop launches
@@ -140,6 +143,9 @@ template<class T>
 int launchXMass(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
 template<class T>
 int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
+//! the velocity of every particle into its hydro record (after a VeDefGradh with recordNoVelocity)
+template<class T>
+int launchPackVelocity(const ChainArrays<T>& a, cudaStream_t s);
 template<class T>
 int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s);
 template<class T>

@@ -170,8 +170,27 @@ __global__ void __launch_bounds__(kChainMaxThreads, sizeof(T) == 4 ? 6 : 0)
     a.gradh[t.i] = gradhi;
     a.prho[t.i]  = T(prho);
     a.c[t.i]     = T(c);
-    a.hrec[t.i]  = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), T(1) / hi, xmassi, xmassi / kxi, T(c),
-                              T(prho)};
+    if (a.recordNoVelocity)
+    {
+        a.hrec[t.i] = HydroRec<T>{T(0), T(0), T(0), T(1) / hi, xmassi, xmassi / kxi, T(c), T(prho)};
+    }
+    else
+    {
+        a.hrec[t.i] = HydroRec<T>{T(a.vx[t.i]), T(a.vy[t.i]), T(a.vz[t.i]), T(1) / hi, xmassi, xmassi / kxi, T(c),
+                                  T(prho)};
+    }
+}
+
+//! the velocity part of the hydro record, the same values VeDefGradh writes there otherwise
+template<class T>
+__global__ void packVelocityKernel(size_t n, const double* __restrict__ vx, const double* __restrict__ vy,
+                                   const double* __restrict__ vz, HydroRec<T>* __restrict__ hrec)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    hrec[i].vx = T(vx[i]);
+    hrec[i].vy = T(vy[i]);
+    hrec[i].vz = T(vz[i]);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -972,6 +991,16 @@ int launchVeDefGradhEos(const ChainArrays<T>& a, const HydroConsts<T>& k, const 
 }
 
 template<class T>
+int launchPackVelocity(const ChainArrays<T>& a, cudaStream_t s)
+{
+    if (a.n == 0) { return kOk; }
+    packVelocityKernel<T><<<ceilDiv(a.n, 256), 256, 0, s>>>(a.n, a.vx, a.vy, a.vz, a.hrec);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
+
+template<class T>
 int launchIadDivvCurlv(const ChainArrays<T>& a, const HydroConsts<T>& k, const DevBox& box, cudaStream_t s)
 {
     if (a.n == 0 || (a.groupList && a.numListed == 0)) { return kOk; }
@@ -1024,6 +1053,7 @@ int launchMomentumEnergy(const ChainArrays<T>& a, const HydroConsts<T>& k, const
 #define SPHB_INSTANTIATE(T)                                                                                            \
     template int launchXMass<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);          \
     template int launchVeDefGradhEos<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);  \
+    template int launchPackVelocity<T>(const ChainArrays<T>&, cudaStream_t);                                           \
     template int launchIadDivvCurlv<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, cudaStream_t);   \
     template int launchAVswitches<T>(const ChainArrays<T>&, const HydroConsts<T>&, const DevBox&, double,            \
                                      cudaStream_t);                                                                  \

@@ -236,6 +236,11 @@ __global__ void minMaxKernel(const double* v, size_t n, unsigned long long* out)
     }
 }
 
+__global__ void setWordsKernel(unsigned long long* dst, int count, unsigned long long v0, unsigned long long v1)
+{
+    if (threadIdx.x < unsigned(count)) { dst[threadIdx.x] = threadIdx.x == 0 ? v0 : v1; }
+}
+
 //! out[0..6) = ordered bits of the running min/max of x, y and z (after minMax3InitKernel)
 __global__ void minMax3InitKernel(unsigned long long* out)
 {
@@ -275,6 +280,15 @@ __global__ void minMax3Kernel(const double* x, const double* y, const double* z,
 }
 
 } // namespace
+
+int setWords(unsigned long long* dst, int count, unsigned long long v0, unsigned long long v1, cudaStream_t s)
+{
+    if (count < 1 || count > 2) { return kErrArg; }
+    setWordsKernel<<<1, 32, 0, s>>>(dst, count, v0, v1);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
 
 int minMax3(const double* x, const double* y, const double* z, size_t n, unsigned long long* out6, cudaStream_t s)
 {
@@ -356,8 +370,7 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
 
 int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s)
 {
-    unsigned long long init[2] = {orderedBits(INFINITY), orderedBits(-INFINITY)};
-    SPHB_CUDA_TRY(cudaMemcpyAsync(out2, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    SPHB_TRY(setWords(out2, 2, orderedBits(INFINITY), orderedBits(-INFINITY), s));
     int blocks = int(std::min<size_t>(std::max<size_t>(ceilDiv(n, 256), 1), size_t(smCount()) * 4));
     minMaxKernel<<<blocks, 256, 0, s>>>(v, n, out2);
     countLaunch();

@@ -53,5 +53,8 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
 int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s);
 //! the extrema of x, y and z into out6 as ordered bits {min x, max x, min y, max y, min z, max z}, stream-ordered
 int minMax3(const double* x, const double* y, const double* z, size_t n, unsigned long long* out6, cudaStream_t s);
+/*! dst[0] = v0 and, with count 2, dst[1] = v1, written by a kernel: unlike a copy from host memory, it never waits on
+ *  the stream for a copy engine busy with another stream's transfers */
+int setWords(unsigned long long* dst, int count, unsigned long long v0, unsigned long long v1, cudaStream_t s);
 
 } // namespace sphb

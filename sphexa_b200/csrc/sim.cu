@@ -129,6 +129,7 @@ int syncDomain(sphb_sim& s)
 {
     cudaStream_t st = s.stream;
     // late fields a previous reordering sync left ungathered are put in its order before this one reorders again
+    if (s.midGatherPending) { SPHB_TRY(simimpl::waitMidFields(s)); }
     for (int g = 0; g < sphb_sim::kLateGroups; ++g)
     {
         if (s.lateGatherPending[g]) { SPHB_TRY(simimpl::waitLateGroup(s, g)); }
@@ -154,10 +155,9 @@ int syncDomain(sphb_sim& s)
 
     if (!identity)
     {
-        SPHB_TRY(simimpl::waitMidFields(s));
-        // reorder every conserved field and the ids into SFC order; the late groups of a typed host load still in
-        // flight are gathered with the same order once they arrive (waitLateGroup): the rest of the sync, the search
-        // and XMass read none of them
+        // reorder every conserved field and the ids into SFC order. Fields of a typed host load still in flight are
+        // gathered with the same order once they arrive (waitMidFields: h and the ids, before the search;
+        // waitLateGroup): the rest of the sync reads only x, y, z and m
         const void* src[kNumConserved + 2];
         void* dst[kNumConserved + 2];
         bool now[kNumConserved];
@@ -165,16 +165,20 @@ int syncDomain(sphb_sim& s)
         for (int k = 0; k < kNumConserved; ++k)
         {
             int g  = simimpl::lateGroupOf(k);
-            now[k] = g < 0 || !s.latePending[g];
+            now[k] = k == fH ? !s.midPending : (g < 0 || !s.latePending[g]);
             if (g >= 0 && s.latePending[g]) { s.lateGatherPending[g] = true; }
             if (!now[k]) { continue; }
             src[numFields] = s.f[k].data();
             dst[numFields] = s.fAlt[k].data();
             ++numFields;
         }
-        src[numFields] = s.id.data();
-        dst[numFields] = s.idAlt.data();
-        ++numFields;
+        s.midGatherPending = s.midPending;
+        if (!s.midPending)
+        {
+            src[numFields] = s.id.data();
+            dst[numFields] = s.idAlt.data();
+            ++numFields;
+        }
         if (s.bdt)
         {
             src[numFields] = s.rung.data();
@@ -186,7 +190,7 @@ int syncDomain(sphb_sim& s)
         {
             if (now[k]) { s.f[k].swap(s.fAlt[k]); }
         }
-        s.id.swap(s.idAlt);
+        if (!s.midGatherPending) { s.id.swap(s.idAlt); }
         if (s.bdt) { s.rung.swap(s.rungAlt); }
     }
 
@@ -333,7 +337,11 @@ int runChainStage(sphb_sim& s, int stage)
     switch (stage)
     {
     case sXMass: return launchXMass(a, k, s.box, st);
-    case sVeDefGradh: return launchVeDefGradhEos(a, k, s.box, st);
+    case sVeDefGradh:
+        // the velocities of a typed host load still in flight: their part of the hydro record follows before IAD
+        a.recordNoVelocity    = s.latePending[1];
+        s.velocityPackPending = a.recordNoVelocity;
+        return launchVeDefGradhEos(a, k, s.box, st);
     case sIad: return launchIadDivvCurlv(a, k, s.box, st);
     case sAV:
         if (s.taping)
@@ -509,9 +517,10 @@ int searchNeighbors(sphb_sim& s)
 int runStage(sphb_sim& s, int stage)
 {
     cudaStream_t st = s.stream;
-    // the sync (unless it reorders), the search and XMass read only x, y, z, h and m; the force stages no x_m1, y_m1,
-    // z_m1 or du_m1
+    // the sync (unless it reorders), the search and XMass read only x, y, z, h and m, VeDefGradh also temp, IAD and
+    // the later J-loops also v and alpha; the force stages no x_m1, y_m1, z_m1 or du_m1
     if (stage > sXMass) { SPHB_TRY(simimpl::waitLateGroup(s, 0)); }
+    if (stage > sVeDefGradh) { SPHB_TRY(simimpl::waitLateGroup(s, 1)); }
     if (stage >= sConserved) { SPHB_TRY(simimpl::waitLateFields(s)); }
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[stage], st));
     switch (stage)
@@ -526,8 +535,7 @@ int runStage(sphb_sim& s, int stage)
             SPHB_CUDA_TRY(cudaMemcpyAsync(s.hPre.data(), s.f[fH].data(), s.n * sizeof(double),
                                           cudaMemcpyDeviceToDevice, st));
         }
-        unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
-        SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
+        SPHB_TRY(setWords(s.reduce.data(), 2, orderedBits(-INFINITY), orderedBits(INFINITY), st));
         SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
         return searchNeighbors(s);
     }
@@ -738,8 +746,8 @@ int bdtSync(sphb_sim& s)
     SPHB_TRY(packPositionsAndBoxes(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.f[fM].data(), s.n,
                                    s.pos.data(), s.mixed ? s.posq.data() : nullptr, s.box, s.blockLo.data(),
                                    s.blockHi.data(), st));
-    unsigned long long zero = orderedBits(0.0), dmax = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(s.dispMax.data(), &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+    unsigned long long dmax = 0;
+    SPHB_TRY(setWords(s.dispMax.data(), 1, orderedBits(0.0), 0, st));
     SPHB_TRY(launchMaxDisplacement(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.xs.data(), s.ys.data(),
                                    s.zs.data(), s.n, s.box, s.dispMax.data(), st));
     SPHB_CUDA_TRY(cudaMemcpyAsync(&dmax, s.dispMax.data(), sizeof(dmax), cudaMemcpyDeviceToHost, st));
@@ -795,8 +803,7 @@ int bdtComputeForces(sphb_sim& s)
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sSync], st));
     SPHB_TRY(bdtSync(s));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[sNeighbors], st));
-    unsigned long long init[2] = {orderedBits(-INFINITY), orderedBits(INFINITY)};
-    SPHB_CUDA_TRY(cudaMemcpyAsync(s.reduce.data(), init, sizeof(init), cudaMemcpyHostToDevice, st));
+    SPHB_TRY(setWords(s.reduce.data(), 2, orderedBits(-INFINITY), orderedBits(INFINITY), st));
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data(), 0, sizeof(unsigned), st));
     SPHB_TRY(searchNeighbors(s));
     SPHB_TRY(s.mixed ? bdtChain<float>(s) : bdtChain<double>(s));
@@ -1718,10 +1725,12 @@ namespace simimpl
 int runStage(sphb_sim& s, int stage) { return runStageChecked(s, stage); }
 int waitMidFields(sphb_sim& s)
 {
-    if (!s.midPending) { return kOk; }
-    SPHB_CUDA_TRY(cudaStreamWaitEvent(s.stream, s.midReady, 0));
-    s.midPending = false;
-    if (s.idCheckPending)
+    if (s.midPending)
+    {
+        SPHB_CUDA_TRY(cudaStreamWaitEvent(s.stream, s.midReady, 0));
+        s.midPending = false;
+    }
+    if (s.idCheckPending && !s.idCheckIssued)
     {
         // the loaded ids (now s.id) against the previous ones (s.idAlt), before a reordering sync reuses idAlt; the
         // host reads the flag where it decides between the rows and the tree search
@@ -1730,6 +1739,17 @@ int waitMidFields(sphb_sim& s)
         SPHB_CUDA_TRY(cudaMemcpyAsync(s.hostMsg + 14, s.skinWork.data(), sizeof(unsigned), cudaMemcpyDeviceToHost,
                                       s.stream));
         SPHB_CUDA_TRY(cudaEventRecord(s.idCheckDone, s.stream));
+        s.idCheckIssued = true;
+    }
+    if (s.midGatherPending)
+    {
+        // h and the ids into the order of the last sync (which gathered the fields it reads itself)
+        const void* src[2] = {s.f[fH].data(), s.id.data()};
+        void* dst[2]       = {s.fAlt[fH].data(), s.idAlt.data()};
+        SPHB_TRY(gather8(s.order.data(), s.n, 2, src, dst, s.stream));
+        s.f[fH].swap(s.fAlt[fH]);
+        s.id.swap(s.idAlt);
+        s.midGatherPending = false;
     }
     return kOk;
 }
@@ -1743,6 +1763,7 @@ int resolveIdCheck(sphb_sim& s)
     std::memcpy(&differ, s.hostMsg + 14, sizeof(differ));
     if (differ) { s.skinValid = false; }
     s.idCheckPending = false;
+    s.idCheckIssued  = false;
     return kOk;
 }
 
@@ -1750,17 +1771,23 @@ int lateGroupOf(int field)
 {
     switch (field)
     {
-    case fTemp:
+    case fTemp: return 0;
     case fVx:
     case fVy:
     case fVz:
-    case fAlpha: return 0;
+    case fAlpha: return 1;
     case fXm1:
     case fYm1:
     case fZm1:
-    case fDuM1: return 1;
+    case fDuM1: return 2;
     default: return -1;
     }
+}
+
+int packVelocity(sphb_sim& s)
+{
+    return s.mixed ? launchPackVelocity(chainArrays<float>(s), s.stream)
+                   : launchPackVelocity(chainArrays<double>(s), s.stream);
 }
 
 int waitLateGroup(sphb_sim& s, int group)
@@ -1790,6 +1817,11 @@ int waitLateGroup(sphb_sim& s, int group)
             if (lateGroupOf(k) == group) { s.f[k].swap(s.fAlt[k]); }
         }
         s.lateGatherPending[group] = false;
+    }
+    if (group == 1 && s.velocityPackPending)
+    {
+        SPHB_TRY(packVelocity(s));
+        s.velocityPackPending = false;
     }
     return kOk;
 }
@@ -1843,6 +1875,7 @@ int finishLoad(sphb_sim& s)
         // host before the neighbour search
         s.id.swap(s.idAlt);
         s.idCheckPending = true;
+        s.idCheckIssued  = false;
         return kOk;
     }
     SPHB_TRY(idsDiffer(s.id.data(), s.idAlt.data(), s.n, s.skinWork.data(), s.stream));

@@ -120,12 +120,13 @@ struct sphb_sim
     cudaStream_t sideStream{nullptr}; // the tree search of deferred groups, beside the refilter
     // typed loads from host memory: x, y, z and m come first on the compute stream; the rest follows on copyStream in
     // the order the step reads it: h and the ids while the sync runs (midReady: read by a reordering sync's gather,
-    // else by the search); temp, v and alpha, first read by VeDefGradh and IAD, while the search and XMass run (late
-    // group 0); x_m1, y_m1, z_m1 and du_m1, first read by the integration, while the J-loops run (late group 1).
+    // else by the search); then the late groups, temp (first read by VeDefGradh, group 0), v and alpha (IAD and the
+    // velocity part of the hydro record, group 1), x_m1, y_m1, z_m1 and du_m1 (the integration, group 2).
     // midPending / latePending say that the compute stream has not waited for them yet; lateGatherPending, that a
-    // reordering sync left the group to be gathered once it arrives; idCheckPending, that the comparison of the loaded
-    // ids with the previous ones (whether the skin rows stay usable) is on its way to hostMsg[14] (idCheckDone)
-    static constexpr int kLateGroups = 2;
+    // reordering sync left the group to be gathered once it arrives; velocityPackPending, that VeDefGradh left the
+    // velocities of the hydro record to the arrival of group 1; idCheckPending, that the comparison of the loaded ids
+    // with the previous ones (whether the skin rows stay usable) is on its way to hostMsg[14] (idCheckDone)
+    static constexpr int kLateGroups = 3;
     cudaStream_t copyStream{nullptr};
     cudaEvent_t copyFork{nullptr}, midReady{nullptr}, idCheckDone{nullptr};
     cudaEvent_t lateReady[kLateGroups]{};
@@ -133,6 +134,9 @@ struct sphb_sim
     bool latePending[kLateGroups]{};
     bool lateGatherPending[kLateGroups]{};
     bool idCheckPending{false};
+    bool idCheckIssued{false}; // the comparison is on the compute stream (idCheckDone recorded)
+    bool velocityPackPending{false};
+    bool midGatherPending{false}; // a reordering sync left h and the ids to be gathered once they arrive
     cudaEvent_t skinFork{nullptr}, skinJoin{nullptr};
     unsigned skinCap{0};
     bool skinValid{false};    // rows match the particles' current indices (up to the tracked permutation)
@@ -224,8 +228,8 @@ int positions(sphb_sim& s, double dt, double dtM1);
 //! the compute stream waits for h and the ids of a typed host load, if they are still in flight, and compares the
 //! ids with the previous ones when skin rows exist
 int waitMidFields(sphb_sim& s);
-//! late group of a conserved field of a typed host load (temp, v, alpha: 0; x_m1, y_m1, z_m1, du_m1: 1; -1 for the
-//! fields copied before them)
+//! late group of a conserved field of a typed host load (temp: 0; v, alpha: 1; x_m1, y_m1, z_m1, du_m1: 2; -1 for
+//! the fields copied before them)
 int lateGroupOf(int field);
 //! the compute stream waits for one late group of a typed host load if it is still in flight, and gathers it if a
 //! reordering sync left it

@@ -195,9 +195,9 @@ def _shuffle(bufs, seed):
 
 
 def test_host_load_overlapped_copies_equal_device_load(lib):
-    """A typed load from host memory leaves h, m and the ids in flight beside the next step's keys, sort and trees,
-    temp, v and alpha beside the sync, the search and XMass, and x_m1, y_m1, z_m1 and du_m1 beside the J-loops. Seven
-    round trips (store to pinned host
+    """A typed load from host memory leaves h and the ids in flight beside the next step's sync, temp, v and alpha
+    beside the search and XMass (VeDefGradh then leaves the velocities of its hydro record to a later kernel), and
+    x_m1, y_m1, z_m1 and du_m1 beside the J-loops. Seven round trips (store to pinned host
     buffers in the reference's default types, load, step) give the same states, bit for bit, as the same round trips
     through device buffers, where every copy is ordered on the simulation's stream. Twice the stored particles are
     shuffled before the load: the sync then reorders all of them while the late fields are still in flight (they
