@@ -458,6 +458,25 @@ int exportEarly(sphb_sim& s, std::vector<OutField>& out, std::initializer_list<c
     }
     return kOk;
 }
+/*! h as the end-of-step update will leave it: it depends only on nc and h, both final after the neighbour search, so
+ *  it is computed now into a staging slot and copied out on the copy stream while the J-loops run */
+int exportH(sphb_sim& s, std::vector<OutField>& out, size_t& slot)
+{
+    for (auto& o : out)
+    {
+        if (o.done || std::strcmp(o.d->name, "h") != 0) { continue; }
+        char* stage = s.earlyStage.data() + slot * s.n * 8;
+        ++slot;
+        SPHB_TRY(predictH(s.n, s.p.ng0, s.nc.data(), s.f[fH].data(), stage, o.d->dtype, s.stream));
+        SPHB_CUDA_TRY(cudaEventRecord(s.copyFork, s.stream));
+        SPHB_CUDA_TRY(cudaStreamWaitEvent(s.copyStream, s.copyFork, 0));
+        SPHB_CUDA_TRY(cudaMemcpyAsync(o.d->data, stage, s.n * widthOf(o.d->dtype), cudaMemcpyDeviceToHost,
+                                      s.copyStream));
+        o.done = true;
+    }
+    return kOk;
+}
+
 /*! the outputs left after the step: the fields in their own type are copied straight from their buffers on the copy
  *  stream while the compute stream converts the others into their staging slots; the converted ones follow */
 int exportFinal(sphb_sim& s, std::vector<OutField>& out, size_t& slot)
@@ -522,7 +541,7 @@ extern "C" int sphb_sim_step_fields(sphb_sim* s, const sphb_field* in, int num_i
     {
         numConverted += o.src != o.d->dtype ? 1 : 0;
     }
-    SPHB_TRY(s->earlyStage.reserve(std::max<size_t>(numConverted, 1) * s->n * 8));
+    SPHB_TRY(s->earlyStage.reserve((numConverted + 1) * s->n * 8));
     SPHB_TRY(importConserved(*s, in, num_in, false, true));
     SPHB_TRY(simimpl::finishLoad(*s));
     size_t slot = 0;
@@ -538,6 +557,7 @@ extern "C" int sphb_sim_step_fields(sphb_sim* s, const sphb_field* in, int num_i
         // m and the ids are final once the sync has ordered them, alpha once the AV switches have updated it. m and
         // the ids are copied out from IAD on, when the loaded fields have arrived: earlier, the two directions would
         // share the link while the step waits for the loaded fields
+        if (rc == kOk && stage == sNeighbors) { rc = exportH(*s, outs, slot); }
         if (rc == kOk && stage == sIad) { rc = exportEarly(*s, outs, {"m", "id"}, slot); }
         if (rc == kOk && stage == sAV) { rc = exportEarly(*s, outs, {"alpha"}, slot); }
         if (rc != kOk) { return fail(rc); }

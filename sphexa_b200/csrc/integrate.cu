@@ -148,6 +148,17 @@ __global__ void updateHKernel(size_t n, unsigned ng0, const unsigned* nc, double
     h[i]         = __dmul_rn(__dmul_rn(h[i], 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
 }
 
+//! the smoothing length updateHKernel will write, in FP32 or FP64 (SPHB_F32 / SPHB_F64), without its side effects
+__global__ void predictHKernel(size_t n, unsigned ng0, const unsigned* nc, const double* h, void* out, int outType)
+{
+    size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x;
+    if (i >= n) { return; }
+    double ratio = __ddiv_rn(__dmul_rn(1023.0, double(ng0)), double(nc[i]));
+    double hNew  = __dmul_rn(__dmul_rn(h[i], 0.5), pow(__dadd_rn(1.0, ratio), 0.1));
+    if (outType == SPHB_F32) { static_cast<float*>(out)[i] = float(hNew); }
+    else { static_cast<double*>(out)[i] = hNew; }
+}
+
 constexpr int kRedThreads = 256;
 
 //! per-block partial sums of the conserved quantities: eKin, eInt, P(3), L(3), sum nc (9 doubles)
@@ -280,6 +291,16 @@ __global__ void minMax3Kernel(const double* x, const double* y, const double* z,
 }
 
 } // namespace
+
+int predictH(size_t n, unsigned ng0, const unsigned* nc, const double* h, void* out, int outType, cudaStream_t s)
+{
+    if (outType != SPHB_F32 && outType != SPHB_F64) { return kErrArg; }
+    if (n == 0) { return kOk; }
+    predictHKernel<<<ceilDiv(n, 256), 256, 0, s>>>(n, ng0, nc, h, out, outType);
+    countLaunch();
+    SPHB_CUDA_TRY(cudaGetLastError());
+    return kOk;
+}
 
 int setWords(unsigned long long* dst, int count, unsigned long long v0, unsigned long long v1, cudaStream_t s)
 {

@@ -53,6 +53,10 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
 int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s);
 //! the extrema of x, y and z into out6 as ordered bits {min x, max x, min y, max y, min z, max z}, stream-ordered
 int minMax3(const double* x, const double* y, const double* z, size_t n, unsigned long long* out6, cudaStream_t s);
+/*! the smoothing lengths the end-of-step update (launchUpdateH) will produce from nc and h, into out as SPHB_F32 or
+ *  SPHB_F64, with none of its other effects: for copying them out before the step ends */
+int predictH(size_t n, unsigned ng0, const unsigned* nc, const double* h, void* out, int outType, cudaStream_t s);
+
 /*! dst[0] = v0 and, with count 2, dst[1] = v1, written by a kernel: unlike a copy from host memory, it never waits on
  *  the stream for a copy engine busy with another stream's transfers */
 int setWords(unsigned long long* dst, int count, unsigned long long v0, unsigned long long v1, cudaStream_t s);
