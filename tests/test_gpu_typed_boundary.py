@@ -238,22 +238,30 @@ def test_host_load_overlapped_copies_equal_device_load(lib):
     assert a.search_stats()["skin_builds"] >= 3, a.search_stats()
 
 
-def test_step_fields_equals_load_step_store(lib):
-    """sphb_sim_step_fields (the load, the step and the store in one call, with m, id and alpha copied out while the
-    later stages run) gives the same host state as the three calls one after another, over five round trips with
-    the same pinned arrays as input and output."""
+@pytest.mark.parametrize("types,precision", [("reference", "mixed"), ("double", "mixed"), ("float", "fp64")])
+def test_step_fields_equals_load_step_store(lib, types, precision):
+    """sphb_sim_step_fields (the load, the step and the store in one call, with m, id, alpha and h copied out while
+    the later stages run) gives the same host state as the three calls one after another, over five round trips with
+    the same pinned arrays as input and output. The caller's arrays have the reference's default types (a mix of
+    float and double), or all double (no conversion on either side), or all float (every field converted)."""
     import torch
     from sphexa_b200 import ic as icm
     from sphexa_b200 import lib as L
     from sphexa_b200.simulation import Simulation
     ic = icm.sedov(24)
-    a = Simulation(ic, "mixed")
-    b = Simulation(ic, "mixed")
+    a = Simulation(ic, precision)
+    b = Simulation(ic, precision)
     n = a.n
 
+    def dtype_of(f):
+        if types == "double":
+            return torch.float64
+        if types == "float":
+            return torch.float32
+        return torch.float64 if f in DOUBLE_FIELDS else torch.float32
+
     def buffers():
-        d = {f: torch.empty(n, dtype=torch.float64 if f in DOUBLE_FIELDS else torch.float32, pin_memory=True)
-             for f in CONSERVED}
+        d = {f: torch.empty(n, dtype=dtype_of(f), pin_memory=True) for f in CONSERVED}
         d["id"] = torch.empty(n, dtype=torch.int64, pin_memory=True)
         return d
 
