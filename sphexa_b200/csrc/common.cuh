@@ -1,5 +1,6 @@
 // Shared device/host helpers of the sm_100a hydro library.
 #pragma once
+#include <initializer_list>
 
 #include <algorithm>
 #include <cstdint>
@@ -94,5 +95,24 @@ inline unsigned ceilDiv(size_t a, unsigned b) { return unsigned((a + b - 1) / b)
 
 //! number of SMs of the current device, cached per process
 int smCount();
+
+/*! A small block of pinned host memory of the calling thread (kReadbackWords words, usable from every device), for
+ *  the small reads of the per-step host decisions: a copy into pageable memory returns only when it has completed, so
+ *  two of them wait for the stream twice, while copies into pinned memory queue behind the kernels and one
+ *  synchronisation serves them all. Null if the allocation failed. */
+constexpr int kReadbackWords = 16;
+unsigned long long* pinnedReadback();
+
+//! one small read of readBack: bytes of device memory at src, for host memory at dst
+struct ReadItem
+{
+    void* dst;
+    const void* src;
+    size_t bytes;
+};
+
+/*! the items copied through pinnedReadback() with one wait on the stream (at most kReadbackWords * 8 bytes in all;
+ *  through pageable memory, one wait per item, if the pinned block is missing) */
+int readBack(cudaStream_t stream, std::initializer_list<ReadItem> items);
 
 } // namespace sphb

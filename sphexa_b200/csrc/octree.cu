@@ -542,9 +542,7 @@ int globalTreeStep(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s
     countLaunch();
     SPHB_CUDA_TRY(cudaGetLastError());
     unsigned msg[3]; // new leaf count, any op, largest count
-    SPHB_CUDA_TRY(cudaMemcpyAsync(msg, s.ints.data() + L, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 1, s.flags.data(), 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    SPHB_TRY(readBack(stream, {{msg, s.ints.data() + L, sizeof(int)}, {msg + 1, s.flags.data(), 2 * sizeof(unsigned)}}));
     int newL       = int(msg[0]);
     unsigned anyOp = msg[1];
     if (anyOp)
@@ -564,8 +562,7 @@ int globalTreeStep(GlobalTree& g, const uint64_t* keys, size_t n, TreeScratch& s
         maxCountKernel<<<ceilDiv(newL, 256), 256, 0, stream>>>(g.counts.data(), newL, s.flags.data());
         countLaunch();
         SPHB_CUDA_TRY(cudaGetLastError());
-        SPHB_CUDA_TRY(cudaMemcpyAsync(msg + 2, s.flags.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
-        SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+        SPHB_TRY(readBack(stream, {{msg + 2, s.flags.data() + 1, sizeof(unsigned)}}));
     }
     *maxCount = anyOp ? msg[2] : 0u;
     return kOk;
@@ -648,9 +645,7 @@ int focusUpdateTree(FocusTree& f, const GlobalTree& g, TreeScratch& s, cudaStrea
     SPHB_TRY(exclusiveScan(leafOps, leafOps, L + 1, s.scanTmp.data(), stream));
     int newL = 0;
     unsigned flags[3];
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&newL, leafOps + L, sizeof(int), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(flags, s.flags.data(), sizeof(flags), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    SPHB_TRY(readBack(stream, {{&newL, leafOps + L, sizeof(int)}, {flags, s.flags.data(), sizeof(flags)}}));
     unsigned status = flags[0];
     bool conv       = flags[1] == 0;
     if (status == kCancelMerge) { conv = flags[2] == 0; }
@@ -874,9 +869,7 @@ extern "C" int sphb_rebalance_tree(const uint64_t* leaves, size_t num_leaves, co
     SPHB_TRY(exclusiveScan(s.ints.data(), s.ints.data(), L + 1, s.scanTmp.data(), st));
     int newL       = 0;
     unsigned anyOp = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&newL, s.ints.data() + L, sizeof(int), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&anyOp, s.flags.data(), sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    SPHB_TRY(readBack(st, {{&newL, s.ints.data() + L, sizeof(int)}, {&anyOp, s.flags.data(), sizeof(unsigned)}}));
     *num_new   = size_t(newL);
     *converged = anyOp ? 0 : 1;
     if (size_t(newL) + 1 > capacity) { return SPHB_ERR_CAPACITY; }

@@ -1,4 +1,6 @@
 // Scans and gathers (see primitives.cuh).
+#include <cstring>
+
 #include "primitives.cuh"
 
 namespace sphb
@@ -21,6 +23,63 @@ int smCount()
         if (sms <= 0) { sms = 148; }
     }
     return sms;
+}
+
+unsigned long long* pinnedReadback()
+{
+    struct Block
+    {
+        unsigned long long* p{nullptr};
+        Block()
+        {
+            if (cudaHostAlloc(reinterpret_cast<void**>(&p), kReadbackWords * sizeof(unsigned long long),
+                              cudaHostAllocPortable) != cudaSuccess)
+            {
+                p = nullptr;
+                cudaGetLastError();
+            }
+        }
+        ~Block()
+        {
+            if (p) { cudaFreeHost(p); }
+        }
+    };
+    thread_local Block block;
+    return block.p;
+}
+
+int readBack(cudaStream_t stream, std::initializer_list<ReadItem> items)
+{
+    unsigned long long* pin = pinnedReadback();
+    size_t total            = 0;
+    for (const ReadItem& it : items)
+    {
+        total += (it.bytes + 7) / 8 * 8;
+    }
+    if (!pin || total > kReadbackWords * sizeof(unsigned long long))
+    {
+        for (const ReadItem& it : items)
+        {
+            SPHB_CUDA_TRY(cudaMemcpyAsync(it.dst, it.src, it.bytes, cudaMemcpyDeviceToHost, stream));
+        }
+        SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+        return kOk;
+    }
+    size_t off = 0;
+    for (const ReadItem& it : items)
+    {
+        SPHB_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(pin) + off, it.src, it.bytes, cudaMemcpyDeviceToHost,
+                                      stream));
+        off += (it.bytes + 7) / 8 * 8;
+    }
+    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    off = 0;
+    for (const ReadItem& it : items)
+    {
+        std::memcpy(it.dst, reinterpret_cast<const char*>(pin) + off, it.bytes);
+        off += (it.bytes + 7) / 8 * 8;
+    }
+    return kOk;
 }
 
 namespace

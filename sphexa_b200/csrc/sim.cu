@@ -93,8 +93,7 @@ int updateBox(sphb_sim& s)
     SPHB_TRY(s.boxExtrema.reserve(6));
     SPHB_TRY(minMax3(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.n, s.boxExtrema.data(), s.stream));
     unsigned long long mm[6];
-    SPHB_CUDA_TRY(cudaMemcpyAsync(mm, s.boxExtrema.data(), sizeof(mm), cudaMemcpyDeviceToHost, s.stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    SPHB_TRY(readBack(s.stream, {{mm, s.boxExtrema.data(), sizeof(mm)}}));
     for (int k = 0; k < 3; ++k)
     {
         fit[2 * k]     = s.hbox.lo[k];
@@ -649,9 +648,8 @@ int integrateStep(sphb_sim& s)
     SPHB_CUDA_TRY(cudaMemsetAsync(s.status.data() + 1, 0, sizeof(unsigned), st));
     SPHB_TRY(launchUpdateH(s.n, s.p.ng0, s.nc.data(), s.f[fH].data(), s.keys.data(), s.status.data() + 1, st));
     unsigned flag = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&flag, s.status.data() + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     SPHB_CUDA_TRY(cudaEventRecord(s.ev[kNumStages], st));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    SPHB_TRY(readBack(st, {{&flag, s.status.data() + 1, sizeof(unsigned)}}));
     for (int k = 0; k < kNumStages; ++k)
     {
         cudaEventElapsedTime(&s.stageMs[k], s.ev[k], s.ev[k + 1]);
@@ -750,8 +748,7 @@ int bdtSync(sphb_sim& s)
     SPHB_TRY(setWords(s.dispMax.data(), 1, orderedBits(0.0), 0, st));
     SPHB_TRY(launchMaxDisplacement(s.f[fX].data(), s.f[fY].data(), s.f[fZ].data(), s.xs.data(), s.ys.data(),
                                    s.zs.data(), s.n, s.box, s.dispMax.data(), st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&dmax, s.dispMax.data(), sizeof(dmax), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    SPHB_TRY(readBack(st, {{&dmax, s.dispMax.data(), sizeof(dmax)}}));
     double lenMax = std::max({s.box.len[0], s.box.len[1], s.box.len[2]});
     s.treeExt     = fromOrderedBits(dmax) * (1.0 + 1e-9) + 1e-14 * lenMax;
     int highest   = butterflyOf(uint32_t(s.bts.substep));
@@ -845,9 +842,7 @@ int sortGroupDt(sphb_sim& s, unsigned num, float* minDt, float* fastDt, uint32_t
     SPHB_TRY(launchSortedDt(s.dtKeys.data(), num, fastIdx, s.groupDt.data(), s.rungInfo.data(), st));
     uint32_t info[1 + kMaxRungs];
     unsigned err = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(info, s.rungInfo.data(), sizeof(info), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.status.data() + 2, sizeof(err), cudaMemcpyDeviceToHost, st));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(st));
+    SPHB_TRY(readBack(st, {{info, s.rungInfo.data(), sizeof(info)}, {&err, s.status.data() + 2, sizeof(err)}}));
     if (err) { return kErrCuda; }
     std::memcpy(minDt, &info[0], sizeof(float));
     std::memcpy(fastDt, &info[1], sizeof(float));

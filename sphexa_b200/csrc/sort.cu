@@ -488,8 +488,7 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
     }
     SPHB_TRY(runPasses(keys, values, n, s, mask, stream));
     uint32_t err = 0;
-    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+    SPHB_TRY(readBack(stream, {{&err, s.counters + 1, sizeof(uint32_t)}}));
     // 1: a look-back wait gave up; 2: offsets left inconsistent by such a wait (nothing else produces them)
     return err ? kErrTimeout : kOk;
 }
@@ -513,8 +512,7 @@ int sortNearlySorted(uint64_t* keys, uint32_t* values, size_t n, void* scratch, 
         SPHB_CUDA_TRY(cudaMemsetAsync(s.counters, 0, sizeof(uint32_t), stream));
         inversionsKernel<<<blocks, 256, 0, stream>>>(keys, n, s.counters);
         SPHB_CUDA_TRY(cudaGetLastError());
-        SPHB_CUDA_TRY(cudaMemcpyAsync(out, s.counters, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
+        SPHB_TRY(readBack(stream, {{out, s.counters, sizeof(uint32_t)}}));
         return kOk;
     };
     uint32_t inv = 0;
