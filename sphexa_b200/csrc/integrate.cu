@@ -227,26 +227,6 @@ __global__ void conservedFinalKernel(const double* partial, int numBlocks, doubl
     if (lane == 0) { out[q] = s; }
 }
 
-__global__ void minMaxKernel(const double* v, size_t n, unsigned long long* out)
-{
-    double lo = INFINITY, hi = -INFINITY;
-    for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
-    {
-        lo = fmin(lo, v[i]);
-        hi = fmax(hi, v[i]);
-    }
-    for (int off = 16; off > 0; off >>= 1)
-    {
-        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, off));
-        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, off));
-    }
-    if ((threadIdx.x & 31) == 0)
-    {
-        atomicMin(out, orderedBits(lo));
-        atomicMax(out + 1, orderedBits(hi));
-    }
-}
-
 __global__ void setWordsKernel(unsigned long long* dst, int count, unsigned long long v0, unsigned long long v1)
 {
     if (threadIdx.x < unsigned(count)) { dst[threadIdx.x] = threadIdx.x == 0 ? v0 : v1; }
@@ -389,15 +369,6 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
     return kOk;
 }
 
-int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s)
-{
-    SPHB_TRY(setWords(out2, 2, orderedBits(INFINITY), orderedBits(-INFINITY), s));
-    int blocks = int(std::min<size_t>(std::max<size_t>(ceilDiv(n, 256), 1), size_t(smCount()) * 4));
-    minMaxKernel<<<blocks, 256, 0, s>>>(v, n, out2);
-    countLaunch();
-    SPHB_CUDA_TRY(cudaGetLastError());
-    return kOk;
-}
 
 template int launchPositions<double>(size_t, const IntegrateArrays<double>&, const DevBox&, double, double, double,
                                      cudaStream_t);

@@ -49,8 +49,6 @@ int conservedSums(size_t n, const double* x, const double* y, const double* z, c
                   const double* vz, const double* m, const double* temp, const unsigned* nc, double cv,
                   double* partial, int maxBlocks, double* out9, cudaStream_t s);
 
-//! out2 = ordered bits of (min, max) of v
-int minMax(const double* v, size_t n, unsigned long long* out2, cudaStream_t s);
 //! the extrema of x, y and z into out6 as ordered bits {min x, max x, min y, max y, min z, max z}, stream-ordered
 int minMax3(const double* x, const double* y, const double* z, size_t n, unsigned long long* out6, cudaStream_t s);
 /*! the smoothing lengths the end-of-step update (launchUpdateH) will produce from nc and h, into out as SPHB_F32 or
