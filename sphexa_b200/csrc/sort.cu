@@ -488,7 +488,10 @@ int sortByKey(uint64_t* keys, uint32_t* values, size_t n, bool initValues, void*
     }
     SPHB_TRY(runPasses(keys, values, n, s, mask, stream));
     uint32_t err = 0;
-    SPHB_TRY(readBack(stream, {{&err, s.counters + 1, sizeof(uint32_t)}}));
+    // a plain read: this path serves sphb_sort_by_key_static, which must call no allocating routine (the pinned
+    // block of readBack is allocated on its first use in a thread)
+    SPHB_CUDA_TRY(cudaMemcpyAsync(&err, s.counters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    SPHB_CUDA_TRY(cudaStreamSynchronize(stream));
     // 1: a look-back wait gave up; 2: offsets left inconsistent by such a wait (nothing else produces them)
     return err ? kErrTimeout : kOk;
 }
